@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Throughput benchmark: RCWA solves/s on B200.
+
+Workload (default): the 2D rectangular-pillar grating, Nx=Ny=10 (441 orders,
+882 x 882 complex layer matrices), period 400 x 400 nm, 5 patterned layers,
+256 wavelengths x 8 conical incidences (2048 solves), seeded synthetic inputs.
+One step = one batched pass of the full RCWA solve (convolution matrices,
+per-layer eigenproblems, interface solves, S-matrix cascade, per-order
+efficiencies of TE and TM) over a batch of --batch points of that sweep.
+
+value: device time of K plan executions with the inputs resident (CUDA events
+on the launching stream, max over ranks).  e2e: the same metric through the
+public C ABI (rcwa_engine_solve_batch) with host buffers, host<->device copies
+inside the timed region.  --impl reference times the CPU oracle (the NumPy
+restatement of the reference's LAPACK path) on the host cores.
+
+Multi-GPU: every rank solves its own batch of the sweep (weak scaling, no
+data-path collective); only the barrier and the max of the timings cross ranks.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "RCWA solves/s on 1 B200: batched mixed vs plain FP64, max|dR,T|<=1e-4"
+WORKLOAD = "2D rectangular-pillar grating Nx=Ny=10 (441 orders, 882x882), 5 patterned layers, 400x400 nm, " \
+           "256 wavelengths x 8 conical angles, TE+TM"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=32, help="solve points per step per GPU")
+    ap.add_argument("--nh", type=int, default=10, help="harmonics per axis (Nx=Ny)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def fp64_gemm_peak_tflops(torch):
+    """cuBLAS DGEMM throughput (torch.matmul float64, 8192^3, best of 5): the
+    FP64 denominator of the eigensolver roofline (the pool's peak file has
+    only HBM and BF16)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def eig_flops(n):
+    """Algorithmic real flops of one complex eigen-decomposition with
+    eigenvectors, split as in Golub & Van Loan (complex = 4x real counts):
+    Hessenberg + Q accumulation 4.67 n^3 x 4, QR iteration with T and Z
+    20.33 n^3 x 4 (together 25 n^3 x 4 = 100 n^3)."""
+    return {"hessenberg": 18.67 * n ** 3, "schur_qr": 81.33 * n ** 3, "total": 100.0 * n ** 3}
+
+
+def cpu_solve_sample(stacks, pts, pxy, count):
+    """Time `count` solves of the oracle on the host (all BLAS threads)."""
+    import oracle.rcwa_oracle as orc
+    st = stacks[0]
+    t0 = time.perf_counter()
+    for p in range(count):
+        _, lam, kx0, ky0 = pts[p]
+        s = orc.RCWASolver(st.nHx, st.nHy)
+        for l in range(st.eps.shape[0]):
+            s.addLayer(orc.OracleLayer(st.cx, st.cy, st.eps[l]))
+        s.setBlochWavevector(kx0, ky0)
+        s.solve(lam, list(range(st.eps.shape[0])), list(st.thickness))
+        k0 = 2 * np.pi / lam
+        for e in range(pxy.shape[1]):
+            c = s.generateHorizontalPlaneWave(pxy[p, e, 0], pxy[p, e, 1], 0)
+            s.scatterPlaneWave(c, 0, st.eps.shape[0] - 1, k0)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    from openrcwa_b200 import workloads
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    stacks, pts, pxy = workloads.pillars_2d(seed=0, nH=args.nh)
+    for _ in range(args.warmup):
+        cpu_solve_sample(stacks, pts, pxy, 1)
+    tt = 0.0
+    for k in range(args.steps):
+        tt += cpu_solve_sample(stacks, pts[k:], pxy[k:], 1)
+    value = args.steps / tt
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tt / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "sample": "1 solve per step", "parallelism": "host BLAS threads"},
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{args.steps} solves of the sweep (points 0..{args.steps - 1}), "
+                                       "NumPy/OpenBLAS zgeev path, all host threads"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+
+    import openrcwa_b200 as o
+    from openrcwa_b200 import workloads
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def allmax(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    stacks, pts, pxy = workloads.pillars_2d(seed=0, nH=args.nh)
+    N = stacks[0].N
+    n = 2 * N
+    B = args.batch
+    eng = o.Engine(local)
+    bpts, bpxy = workloads.batch_slice(pts, pxy, rank * B, B)
+    plan = eng.plan(stacks, bpts, bpxy)
+    stream = torch.cuda.Stream()
+    for _ in range(args.warmup):
+        plan.execute(stream.cuda_stream)
+    stream.synchronize()
+    R, T, _, _, status = plan.results()
+    if np.any(status):
+        raise SystemExit(f"solve status {status}")
+    fp64_peak = fp64_gemm_peak_tflops(torch)
+    barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    plan.set_profiling(True)
+    stage_ms = {}
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        plan.execute(stream.cuda_stream)
+        for k, v in plan.stage_times().items():
+            stage_ms[k] = stage_ms.get(k, 0.0) + v
+    e1.record(stream)
+    stream.synchronize()
+    clk = clocks.stop()
+    plan.set_profiling(False)
+    t_ms = allmax(e0.elapsed_time(e1))
+    launches = plan.launch_count() * args.steps
+    value = world * B * args.steps / (t_ms * 1e-3)
+
+    # e2e: the public C ABI with host buffers, a different batch each step
+    barrier()
+    h2d = d2h = 0
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        p2, x2 = workloads.batch_slice(pts, pxy, (rank + world * (k + 1)) * B, B)
+        R2, T2, _, _, st2 = eng.solve_batch(stacks, p2, x2, orders=False)
+        st = stacks[0]
+        h2d += st.eps.nbytes + st.cx.nbytes + st.cy.nbytes + st.thickness.nbytes + p2.nbytes + x2.nbytes
+        d2h += R2.nbytes + T2.nbytes + st2.nbytes
+    barrier()
+    e2e_s = allmax(time.perf_counter() - t0)
+    e2e = world * B * args.steps / e2e_s
+
+    # roofline of the dominant stage
+    peaks, peak_kind = measured_peaks()
+    per_launch = {k: v / args.steps for k, v in stage_ms.items()}
+    dom = max(per_launch, key=per_launch.get)
+    jobs = B * (stacks[0].eps.shape[0] - 2)
+    fl = eig_flops(n)
+    roof = None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get(dom)
+    if dom in ("schur_qr", "hessenberg"):
+        achieved = fl[dom] * jobs / (per_launch[dom] * 1e-3) / 1e12
+        roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp64_peak, "traffic": traffic,
+                "peak_source": "FP64 DGEMM measured in this run (cuBLAS via torch)",
+                "flops_per_launch": fl[dom] * jobs, "ms_per_launch": per_launch[dom]}
+    conv = None
+    if per_launch.get("conv_gather"):
+        pass
+    line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "batch_points_per_gpu": B, "orders": N, "matrix": n,
+                       "precision": "plain FP64 (mixed path not built)", "parallelism": f"replicas x{world}",
+                       "l2": "per-step working set several GB > 126 MB L2"},
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
+                    "d2h_bytes_per_step": d2h // args.steps},
+            "gpu_launches": launches, "clocks": clk, "roofline": roof,
+            "stage_ms_per_step": per_launch, "peaks": {"fp64_dgemm_tflops": fp64_peak,
+                                                       "hbm_gbs": peaks.get("hbm_gbs"), "source": peak_kind}}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        tcpu = cpu_solve_sample(stacks, pts, pxy, 1)
+        line["cpu_baseline"] = {"value": 1.0 / tcpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
+                                "sample": "1 solve (point 0) of the sweep through the NumPy oracle, all BLAS threads"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

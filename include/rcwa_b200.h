@@ -1,0 +1,205 @@
+/*
+ * rcwa_b200.h — C ABI of the B200 RCWA diffraction-efficiency engine.
+ *
+ * Plain C types only: pointers, sizes, and complex numbers as interleaved
+ * double pairs.  Every entry point returns an RCWA_* status code.  All device
+ * memory is owned by the engine; host buffers passed in are only read during
+ * the call, host buffers passed out are written before the call returns.
+ *
+ * Each entry point names the reference interface it replaces
+ * (Sirokujira/OpenRCWA paths, file:line).  Units are the caller's: lengths in
+ * any unit (the .ofd bridge uses metres), wavenumbers in rad per that unit.
+ */
+#ifndef RCWA_B200_H
+#define RCWA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define RCWA_OK            0
+#define RCWA_ERR_INVALID   1  /* bad sizes / pointers / geometry                     */
+#define RCWA_ERR_CUDA      2  /* CUDA runtime failure                                */
+#define RCWA_ERR_NOCONV    3  /* eigenvalue QR exceeded its iteration budget         */
+#define RCWA_ERR_SINGULAR  4  /* exactly zero pivot in an LU factorisation           */
+#define RCWA_ERR_NONFINITE 5  /* NaN / Inf in a result                               */
+#define RCWA_ERR_GRAZING   6  /* kz == 0 or incident kz ~ 0 (scatterPlaneWave early return,
+                                 rcwa/RCWASolver.cpp:1843-1847,1898-1901)            */
+#define RCWA_ERR_NOMEM     7  /* device allocation failed                            */
+#define RCWA_ERR_NODEVICE  8  /* no usable CUDA device                               */
+#define RCWA_ERR_UNSUPPORTED 9 /* a feature outside this engine's scope (see docs)  */
+
+/* ---- Fourier rule options (rcwa/FourierSolver2D.h:8-13) ------------------- */
+#define RCWA_CONTINUOUS_XY   0
+#define RCWA_DISCONTINUOUS_X 1
+#define RCWA_DISCONTINUOUS_Y 2
+
+/* ---- precision of the batched solve ---------------------------------------- */
+#define RCWA_PREC_FP64  0     /* every stage complex128                           */
+
+typedef struct { double re, im; } rcwa_cplx;
+
+typedef struct rcwa_engine rcwa_engine;
+typedef struct rcwa_plan rcwa_plan;
+
+/* A layer stack on one common cell grid: what RCWASolver(nX, nY) holds after
+ * addLayer() of every layer (rcwa/RCWASolver.h:67-84, rcwa/Layer.h:29-31).
+ * eps[l] is a (ncy-1) x (ncx-1) row-major grid, row = y strip, column = x
+ * strip, exactly the Layer eps_ matrix.  Layer 0 is the incidence half-space,
+ * layer n_layers-1 the transmission half-space; both must be uniform (every
+ * cell equal), as sol/rcwa_bridge.cpp:255-259 assumes.  thickness[l] is used
+ * for 0 < l < n_layers-1 only (rcwa/RCWASolver.cpp:415-431). */
+typedef struct {
+  int nHx, nHy;              /* harmonics: 2*nHx+1 by 2*nHy+1 orders            */
+  int ncx, ncy;              /* number of cell edges along x and y (>= 2)        */
+  const double* cx;          /* [ncx] ascending; period Lx = cx[ncx-1]-cx[0]     */
+  const double* cy;          /* [ncy] ascending                                  */
+  int n_layers;              /* >= 2                                             */
+  const rcwa_cplx* eps;      /* [n_layers][ncy-1][ncx-1]                         */
+  const double* thickness;   /* [n_layers]                                       */
+} rcwa_stack;
+
+/* One solve point: one RCWASolver::solve (rcwa/RCWASolver.cpp:139-148) of a
+ * stack at one wavelength and Bloch wavevector (setBlochWavevector,
+ * rcwa/RCWASolver.h:180). */
+typedef struct {
+  int stack;                 /* index into the stack array                       */
+  double lambda;             /* vacuum wavelength                                */
+  double kx0, ky0;           /* Bloch wavevector offsets                         */
+} rcwa_point;
+
+/* ---- engine ----------------------------------------------------------------- */
+const char* rcwa_status_string(int status);
+int rcwa_engine_create(int device, rcwa_engine** out);
+void rcwa_engine_destroy(rcwa_engine* e);
+/* Message of the last failure on this engine ("" if none). */
+const char* rcwa_engine_last_error(const rcwa_engine* e);
+
+/* Batched diffraction efficiencies.  Replaces, for every point, the sequence
+ *   RCWASolver::solve                         rcwa/RCWASolver.cpp:139-148
+ *   generateHorizontalPlaneWave(px, py, 0)    rcwa/RCWASolver.cpp:1778-1789
+ *   scatterPlaneWave(c, 0, L-1, k0, REF, TRN) rcwa/RCWASolver.cpp:1792-1908
+ *   R = REF.sum(), T = TRN.sum()              sol/rcwa_bridge.cpp:311-312
+ * for n_exc incident transverse polarisation vectors per point.
+ *   pxy        [n_pts][n_exc][2] complex (px, py), host
+ *   R, T       [n_pts][n_exc], host
+ *   ref_orders, trn_orders: NULL or per-point blocks of n_exc*N doubles, point
+ *              p's block starting at sum_{q<p} n_exc*N_q (N = orders of the
+ *              point's stack), order k = (2nHy+1)*(m+nHx) + (n+nHy); unmasked
+ *              REF/TRN vectors as scatterPlaneWave returns them
+ *   status     [n_pts] per-point RCWA_* code, host (may be NULL)
+ * Returns RCWA_OK when the call itself ran; per-point failures are reported in
+ * status (and the call returns the first non-zero point status). */
+int rcwa_engine_solve_batch(rcwa_engine* e,
+                            const rcwa_stack* stacks, int n_stacks,
+                            const rcwa_point* pts, int n_pts,
+                            int n_exc, const rcwa_cplx* pxy,
+                            int precision,
+                            double* R, double* T,
+                            double* ref_orders, double* trn_orders,
+                            int* status);
+
+/* The same solve split in three so that a caller can keep the inputs resident
+ * and time the device work alone: plan_create uploads the inputs and sizes the
+ * workspace, plan_execute enqueues every kernel on `stream` (a cudaStream_t,
+ * NULL = the engine's own stream) without synchronising, plan_results waits
+ * and copies the outputs back (same layouts as rcwa_engine_solve_batch). */
+int rcwa_plan_create(rcwa_engine* e,
+                     const rcwa_stack* stacks, int n_stacks,
+                     const rcwa_point* pts, int n_pts,
+                     int n_exc, const rcwa_cplx* pxy, int precision,
+                     rcwa_plan** out);
+int rcwa_plan_execute(rcwa_plan* p, void* stream);
+int rcwa_plan_results(rcwa_plan* p, double* R, double* T,
+                      double* ref_orders, double* trn_orders, int* status);
+/* Number of engine kernel launches the last plan_execute enqueued. */
+long long rcwa_plan_launch_count(const rcwa_plan* p);
+/* Per-stage device time: with profiling on, plan_execute records CUDA events
+ * between the stages on its stream; plan_stage_times waits and writes the
+ * milliseconds of every stage of the last execution into ms[max_stages] and
+ * returns the number of stages; rcwa_stage_name names stage i.  (The
+ * reference only has commented-out host timers, rcwa/Layer.cpp:245-252.) */
+int rcwa_plan_set_profiling(rcwa_plan* p, int on);
+int rcwa_plan_stage_times(rcwa_plan* p, double* ms, int max_stages);
+const char* rcwa_stage_name(int stage);
+void rcwa_plan_destroy(rcwa_plan* p);
+
+/* ---- stage entry points (host buffers in and out, synchronous) -------------- */
+
+/* FourierSolver1D(x, d).solve(f, M, Ff)   rcwa/FourierSolver1D.cpp:11-41.
+ * x[nxe] edges, f[nxe-1], Ff[M]. */
+int rcwa_fourier1d(rcwa_engine* e, const double* x, int nxe, double d,
+                   const rcwa_cplx* f, int M, rcwa_cplx* Ff);
+
+/* FourierSolver2D(cx, cy).solve(f, nx, ny, opt, Ff)   rcwa/FourierSolver2D.cpp:12-351.
+ * f[(ncy-1)*(ncx-1)] row-major (row = y), Ff[(nx*ny)^2] row-major. */
+int rcwa_fourier2d(rcwa_engine* e, const double* cx, int ncx, const double* cy, int ncy,
+                   const rcwa_cplx* f, int nx, int ny, int opt, rcwa_cplx* Ff);
+
+/* Layer::solve for one patterned layer   rcwa/Layer.cpp:255-273 with
+ * Layer::waveEqnCoeff (:75-253) and WaveEquationSolver::solve
+ * (rcwa/WaveEquationSolver.cpp:24-37).  alpha/beta[nx*ny] are the diagonals
+ * of Kx/Ky (RCWASolver::evaluateAlphaBeta, rcwa/RCWASolver.cpp:242-266).
+ * Outputs (any may be NULL), n = 2*nx*ny:
+ *   W, V [n*n] row-major: eigvecE / eigvecH (columns = modes, unit 2-norm)
+ *   gamma [n]: Layer::gamma() = keff/k0
+ *   eigenvalues [n]: eigenvalues of P*Q. */
+int rcwa_layer_solve(rcwa_engine* e, const double* cx, int ncx, const double* cy, int ncy,
+                     const rcwa_cplx* eps, int nx, int ny,
+                     const double* alpha, const double* beta, double lambda,
+                     rcwa_cplx* W, rcwa_cplx* V, rcwa_cplx* gamma, rcwa_cplx* eigenvalues);
+
+/* Batched right eigenvectors of general complex matrices:
+ * MKLEigenSolver<MatrixXcs>::compute (LAPACKE zgeev('N','V') branch,
+ * rcwa/MKLEigenSolver.hpp:102-179).  A[batch][n*n] row-major, w[batch][n],
+ * VR[batch][n*n] row-major (columns unit 2-norm), info[batch]. */
+int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
+                       rcwa_cplx* w, rcwa_cplx* VR, int* info);
+
+/* ---- the .ofd RCWA mode (sol/rcwa_bridge.cpp) --------------------------- */
+
+/* rcwalayer_t, same fields and order (include/orcwa_rcwa.h:33-41). */
+typedef struct {
+  double eps1, eps2, eps1i, eps2i, fill, fill_y, thickness;
+} rcwa_layer_spec;
+
+/* rcwapole_t, same fields and order (include/orcwa_rcwa.h:51-58); layer 0-based. */
+typedef struct {
+  int layer, side;
+  double einf, ae, be, ce;
+} rcwa_pole_spec;
+
+/* The globals rcwa_run() reads (include/orcwa_rcwa.h:60-76, sol/rcwa_bridge.cpp:35-40). */
+typedef struct {
+  int nHx;                       /* NRcwaHarmonics   */
+  double period_x;               /* RcwaPeriod       */
+  int nHy;                       /* NRcwaHarmonicsY  */
+  double period_y;               /* RcwaPeriodY (used when nHy > 0, else period_x) */
+  int n_layers;                  /* NRcwaLayer       */
+  const rcwa_layer_spec* layers; /* RcwaLayer        */
+  int n_poles;                   /* NRcwaPole        */
+  const rcwa_pole_spec* poles;   /* RcwaPole         */
+  double theta_deg, phi_deg;     /* RcwaTheta, RcwaPhi */
+  int n_freq;                    /* NFreq1           */
+  const double* freq;            /* Freq1 [Hz]       */
+} rcwa_ofd_setup;
+
+/* The computation of rcwa_run (sol/rcwa_bridge.cpp:145-366) with every
+ * frequency solved in one batch, without the file output:
+ *   R, T        [n_freq][2]  (TE, TM) totals, REF.sum() / TRN.sum() (:311-312)
+ *   ordR, ordT  NULL or [2][n_freq][nOrdX*nOrdY] propagating-order efficiencies,
+ *               evanescent orders set to 0 (the bridge's ordR/ordT, :289-319)
+ *   status      NULL or [n_freq]
+ * Returns 1-style errors as RCWA_ERR_INVALID for an invalid setup (:149-152,
+ * :246-249). */
+int rcwa_ofd_solve(rcwa_engine* e, const rcwa_ofd_setup* s, double* R, double* T,
+                   double* ordR, double* ordT, int* status);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RCWA_B200_H */

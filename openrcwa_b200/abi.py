@@ -1,0 +1,345 @@
+"""ctypes binding of the C ABI in ``include/rcwa_b200.h``.
+
+The library is loaded from ``openrcwa_b200/lib/librcwa_b200.so`` (built by
+``openrcwa_b200.build``); a missing library raises immediately: there is no
+CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "librcwa_b200.so")
+
+RCWA_OK = 0
+RCWA_ERR_INVALID = 1
+RCWA_ERR_CUDA = 2
+RCWA_ERR_NOCONV = 3
+RCWA_ERR_SINGULAR = 4
+RCWA_ERR_NONFINITE = 5
+RCWA_ERR_GRAZING = 6
+RCWA_ERR_NOMEM = 7
+RCWA_ERR_NODEVICE = 8
+RCWA_ERR_UNSUPPORTED = 9
+RCWA_CONTINUOUS_XY, RCWA_DISCONTINUOUS_X, RCWA_DISCONTINUOUS_Y = 0, 1, 2
+RCWA_PREC_FP64 = 0
+
+# every symbol declared in include/rcwa_b200.h
+EXPORTS = [
+    "rcwa_status_string", "rcwa_engine_create", "rcwa_engine_destroy", "rcwa_engine_last_error",
+    "rcwa_engine_solve_batch", "rcwa_plan_create", "rcwa_plan_execute", "rcwa_plan_results",
+    "rcwa_plan_launch_count", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
+    "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
+    "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_ofd_solve",
+]
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int)
+
+
+class rcwa_stack(C.Structure):
+    _fields_ = [("nHx", C.c_int), ("nHy", C.c_int), ("ncx", C.c_int), ("ncy", C.c_int),
+                ("cx", C.c_void_p), ("cy", C.c_void_p), ("n_layers", C.c_int),
+                ("eps", C.c_void_p), ("thickness", C.c_void_p)]
+
+
+class rcwa_point(C.Structure):
+    _fields_ = [("stack", C.c_int), ("lambda_", C.c_double), ("kx0", C.c_double), ("ky0", C.c_double)]
+
+
+class rcwa_layer_spec(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("eps1", "eps2", "eps1i", "eps2i", "fill", "fill_y", "thickness")]
+
+
+class rcwa_pole_spec(C.Structure):
+    _fields_ = [("layer", C.c_int), ("side", C.c_int)] + [(k, C.c_double) for k in ("einf", "ae", "be", "ce")]
+
+
+class rcwa_ofd_setup(C.Structure):
+    _fields_ = [("nHx", C.c_int), ("period_x", C.c_double), ("nHy", C.c_int), ("period_y", C.c_double),
+                ("n_layers", C.c_int), ("layers", C.POINTER(rcwa_layer_spec)),
+                ("n_poles", C.c_int), ("poles", C.POINTER(rcwa_pole_spec)),
+                ("theta_deg", C.c_double), ("phi_deg", C.c_double),
+                ("n_freq", C.c_int), ("freq", _DP)]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the engine library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"RCWA engine library missing: {LIB_PATH} (run python -m openrcwa_b200.build)")
+    lib = C.CDLL(LIB_PATH)
+    lib.rcwa_status_string.restype = C.c_char_p
+    lib.rcwa_status_string.argtypes = [C.c_int]
+    lib.rcwa_engine_create.argtypes = [C.c_int, C.POINTER(C.c_void_p)]
+    lib.rcwa_engine_destroy.argtypes = [C.c_void_p]
+    lib.rcwa_engine_destroy.restype = None
+    lib.rcwa_engine_last_error.argtypes = [C.c_void_p]
+    lib.rcwa_engine_last_error.restype = C.c_char_p
+    lib.rcwa_engine_solve_batch.argtypes = [C.c_void_p, C.POINTER(rcwa_stack), C.c_int, C.POINTER(rcwa_point),
+                                            C.c_int, C.c_int, C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _IP]
+    lib.rcwa_plan_create.argtypes = [C.c_void_p, C.POINTER(rcwa_stack), C.c_int, C.POINTER(rcwa_point), C.c_int,
+                                     C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
+    lib.rcwa_plan_execute.argtypes = [C.c_void_p, C.c_void_p]
+    lib.rcwa_plan_results.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _IP]
+    lib.rcwa_plan_launch_count.argtypes = [C.c_void_p]
+    lib.rcwa_plan_launch_count.restype = C.c_longlong
+    lib.rcwa_plan_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    lib.rcwa_plan_stage_times.argtypes = [C.c_void_p, _DP, C.c_int]
+    lib.rcwa_stage_name.argtypes = [C.c_int]
+    lib.rcwa_stage_name.restype = C.c_char_p
+    lib.rcwa_plan_destroy.argtypes = [C.c_void_p]
+    lib.rcwa_plan_destroy.restype = None
+    lib.rcwa_fourier1d.argtypes = [C.c_void_p, _DP, C.c_int, C.c_double, C.c_void_p, C.c_int, C.c_void_p]
+    lib.rcwa_fourier2d.argtypes = [C.c_void_p, _DP, C.c_int, _DP, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                                   C.c_void_p]
+    lib.rcwa_layer_solve.argtypes = [C.c_void_p, _DP, C.c_int, _DP, C.c_int, C.c_void_p, C.c_int, C.c_int, _DP, _DP,
+                                     C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    lib.rcwa_zgeev_batched.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, _IP]
+    lib.rcwa_ofd_solve.argtypes = [C.c_void_p, C.POINTER(rcwa_ofd_setup), _DP, _DP, _DP, _DP, _IP]
+    _lib = lib
+    return lib
+
+
+def _d(a):
+    return a.ctypes.data_as(_DP)
+
+
+def _v(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_IP)
+
+
+class RcwaError(RuntimeError):
+    def __init__(self, code, msg=""):
+        self.code = code
+        super().__init__(f"rcwa status {code} ({load().rcwa_status_string(code).decode()}) {msg}")
+
+
+class Stack:
+    """A layer stack on a common cell grid (owns its numpy buffers)."""
+
+    def __init__(self, nHx, nHy, cx, cy, eps, thickness):
+        self.nHx, self.nHy = int(nHx), int(nHy)
+        self.cx = np.ascontiguousarray(cx, dtype=np.float64)
+        self.cy = np.ascontiguousarray(cy, dtype=np.float64)
+        self.eps = np.ascontiguousarray(eps, dtype=np.complex128)
+        assert self.eps.ndim == 3 and self.eps.shape[1:] == (self.cy.size - 1, self.cx.size - 1)
+        self.thickness = np.ascontiguousarray(thickness, dtype=np.float64)
+        assert self.thickness.size == self.eps.shape[0]
+
+    @property
+    def N(self):
+        return (2 * self.nHx + 1) * (2 * self.nHy + 1)
+
+    def c_struct(self):
+        return rcwa_stack(self.nHx, self.nHy, self.cx.size, self.cy.size, self.cx.ctypes.data, self.cy.ctypes.data,
+                          self.eps.shape[0], self.eps.ctypes.data, self.thickness.ctypes.data)
+
+
+class Engine:
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.rcwa_engine_create(device, C.byref(h))
+        if rc:
+            raise RcwaError(rc, "engine_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            self.lib.rcwa_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self):
+        return self.lib.rcwa_engine_last_error(self.h).decode()
+
+    def _check(self, rc, what):
+        if rc:
+            raise RcwaError(rc, f"{what}: {self.last_error()}")
+
+    # -- batched solve ------------------------------------------------------
+    @staticmethod
+    def _pack(stacks: Sequence[Stack], points, pxy):
+        st = (rcwa_stack * len(stacks))(*[s.c_struct() for s in stacks])
+        pts = np.asarray(points, dtype=np.float64).reshape(-1, 4)
+        cp = (rcwa_point * len(pts))(*[rcwa_point(int(p[0]), p[1], p[2], p[3]) for p in pts])
+        pxy = np.ascontiguousarray(pxy, dtype=np.complex128)
+        n_exc = pxy.shape[1]
+        assert pxy.shape == (len(pts), n_exc, 2)
+        return st, cp, pxy, n_exc
+
+    def solve_batch(self, stacks, points, pxy, orders=True, precision=RCWA_PREC_FP64):
+        """points: rows (stack, lambda, kx0, ky0); pxy: [n_pts][n_exc][2] complex.
+        Returns R, T [n_pts, n_exc], per-order lists (REF, TRN) [n_pts] of
+        [n_exc, N] arrays, status [n_pts]."""
+        st, cp, pxy, n_exc = self._pack(stacks, points, pxy)
+        npt = len(cp)
+        R = np.zeros((npt, n_exc))
+        T = np.zeros((npt, n_exc))
+        Ns = [stacks[int(p.stack)].N for p in cp]
+        tot = sum(Ns) * n_exc
+        ref = np.zeros(max(tot, 1)) if orders else None
+        trn = np.zeros(max(tot, 1)) if orders else None
+        status = np.zeros(npt, dtype=np.int32)
+        rc = self.lib.rcwa_engine_solve_batch(self.h, st, len(stacks), cp, npt, n_exc, _v(pxy), precision, _d(R),
+                                              _d(T), _d(ref) if orders else None, _d(trn) if orders else None,
+                                              _i(status))
+        if rc and not np.any(status):
+            self._check(rc, "solve_batch")
+        REF = TRN = None
+        if orders:
+            REF, TRN, o = [], [], 0
+            for N in Ns:
+                REF.append(ref[o:o + n_exc * N].reshape(n_exc, N))
+                TRN.append(trn[o:o + n_exc * N].reshape(n_exc, N))
+                o += n_exc * N
+        return R, T, REF, TRN, status
+
+    def plan(self, stacks, points, pxy, precision=RCWA_PREC_FP64):
+        return Plan(self, stacks, points, pxy, precision)
+
+    # -- stage entry points --------------------------------------------------
+    def fourier1d(self, x, d, f, M):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        f = np.ascontiguousarray(f, dtype=np.complex128)
+        out = np.zeros(M, dtype=np.complex128)
+        self._check(self.lib.rcwa_fourier1d(self.h, _d(x), x.size, d, _v(f), M, _v(out)), "fourier1d")
+        return out
+
+    def fourier2d(self, cx, cy, f, nx, ny, opt):
+        cx = np.ascontiguousarray(cx, dtype=np.float64)
+        cy = np.ascontiguousarray(cy, dtype=np.float64)
+        f = np.ascontiguousarray(f, dtype=np.complex128)
+        out = np.zeros((nx * ny, nx * ny), dtype=np.complex128)
+        self._check(self.lib.rcwa_fourier2d(self.h, _d(cx), cx.size, _d(cy), cy.size, _v(f), nx, ny, opt, _v(out)),
+                    "fourier2d")
+        return out
+
+    def layer_solve(self, cx, cy, eps, nx, ny, alpha, beta, lam):
+        cx = np.ascontiguousarray(cx, dtype=np.float64)
+        cy = np.ascontiguousarray(cy, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.complex128)
+        alpha = np.ascontiguousarray(alpha, dtype=np.float64)
+        beta = np.ascontiguousarray(beta, dtype=np.float64)
+        n = 2 * nx * ny
+        W = np.zeros((n, n), dtype=np.complex128)
+        V = np.zeros((n, n), dtype=np.complex128)
+        g = np.zeros(n, dtype=np.complex128)
+        ev = np.zeros(n, dtype=np.complex128)
+        self._check(self.lib.rcwa_layer_solve(self.h, _d(cx), cx.size, _d(cy), cy.size, _v(eps), nx, ny, _d(alpha),
+                                              _d(beta), lam, _v(W), _v(V), _v(g), _v(ev)), "layer_solve")
+        return W, V, g, ev
+
+    def zgeev(self, A):
+        A = np.ascontiguousarray(A, dtype=np.complex128)
+        if A.ndim == 2:
+            A = A[None]
+        b, n, _ = A.shape
+        w = np.zeros((b, n), dtype=np.complex128)
+        VR = np.zeros((b, n, n), dtype=np.complex128)
+        info = np.zeros(b, dtype=np.int32)
+        rc = self.lib.rcwa_zgeev_batched(self.h, n, b, _v(A), _v(w), _v(VR), _i(info))
+        if rc and not np.any(info):
+            self._check(rc, "zgeev")
+        return w, VR, info
+
+    def ofd_solve(self, setup, orders=True):
+        """The rcwa_run computation for an oracle-style setup object with the
+        fields of rcwa_ofd_setup (layers with eps1..thickness, poles, freqs)."""
+        L = len(setup.layers)
+        lay = (rcwa_layer_spec * L)(*[rcwa_layer_spec(l.eps1, l.eps2, l.eps1i, l.eps2i, l.fill, l.fill_y,
+                                                       l.thickness) for l in setup.layers])
+        npo = len(setup.poles)
+        pol = (rcwa_pole_spec * max(npo, 1))(*[rcwa_pole_spec(p.layer, p.side, p.einf, p.ae, p.be, p.ce)
+                                               for p in setup.poles])
+        fr = np.ascontiguousarray(setup.freqs, dtype=np.float64)
+        py = setup.period_y if setup.period_y is not None else setup.period_x
+        s = rcwa_ofd_setup(setup.nHx, setup.period_x, setup.nHy, py, L, lay, npo, pol, setup.theta, setup.phi,
+                           fr.size, _d(fr))
+        nf = fr.size
+        nord = (2 * setup.nHx + 1) * (2 * setup.nHy + 1)
+        R = np.zeros((nf, 2))
+        T = np.zeros((nf, 2))
+        oR = np.zeros((2, nf, nord)) if orders else None
+        oT = np.zeros((2, nf, nord)) if orders else None
+        st = np.zeros(nf, dtype=np.int32)
+        rc = self.lib.rcwa_ofd_solve(self.h, C.byref(s), _d(R), _d(T), _d(oR) if orders else None,
+                                     _d(oT) if orders else None, _i(st))
+        if rc and not np.any(st):
+            self._check(rc, "ofd_solve")
+        return R, T, oR, oT, st
+
+
+class Plan:
+    """Inputs resident on the device; execute() enqueues the kernels only."""
+
+    def __init__(self, eng: Engine, stacks, points, pxy, precision=RCWA_PREC_FP64):
+        self.eng = eng
+        self.stacks = stacks
+        st, cp, pxy, n_exc = Engine._pack(stacks, points, pxy)
+        self._keep = (st, cp, pxy)
+        self.n_pts, self.n_exc = len(cp), n_exc
+        self.Ns = [stacks[int(p.stack)].N for p in cp]
+        h = C.c_void_p()
+        rc = eng.lib.rcwa_plan_create(eng.h, st, len(stacks), cp, len(cp), n_exc, _v(pxy), precision, C.byref(h))
+        eng._check(rc, "plan_create")
+        self.h = h
+
+    def execute(self, stream: Optional[int] = None):
+        self.eng._check(self.eng.lib.rcwa_plan_execute(self.h, C.c_void_p(stream) if stream else None),
+                        "plan_execute")
+
+    def launch_count(self):
+        return int(self.eng.lib.rcwa_plan_launch_count(self.h))
+
+    def set_profiling(self, on=True):
+        self.eng._check(self.eng.lib.rcwa_plan_set_profiling(self.h, 1 if on else 0), "set_profiling")
+
+    def stage_times(self):
+        """{stage name: milliseconds} of the last execution (profiling on)."""
+        ms = np.zeros(64)
+        n = self.eng.lib.rcwa_plan_stage_times(self.h, _d(ms), 64)
+        return {self.eng.lib.rcwa_stage_name(i).decode(): float(ms[i]) for i in range(n)}
+
+    def results(self, orders=False):
+        R = np.zeros((self.n_pts, self.n_exc))
+        T = np.zeros((self.n_pts, self.n_exc))
+        tot = sum(self.Ns) * self.n_exc
+        ref = np.zeros(max(tot, 1)) if orders else None
+        trn = np.zeros(max(tot, 1)) if orders else None
+        status = np.zeros(self.n_pts, dtype=np.int32)
+        rc = self.eng.lib.rcwa_plan_results(self.h, _d(R), _d(T), _d(ref) if orders else None,
+                                            _d(trn) if orders else None, _i(status))
+        if rc and not np.any(status):
+            self.eng._check(rc, "plan_results")
+        return R, T, ref, trn, status
+
+    def close(self):
+        if self.h:
+            self.eng.lib.rcwa_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

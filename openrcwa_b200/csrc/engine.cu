@@ -1,0 +1,906 @@
+// Host orchestration of the batched RCWA solve and the C ABI.
+//
+// A plan groups the points by their harmonic grid (nx, ny); each group is cut
+// into chunks sized to the device memory budget.  For one chunk the device
+// work is:
+//   conv    per distinct (stack, patterned layer): fe11, fe22, fe33 -> E = fe33^-1
+//   modes   per (point, patterned layer): X1 = E Da fe11, X2 = E Db fe22,
+//           M = PQ/k0^2, eig(M) -> (mu, W), gamma, V = QW/keff; analytic
+//           half-space modes per point
+//   cascade per interface, bottom to top (rcwa/RCWASolver.cpp:378-492):
+//           IE = Wa^-1 Wb, IH = Va^-1 Vb, phase, F, G, tau = (F+G)^-1,
+//           Rud = I - 2 G tau, Tdd = 2 waveTdd tau
+//   scatter per (point, excitation): per-order efficiencies and their sums.
+// Every batched call receives device pointer arrays that the plan built once,
+// so executing a plan is a fixed sequence of kernel launches on one stream.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "eig.cuh"
+#include "engine_internal.cuh"
+#include "fourier.cuh"
+#include "linalg.cuh"
+#include "rcwa_kernels.cuh"
+
+
+namespace {
+
+constexpr double kPi = 3.1415926535897932;
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  ~DevBuf() { if (p) cudaFree(p); }
+};
+
+// Bump allocator over byte offsets; turned into addresses once the base exists.
+struct Layout {
+  size_t off = 0;
+  size_t take(size_t bytes) {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + bytes;
+    return o;
+  }
+};
+
+// Host-side staging of plan metadata (item structs and pointer arrays) that is
+// uploaded in one copy.  Entries are recorded as offsets.
+struct Meta {
+  std::vector<unsigned char> bytes;
+  size_t add(const void* src, size_t n) {
+    size_t o = (bytes.size() + 15) & ~(size_t)15;
+    bytes.resize(o + n);
+    if (n) std::memcpy(bytes.data() + o, src, n);
+    return o;
+  }
+  template <class T>
+  size_t add_vec(const std::vector<T>& v) { return add(v.data(), v.size() * sizeof(T)); }
+};
+
+struct StackInfo {
+  int nx, ny, N, L;
+  double Lx, Ly;
+  std::vector<double> cx, cy;
+  std::vector<cplx> eps;   // L * cells
+  std::vector<double> thick;
+  int ncx, ncy;
+};
+
+}  // namespace
+
+struct rcwa_plan {
+  rcwa_engine* e = nullptr;
+  int n_pts = 0, n_exc = 0;
+  std::vector<int> point_N;            // orders per point
+  std::vector<size_t> order_offset;    // per point, into ref/trn outputs
+  size_t total_orders = 0;
+  DevBuf inputs, meta, work, outputs;
+  double* dR = nullptr;
+  double* dT = nullptr;
+  double* dRef = nullptr;
+  double* dTrn = nullptr;
+  int* dStatus = nullptr;
+  std::vector<std::function<cudaError_t(cudaStream_t, long long&, StageProf&)>> steps;
+  long long launches = 0;
+  std::unique_ptr<StageProf> prof{new StageProf()};
+};
+
+namespace {
+
+int fail(rcwa_engine* e, int code, const std::string& msg) {
+  if (e) e->last_error = msg;
+  return code;
+}
+
+bool finite_c(const rcwa_cplx& z) { return std::isfinite(z.re) && std::isfinite(z.im); }
+
+int validate_stack(const rcwa_stack& s, std::string& why) {
+  if (s.nHx < 0 || s.nHy < 0) { why = "negative harmonic count"; return RCWA_ERR_INVALID; }
+  if (s.ncx < 2 || s.ncy < 2 || !s.cx || !s.cy) { why = "need >= 2 cell edges per axis"; return RCWA_ERR_INVALID; }
+  if (s.n_layers < 2 || !s.eps || !s.thickness) { why = "need >= 2 layers"; return RCWA_ERR_INVALID; }
+  for (int i = 0; i + 1 < s.ncx; ++i)
+    if (!(s.cx[i + 1] >= s.cx[i]) || !std::isfinite(s.cx[i + 1])) { why = "x edges must ascend"; return RCWA_ERR_INVALID; }
+  for (int i = 0; i + 1 < s.ncy; ++i)
+    if (!(s.cy[i + 1] >= s.cy[i]) || !std::isfinite(s.cy[i + 1])) { why = "y edges must ascend"; return RCWA_ERR_INVALID; }
+  if (!(s.cx[s.ncx - 1] > s.cx[0]) || !(s.cy[s.ncy - 1] > s.cy[0])) { why = "zero period"; return RCWA_ERR_INVALID; }
+  const size_t cells = (size_t)(s.ncx - 1) * (s.ncy - 1);
+  for (int l = 0; l < s.n_layers; ++l) {
+    for (size_t c = 0; c < cells; ++c) {
+      const rcwa_cplx z = s.eps[(size_t)l * cells + c];
+      if (!finite_c(z)) { why = "non-finite permittivity"; return RCWA_ERR_INVALID; }
+      if (z.re == 0.0 && z.im == 0.0) { why = "zero permittivity"; return RCWA_ERR_INVALID; }
+    }
+    if (l == 0 || l == s.n_layers - 1) {
+      const rcwa_cplx z0 = s.eps[(size_t)l * cells];
+      for (size_t c = 1; c < cells; ++c) {
+        const rcwa_cplx z = s.eps[(size_t)l * cells + c];
+        if (z.re != z0.re || z.im != z0.im) { why = "half-spaces must be uniform"; return RCWA_ERR_UNSUPPORTED; }
+      }
+    } else if (!std::isfinite(s.thickness[l]) || s.thickness[l] < 0) {
+      why = "invalid thickness";
+      return RCWA_ERR_INVALID;
+    }
+  }
+  return RCWA_OK;
+}
+
+StackInfo make_stack_info(const rcwa_stack& s) {
+  StackInfo si;
+  si.nx = 2 * s.nHx + 1;
+  si.ny = 2 * s.nHy + 1;
+  si.N = si.nx * si.ny;
+  si.L = s.n_layers;
+  si.ncx = s.ncx;
+  si.ncy = s.ncy;
+  si.cx.assign(s.cx, s.cx + s.ncx);
+  si.cy.assign(s.cy, s.cy + s.ncy);
+  si.Lx = si.cx.back() - si.cx.front();
+  si.Ly = si.cy.back() - si.cy.front();
+  const size_t cells = (size_t)(s.ncx - 1) * (s.ncy - 1);
+  si.eps.resize(cells * s.n_layers);
+  for (size_t i = 0; i < si.eps.size(); ++i) si.eps[i] = mkc(s.eps[i].re, s.eps[i].im);
+  si.thick.assign(s.thickness, s.thickness + s.n_layers);
+  return si;
+}
+
+// alpha/beta of RCWASolver::evaluateAlphaBeta (rcwa/RCWASolver.cpp:242-266):
+// mode k = ny*i + j, alpha = 2 pi (i - Nx)/Lx + kx0, beta = 2 pi (j - Ny)/Ly + ky0.
+void alpha_beta(const StackInfo& si, double kx0, double ky0, cplx* ab) {
+  const int Nx = (si.nx - 1) / 2, Ny = (si.ny - 1) / 2;
+  const double Kx = 2 * kPi / si.Lx, Ky = 2 * kPi / si.Ly;
+  for (int i = 0; i < si.nx; ++i)
+    for (int j = 0; j < si.ny; ++j) {
+      const double m = i - Nx, n = j - Ny;
+      ab[si.ny * i + j] = mkc(Kx * m + kx0, 0.0);
+      ab[si.N + si.ny * i + j] = mkc(Ky * n + ky0, 0.0);
+    }
+}
+
+
+}  // namespace
+
+// ------------------------------------------------------------------ C ABI
+extern "C" {
+
+const char* rcwa_status_string(int status) {
+  switch (status) {
+    case RCWA_OK: return "ok";
+    case RCWA_ERR_INVALID: return "invalid argument";
+    case RCWA_ERR_CUDA: return "CUDA error";
+    case RCWA_ERR_NOCONV: return "eigenvalue iteration did not converge";
+    case RCWA_ERR_SINGULAR: return "singular matrix";
+    case RCWA_ERR_NONFINITE: return "non-finite result";
+    case RCWA_ERR_GRAZING: return "grazing / zero kz";
+    case RCWA_ERR_NOMEM: return "out of device memory";
+    case RCWA_ERR_NODEVICE: return "no CUDA device";
+    case RCWA_ERR_UNSUPPORTED: return "unsupported input";
+    default: return "unknown status";
+  }
+}
+
+int rcwa_engine_create(int device, rcwa_engine** out) {
+  if (!out) return RCWA_ERR_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count <= device || device < 0) return RCWA_ERR_NODEVICE;
+  if (cudaSetDevice(device) != cudaSuccess) return RCWA_ERR_NODEVICE;
+  auto* e = new rcwa_engine();
+  e->device = device;
+  if (cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete e;
+    return RCWA_ERR_CUDA;
+  }
+  *out = e;
+  return RCWA_OK;
+}
+
+void rcwa_engine_destroy(rcwa_engine* e) {
+  if (!e) return;
+  cudaSetDevice(e->device);
+  if (e->stream) cudaStreamDestroy(e->stream);
+  delete e;
+}
+
+const char* rcwa_engine_last_error(const rcwa_engine* e) { return e ? e->last_error.c_str() : ""; }
+
+}  // extern "C"
+
+namespace {
+
+// Workspace offsets of one chunk (relative to the workspace base).
+struct ChunkWork {
+  // conv
+  std::vector<int> conv_stack, conv_layer;       // per conv job
+  std::map<std::pair<int, int>, int> conv_index;  // (stack, layer) -> job
+  size_t conv_jobs_off = 0, fe11 = 0, fe22 = 0, fe33 = 0, Einv = 0, tab = 0, tab_elems = 0;
+  size_t tptr = 0, tipiv = 0, tinfo = 0, cipiv = 0, cinfo = 0, convptr = 0;
+  int max_ncx = 2, max_ncy = 2;
+  // layer jobs
+  std::vector<int> job_point, job_layer;          // per layer job (chunk-local point)
+  size_t X1 = 0, X2 = 0, M = 0, W = 0, V = 0, mu = 0, gam = 0, eigw = 0, einfo = 0;
+  // per point
+  std::vector<int> points;                        // global point index
+  size_t hW0 = 0, hV0 = 0, hWL = 0, hVL = 0, hg0 = 0, hgL = 0;
+  size_t Rud = 0, Tdd = 0, F = 0, G = 0, tau = 0, IE = 0, IH = 0, WLU = 0, VLU = 0, pipiv = 0, pinfo = 0;
+  size_t total = 0;
+};
+
+}  // namespace
+
+static size_t chunk_layout(ChunkWork& c, const std::vector<StackInfo>& stacks, int N) {
+  const size_t n = 2 * (size_t)N;
+  const size_t NN = (size_t)N * N, nn = n * n;
+  const size_t cs = sizeof(cplx);
+  Layout L;
+  const size_t nconv = c.conv_stack.size();
+  const int nx = stacks[c.conv_stack.empty() ? 0 : c.conv_stack[0]].nx;
+  const int ny = stacks[c.conv_stack.empty() ? 0 : c.conv_stack[0]].ny;
+  c.tab_elems = conv_table_elems(nx, ny, c.max_ncx, c.max_ncy);
+  const size_t strips = (size_t)std::max(c.max_ncx - 1, c.max_ncy - 1);
+  c.conv_jobs_off = L.take(sizeof(ConvJob) * std::max<size_t>(nconv, 1));
+  c.fe11 = L.take(cs * NN * nconv);
+  c.fe22 = L.take(cs * NN * nconv);
+  c.fe33 = L.take(cs * NN * nconv);
+  c.Einv = L.take(cs * NN * nconv);
+  c.tab = L.take(cs * c.tab_elems * nconv);
+  c.tptr = L.take(sizeof(void*) * 4 * strips * std::max<size_t>(nconv, 1));
+  c.tipiv = L.take(sizeof(int) * strips * std::max(nx, ny) * std::max<size_t>(nconv, 1));
+  c.tinfo = L.take(sizeof(int) * strips * std::max<size_t>(nconv, 1));
+  c.cipiv = L.take(sizeof(int) * N * std::max<size_t>(nconv, 1));
+  c.cinfo = L.take(sizeof(int) * std::max<size_t>(nconv, 1));
+  const size_t nj = c.job_point.size();
+  c.X1 = L.take(cs * NN * nj);
+  c.X2 = L.take(cs * NN * nj);
+  c.M = L.take(cs * nn * nj);
+  c.W = L.take(cs * nn * nj);
+  c.V = L.take(cs * nn * nj);
+  c.mu = L.take(cs * n * nj);
+  c.gam = L.take(cs * n * nj);
+  c.eigw = L.take(zgeev_workspace_bytes((int)n) * nj);
+  c.einfo = L.take(sizeof(int) * std::max<size_t>(nj, 1));
+  const size_t np = c.points.size();
+  c.hW0 = L.take(cs * nn * np);
+  c.hV0 = L.take(cs * nn * np);
+  c.hWL = L.take(cs * nn * np);
+  c.hVL = L.take(cs * nn * np);
+  c.hg0 = L.take(cs * n * np);
+  c.hgL = L.take(cs * n * np);
+  c.Rud = L.take(cs * nn * np);
+  c.Tdd = L.take(cs * nn * np);
+  c.F = L.take(cs * nn * np);
+  c.G = L.take(cs * nn * np);
+  c.tau = L.take(cs * nn * np);
+  c.IE = L.take(cs * nn * np);
+  c.IH = L.take(cs * nn * np);
+  c.WLU = L.take(cs * nn * np);
+  c.VLU = L.take(cs * nn * np);
+  c.pipiv = L.take(sizeof(int) * n * 3 * np);
+  c.pinfo = L.take(sizeof(int) * 3 * np);
+  c.total = L.off;
+  return L.off;
+}
+
+static size_t chunk_bytes_per_point(int N, int Lp) {
+  const double n = 2.0 * N;
+  const double nn = n * n * sizeof(cplx), NN = (double)N * N * sizeof(cplx);
+  const double per_job = 2 * NN + 3 * nn + zgeev_workspace_bytes((int)n) + 4 * NN;
+  return (size_t)(13 * nn + per_job * std::max(Lp - 2, 0));
+}
+
+extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_stacks, const rcwa_point* pts,
+                                int n_pts, int n_exc, const rcwa_cplx* pxy, int precision, rcwa_plan** out) {
+  if (!e || !out) return RCWA_ERR_INVALID;
+  *out = nullptr;
+  if (n_stacks <= 0 || !stacks || n_pts <= 0 || !pts || n_exc <= 0 || !pxy)
+    return fail(e, RCWA_ERR_INVALID, "empty batch or null pointer");
+  if (precision != RCWA_PREC_FP64) return fail(e, RCWA_ERR_UNSUPPORTED, "precision mode not available");
+  if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, RCWA_ERR_CUDA, "cudaSetDevice failed");
+  std::vector<StackInfo> si;
+  for (int s = 0; s < n_stacks; ++s) {
+    std::string why;
+    int rc = validate_stack(stacks[s], why);
+    if (rc) return fail(e, rc, "stack " + std::to_string(s) + ": " + why);
+    si.push_back(make_stack_info(stacks[s]));
+  }
+  for (int p = 0; p < n_pts; ++p) {
+    const rcwa_point& q = pts[p];
+    if (q.stack < 0 || q.stack >= n_stacks) return fail(e, RCWA_ERR_INVALID, "point stack index out of range");
+    if (!(q.lambda > 0) || !std::isfinite(q.lambda) || !std::isfinite(q.kx0) || !std::isfinite(q.ky0))
+      return fail(e, RCWA_ERR_INVALID, "invalid wavelength or Bloch vector");
+  }
+  std::unique_ptr<rcwa_plan> P(new rcwa_plan());
+  P->e = e;
+  P->n_pts = n_pts;
+  P->n_exc = n_exc;
+  P->point_N.resize(n_pts);
+  P->order_offset.resize(n_pts);
+  size_t acc = 0;
+  for (int p = 0; p < n_pts; ++p) {
+    P->point_N[p] = si[pts[p].stack].N;
+    P->order_offset[p] = acc;
+    acc += (size_t)n_exc * P->point_N[p];
+  }
+  P->total_orders = acc;
+
+  // ---- inputs: stack arrays and per-point alpha/beta
+  Layout il;
+  std::vector<size_t> cx_off(n_stacks), cy_off(n_stacks), eps_off(n_stacks);
+  for (int s = 0; s < n_stacks; ++s) {
+    cx_off[s] = il.take(sizeof(double) * si[s].cx.size());
+    cy_off[s] = il.take(sizeof(double) * si[s].cy.size());
+    eps_off[s] = il.take(sizeof(cplx) * si[s].eps.size());
+  }
+  std::vector<size_t> ab_off(n_pts);
+  for (int p = 0; p < n_pts; ++p) ab_off[p] = il.take(sizeof(cplx) * 2 * P->point_N[p]);
+  if (cudaMalloc(&P->inputs.p, il.off) != cudaSuccess) return fail(e, RCWA_ERR_NOMEM, "input allocation failed");
+  P->inputs.bytes = il.off;
+  {
+    std::vector<unsigned char> h(il.off);
+    for (int s = 0; s < n_stacks; ++s) {
+      std::memcpy(h.data() + cx_off[s], si[s].cx.data(), sizeof(double) * si[s].cx.size());
+      std::memcpy(h.data() + cy_off[s], si[s].cy.data(), sizeof(double) * si[s].cy.size());
+      std::memcpy(h.data() + eps_off[s], si[s].eps.data(), sizeof(cplx) * si[s].eps.size());
+    }
+    for (int p = 0; p < n_pts; ++p) alpha_beta(si[pts[p].stack], pts[p].kx0, pts[p].ky0, (cplx*)(h.data() + ab_off[p]));
+    if (cudaMemcpy(P->inputs.p, h.data(), il.off, cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(e, RCWA_ERR_CUDA, "input upload failed");
+  }
+  char* inb = (char*)P->inputs.p;
+
+  // ---- outputs
+  {
+    Layout ol;
+    size_t oR = ol.take(sizeof(double) * n_pts * n_exc), oT = ol.take(sizeof(double) * n_pts * n_exc);
+    size_t oRef = ol.take(sizeof(double) * std::max<size_t>(acc, 1)), oTrn = ol.take(sizeof(double) * std::max<size_t>(acc, 1));
+    size_t oS = ol.take(sizeof(int) * n_pts);
+    if (cudaMalloc(&P->outputs.p, ol.off) != cudaSuccess) return fail(e, RCWA_ERR_NOMEM, "output allocation failed");
+    P->outputs.bytes = ol.off;
+    char* b = (char*)P->outputs.p;
+    P->dR = (double*)(b + oR);
+    P->dT = (double*)(b + oT);
+    P->dRef = (double*)(b + oRef);
+    P->dTrn = (double*)(b + oTrn);
+    P->dStatus = (int*)(b + oS);
+  }
+
+  // ---- chunking: group by (nx, ny), then fill chunks up to the memory budget
+  size_t free_b = 0, total_b = 0;
+  cudaMemGetInfo(&free_b, &total_b);
+  const size_t budget = std::min<size_t>((size_t)(0.6 * free_b), (size_t)96 << 30);
+  std::map<std::pair<int, int>, std::vector<int>> groups;
+  for (int p = 0; p < n_pts; ++p) groups[{si[pts[p].stack].nx, si[pts[p].stack].ny}].push_back(p);
+  std::vector<ChunkWork> chunks;
+  std::vector<int> chunk_N;
+  for (auto& g : groups) {
+    const int N = g.first.first * g.first.second;
+    size_t used = 0;
+    ChunkWork cur;
+    auto flush = [&]() {
+      if (!cur.points.empty()) { chunks.push_back(cur); chunk_N.push_back(N); }
+      cur = ChunkWork();
+      used = 0;
+    };
+    for (int p : g.second) {
+      const size_t need = chunk_bytes_per_point(N, si[pts[p].stack].L);
+      if (!cur.points.empty() && (used + need > budget || cur.points.size() >= 1024)) flush();
+      cur.points.push_back(p);
+      used += need;
+    }
+    flush();
+  }
+  // conv jobs and layer jobs per chunk
+  for (auto& c : chunks) {
+    for (size_t lp = 0; lp < c.points.size(); ++lp) {
+      const int p = c.points[lp];
+      const int s = pts[p].stack;
+      c.max_ncx = std::max(c.max_ncx, si[s].ncx);
+      c.max_ncy = std::max(c.max_ncy, si[s].ncy);
+      for (int l = 1; l + 1 < si[s].L; ++l) {
+        auto key = std::make_pair(s, l);
+        if (!c.conv_index.count(key)) {
+          c.conv_index[key] = (int)c.conv_stack.size();
+          c.conv_stack.push_back(s);
+          c.conv_layer.push_back(l);
+        }
+        c.job_point.push_back((int)lp);
+        c.job_layer.push_back(l);
+      }
+    }
+  }
+  size_t wbytes = 0;
+  for (size_t ci = 0; ci < chunks.size(); ++ci) wbytes = std::max(wbytes, chunk_layout(chunks[ci], si, chunk_N[ci]));
+  if (cudaMalloc(&P->work.p, std::max<size_t>(wbytes, 256)) != cudaSuccess)
+    return fail(e, RCWA_ERR_NOMEM, "workspace allocation failed (" + std::to_string(wbytes >> 20) + " MiB)");
+  P->work.bytes = wbytes;
+  char* wb = (char*)P->work.p;
+
+  // ---- metadata (items and pointer arrays) per chunk, and the launch steps
+  Meta meta;
+  rcwa_plan* plan = P.get();
+  const bool same_conv_as_prev_possible = true;
+  std::vector<std::pair<int, int>> prev_conv_keys;
+  int prev_N = -1;
+
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    ChunkWork& c = chunks[ci];
+    const int N = chunk_N[ci];
+    const int n = 2 * N;
+    const size_t NN = (size_t)N * N, nn = (size_t)n * n;
+    const StackInfo& s0 = si[pts[c.points[0]].stack];
+    const int nx = s0.nx, ny = s0.ny;
+    auto W_ = [&](size_t off) { return (cplx*)(wb + off); };
+    const int nconv = (int)c.conv_stack.size();
+    const int nj = (int)c.job_point.size();
+    const int np = (int)c.points.size();
+
+    // ---------------- conv
+    std::vector<std::pair<int, int>> keys;
+    for (int j = 0; j < nconv; ++j) keys.push_back({c.conv_stack[j], c.conv_layer[j]});
+    const bool reuse_conv = same_conv_as_prev_possible && prev_N == N && keys == prev_conv_keys && ci > 0 &&
+                            chunks[ci - 1].conv_jobs_off == c.conv_jobs_off && chunks[ci - 1].tab_elems == c.tab_elems;
+    prev_conv_keys = keys;
+    prev_N = N;
+    if (nconv > 0 && !reuse_conv) {
+      std::vector<ConvJob> jobs(nconv);
+      for (int j = 0; j < nconv; ++j) {
+        const int s = c.conv_stack[j], l = c.conv_layer[j];
+        const size_t cells = (size_t)(si[s].ncx - 1) * (si[s].ncy - 1);
+        jobs[j].cx = (const double*)(inb + cx_off[s]);
+        jobs[j].cy = (const double*)(inb + cy_off[s]);
+        jobs[j].eps = (const cplx*)(inb + eps_off[s]) + (size_t)l * cells;
+        jobs[j].ncx = si[s].ncx;
+        jobs[j].ncy = si[s].ncy;
+        jobs[j].fe11 = W_(c.fe11) + NN * j;
+        jobs[j].fe22 = W_(c.fe22) + NN * j;
+        jobs[j].fe33 = W_(c.fe33) + NN * j;
+        jobs[j].tab = W_(c.tab) + c.tab_elems * j;
+      }
+      // ConvJob array lives in the workspace (uploaded by a memcpy step)
+      const size_t jobs_meta = meta.add_vec(jobs);
+      ConvLaunch CL;
+      CL.jobs = nullptr;  // set at execution: the job array lives in the metadata block
+      CL.njobs = nconv;
+      CL.nx = nx;
+      CL.ny = ny;
+      CL.max_ncx = c.max_ncx;
+      CL.max_ncy = c.max_ncy;
+      const size_t strips = (size_t)std::max(c.max_ncx - 1, c.max_ncy - 1);
+      cplx** tp = (cplx**)(wb + c.tptr);
+      CL.tx_ptrs = tp;
+      CL.txinv_ptrs = tp + strips * nconv;
+      CL.ty_ptrs = tp + 2 * strips * nconv;
+      CL.tyinv_ptrs = tp + 3 * strips * nconv;
+      CL.ipiv = (int*)(wb + c.tipiv);
+      CL.info = (int*)(wb + c.tinfo);
+      P->steps.push_back([plan, CL, jobs_meta](cudaStream_t st, long long& nl, StageProf& pf) {
+        ConvLaunch cl = CL;
+        cl.jobs = (ConvJob*)((char*)plan->meta.p + jobs_meta);
+        cudaError_t err = conv_matrices(cl, st, &nl);
+        pf.mark(st, kStConvGather);
+        return err;
+      });
+      // E = fe33^-1: LU in place, then solve against the identity
+      std::vector<cplx*> f33(nconv), einv(nconv);
+      for (int j = 0; j < nconv; ++j) { f33[j] = W_(c.fe33) + NN * j; einv[j] = W_(c.Einv) + NN * j; }
+      const size_t o33 = meta.add_vec(f33), oE = meta.add_vec(einv);
+      int* cipiv = (int*)(wb + c.cipiv);
+      int* cinfo = (int*)(wb + c.cinfo);
+      P->steps.push_back([plan, o33, oE, N, nconv, cipiv, cinfo](cudaStream_t st, long long& nl, StageProf& pf) {
+        cplx* const* a = (cplx* const*)((char*)plan->meta.p + o33);
+        cplx* const* b = (cplx* const*)((char*)plan->meta.p + oE);
+        cudaError_t err;
+        if ((err = zgetrf_batched(a, N, N, cipiv, cinfo, nconv, st)) != cudaSuccess) return err;
+        if ((err = zset_identity_batched(b, N, N, nconv, st)) != cudaSuccess) return err;
+        nl += 3;
+        err = zgetrs_batched(a, N, N, cipiv, b, N, N, nconv, st);
+        pf.mark(st, kStConvInverse);
+        return err;
+      });
+    }
+
+    // ---------------- modes of the patterned layers
+    if (nj > 0) {
+      std::vector<const cplx*> gA(2 * nj), gB(2 * nj), gS(2 * nj);
+      std::vector<cplx*> gD(2 * nj);
+      std::vector<LayerItem> items(nj);
+      std::vector<cplx*> Mp(nj), Wp(nj);
+      std::vector<int> jpoint(nj);
+      for (int j = 0; j < nj; ++j) {
+        const int lp = c.job_point[j], p = c.points[lp], s = pts[p].stack, l = c.job_layer[j];
+        const int cj = c.conv_index.at({s, l});
+        const cplx* ab = (const cplx*)(inb + ab_off[p]);
+        gA[j] = W_(c.Einv) + NN * cj;
+        gB[j] = W_(c.fe11) + NN * cj;
+        gS[j] = ab;
+        gD[j] = W_(c.X1) + NN * j;
+        gA[nj + j] = W_(c.Einv) + NN * cj;
+        gB[nj + j] = W_(c.fe22) + NN * cj;
+        gS[nj + j] = ab + N;
+        gD[nj + j] = W_(c.X2) + NN * j;
+        LayerItem& it = items[j];
+        it.fe11 = W_(c.fe11) + NN * cj;
+        it.fe22 = W_(c.fe22) + NN * cj;
+        it.X1 = W_(c.X1) + NN * j;
+        it.X2 = W_(c.X2) + NN * j;
+        it.ab = ab;
+        it.M = W_(c.M) + nn * j;
+        it.W = W_(c.W) + nn * j;
+        it.V = W_(c.V) + nn * j;
+        it.mu = W_(c.mu) + (size_t)n * j;
+        it.gamma = W_(c.gam) + (size_t)n * j;
+        it.k0 = 2 * kPi / pts[p].lambda;
+        it.point = p;
+        Mp[j] = it.M;
+        Wp[j] = it.W;
+        jpoint[j] = p;
+      }
+      const size_t oA = meta.add_vec(gA), oB = meta.add_vec(gB), oS = meta.add_vec(gS), oD = meta.add_vec(gD);
+      const size_t oItems = meta.add_vec(items), oM = meta.add_vec(Mp), oW = meta.add_vec(Wp);
+      const size_t oJP = meta.add_vec(jpoint);
+      // V GEMMs: top = fe22 * Wb, bottom = fe11 * Wt
+      std::vector<const cplx*> vA(2 * nj), vB(2 * nj);
+      std::vector<cplx*> vD(2 * nj);
+      for (int j = 0; j < nj; ++j) {
+        vA[j] = items[j].fe22;
+        vB[j] = items[j].W + (size_t)N * n;
+        vD[j] = items[j].V;
+        vA[nj + j] = items[j].fe11;
+        vB[nj + j] = items[j].W;
+        vD[nj + j] = items[j].V + (size_t)N * n;
+      }
+      const size_t ovA = meta.add_vec(vA), ovB = meta.add_vec(vB), ovD = meta.add_vec(vD);
+      cplx* mu = W_(c.mu);
+      void* eigw = wb + c.eigw;
+      int* einfo = (int*)(wb + c.einfo);
+      int* status = P->dStatus;
+      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+        char* m = (char*)plan->meta.p;
+        GemmArgs g{};
+        g.A = (const cplx* const*)(m + oA);
+        g.B = (const cplx* const*)(m + oB);
+        g.C = nullptr;
+        g.D = (cplx* const*)(m + oD);
+        g.s = (const cplx* const*)(m + oS);
+        g.M = N; g.N = N; g.K = N;
+        g.lda = N; g.ldb = N; g.ldc = N; g.ldd = N;
+        g.alpha = mkc(1, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
+        g.batch = 2 * nj;
+        cudaError_t err;
+        if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+        pf.mark(st, kStPQGemm);
+        const LayerItem* it = (const LayerItem*)(m + oItems);
+        if ((err = assemble_m(it, nj, N, st)) != cudaSuccess) return err;
+        pf.mark(st, kStAssemble);
+        if ((err = zgeev_batched((cplx* const*)(m + oM), n, n, mu, (cplx* const*)(m + oW), n, eigw, einfo, nj, st,
+                                 &pf)) != cudaSuccess)
+          return err;
+        if ((err = fold_info(einfo, (const int*)(m + oJP), nj, 0, status, st)) != cudaSuccess) return err;
+        GemmArgs v{};
+        v.A = (const cplx* const*)(m + ovA);
+        v.B = (const cplx* const*)(m + ovB);
+        v.D = (cplx* const*)(m + ovD);
+        v.M = N; v.N = n; v.K = N;
+        v.lda = N; v.ldb = n; v.ldc = n; v.ldd = n;
+        v.alpha = mkc(1, 0); v.beta = mkc(0, 0); v.gammaI = mkc(0, 0);
+        v.batch = 2 * nj;
+        if ((err = zgemm_batched(v, st)) != cudaSuccess) return err;
+        nl += 10;
+        err = finish_modes(it, nj, N, status, st);
+        pf.mark(st, kStModes);
+        return err;
+      });
+    }
+
+    // ---------------- half-spaces
+    {
+      std::vector<HalfItem> hs(2 * np);
+      for (int lp = 0; lp < np; ++lp) {
+        const int p = c.points[lp], s = pts[p].stack;
+        const size_t cells = (size_t)(si[s].ncx - 1) * (si[s].ncy - 1);
+        for (int side = 0; side < 2; ++side) {
+          HalfItem& h = hs[2 * lp + side];
+          h.ab = (const cplx*)(inb + ab_off[p]);
+          h.eps = si[s].eps[(side == 0 ? 0 : (size_t)(si[s].L - 1)) * cells];
+          h.k0 = 2 * kPi / pts[p].lambda;
+          h.W = W_(side == 0 ? c.hW0 : c.hWL) + nn * lp;
+          h.V = W_(side == 0 ? c.hV0 : c.hVL) + nn * lp;
+          h.gamma = W_(side == 0 ? c.hg0 : c.hgL) + (size_t)n * lp;
+          h.point = p;
+        }
+      }
+      const size_t oh = meta.add_vec(hs);
+      int* status = P->dStatus;
+      const int cnt = 2 * np;
+      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+        nl += 1;
+        cudaError_t err = halfspace_modes((const HalfItem*)((char*)plan->meta.p + oh), cnt, N, status, st);
+        pf.mark(st, kStHalfspace);
+        return err;
+      });
+    }
+
+    // ---------------- cascade
+    {
+      std::vector<cplx*> rud(np), tdd(np), gbuf(np);
+      for (int lp = 0; lp < np; ++lp) {
+        rud[lp] = W_(c.Rud) + nn * lp;
+        tdd[lp] = W_(c.Tdd) + nn * lp;
+        gbuf[lp] = W_(c.G) + nn * lp;
+      }
+      const size_t oR0 = meta.add_vec(rud), oT0 = meta.add_vec(tdd);
+      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+        nl += 1;
+        cudaError_t err = cascade_init((cplx* const*)((char*)plan->meta.p + oR0),
+                                       (cplx* const*)((char*)plan->meta.p + oT0), n, np, st);
+        pf.mark(st, kStPhase);
+        return err;
+      });
+      // layer buffers of point lp, layer l
+      auto layerW = [&](int lp, int l) -> cplx* {
+        const int p = c.points[lp];
+        const int L = si[pts[p].stack].L;
+        if (l == 0) return W_(c.hW0) + nn * lp;
+        if (l == L - 1) return W_(c.hWL) + nn * lp;
+        for (size_t j = 0; j < c.job_point.size(); ++j)
+          if (c.job_point[j] == lp && c.job_layer[j] == l) return W_(c.W) + nn * j;
+        return nullptr;
+      };
+      auto layerV = [&](int lp, int l) -> cplx* {
+        const int p = c.points[lp];
+        const int L = si[pts[p].stack].L;
+        if (l == 0) return W_(c.hV0) + nn * lp;
+        if (l == L - 1) return W_(c.hVL) + nn * lp;
+        for (size_t j = 0; j < c.job_point.size(); ++j)
+          if (c.job_point[j] == lp && c.job_layer[j] == l) return W_(c.V) + nn * j;
+        return nullptr;
+      };
+      auto layerG = [&](int lp, int l) -> cplx* {
+        for (size_t j = 0; j < c.job_point.size(); ++j)
+          if (c.job_point[j] == lp && c.job_layer[j] == l) return W_(c.gam) + (size_t)n * j;
+        return nullptr;
+      };
+      int maxL = 0;
+      for (int lp = 0; lp < np; ++lp) maxL = std::max(maxL, si[pts[c.points[lp]].stack].L);
+      for (int step = 0; step + 1 < maxL; ++step) {
+        std::vector<int> part;
+        for (int lp = 0; lp < np; ++lp)
+          if (si[pts[c.points[lp]].stack].L - 1 > step) part.push_back(lp);
+        const int k = (int)part.size();
+        if (k == 0) continue;
+        std::vector<const cplx*> csrc(4 * k);
+        std::vector<cplx*> cdst(4 * k), lu(2 * k), rhs(2 * k);
+        std::vector<PhaseItem> ph;
+        std::vector<const cplx*> fA(k), fB(k), fC(k), gA(k), gB(k), gC(k), sF(k), sG(k), tG(k), tT(k), tTau(k);
+        std::vector<cplx*> fD(k), gD(k), sD(k), tauD(k), rD(k), tD(k), Sp(k);
+        std::vector<int> ipoint(2 * k), spoint(k);
+        for (int q = 0; q < k; ++q) {
+          const int lp = part[q], p = c.points[lp];
+          const int L = si[pts[p].stack].L;
+          const int index = L - 1 - step, a = index - 1, b = index;
+          cplx* IE = W_(c.IE) + nn * lp;
+          cplx* IH = W_(c.IH) + nn * lp;
+          cplx* WLU = W_(c.WLU) + nn * lp;
+          cplx* VLU = W_(c.VLU) + nn * lp;
+          csrc[q] = layerW(lp, a); cdst[q] = WLU;
+          csrc[k + q] = layerV(lp, a); cdst[k + q] = VLU;
+          csrc[2 * k + q] = layerW(lp, b); cdst[2 * k + q] = IE;
+          csrc[3 * k + q] = layerV(lp, b); cdst[3 * k + q] = IH;
+          lu[q] = WLU; lu[k + q] = VLU;
+          rhs[q] = IE; rhs[k + q] = IH;
+          ipoint[q] = p; ipoint[k + q] = p;
+          spoint[q] = p;
+          if (step > 0) {
+            PhaseItem it;
+            it.Rud = rud[lp];
+            it.Tdd = tdd[lp];
+            it.gamma = layerG(lp, b);
+            it.thick = si[pts[p].stack].thick[b];
+            ph.push_back(it);
+          }
+          cplx* F = W_(c.F) + nn * lp;
+          fA[q] = IE; fB[q] = rud[lp]; fC[q] = IE; fD[q] = F;
+          gA[q] = IH; gB[q] = rud[lp]; gC[q] = IH; gD[q] = gbuf[lp];
+          sF[q] = F; sG[q] = gbuf[lp]; sD[q] = F; Sp[q] = F;
+          cplx* tau = W_(c.tau) + nn * lp;
+          tauD[q] = tau;
+          // Rud = -2 G tau + I ; Tnew = 2 Tdd tau -> into the G buffer, then swap
+          tG[q] = gbuf[lp]; tTau[q] = tau; rD[q] = rud[lp];
+          tT[q] = tdd[lp]; tD[q] = gbuf[lp];
+          std::swap(tdd[lp], gbuf[lp]);
+        }
+        const size_t ocs = meta.add_vec(csrc), ocd = meta.add_vec(cdst), olu = meta.add_vec(lu), orhs = meta.add_vec(rhs);
+        const size_t oip = meta.add_vec(ipoint), osp = meta.add_vec(spoint);
+        const size_t oph = meta.add_vec(ph);
+        const int nph = (int)ph.size();
+        const size_t ofA = meta.add_vec(fA), ofB = meta.add_vec(fB), ofC = meta.add_vec(fC), ofD = meta.add_vec(fD);
+        const size_t ogA = meta.add_vec(gA), ogB = meta.add_vec(gB), ogC = meta.add_vec(gC), ogD = meta.add_vec(gD);
+        const size_t osF = meta.add_vec(sF), osG = meta.add_vec(sG), osD = meta.add_vec(sD), oSp = meta.add_vec(Sp);
+        const size_t otau = meta.add_vec(tauD), otG = meta.add_vec(tG), otTau = meta.add_vec(tTau), orD = meta.add_vec(rD);
+        const size_t otT = meta.add_vec(tT), otD = meta.add_vec(tD);
+        int* pipiv = (int*)(wb + c.pipiv);
+        int* pinfo = (int*)(wb + c.pinfo);
+        int* status = P->dStatus;
+        P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+          char* m = (char*)plan->meta.p;
+          auto cpa = [m](size_t o) { return (const cplx* const*)(m + o); };
+          auto pa = [m](size_t o) { return (cplx* const*)(m + o); };
+          cudaError_t err;
+          // interface matrices IE = Wa^-1 Wb, IH = Va^-1 Vb (rcwa/RCWASolver.cpp:537-543)
+          if ((err = zcopy_batched(cpa(ocs), n, pa(ocd), n, n, n, 4 * k, st)) != cudaSuccess) return err;
+          if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * k, st)) != cudaSuccess) return err;
+          if ((err = fold_info(pinfo, (const int*)(m + oip), 2 * k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
+            return err;
+          if ((err = zgetrs_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * k, st)) != cudaSuccess) return err;
+          pf.mark(st, kStInterface);
+          nl += 4;
+          if (nph > 0) {
+            if ((err = apply_phase((const PhaseItem*)(m + oph), nph, n, st)) != cudaSuccess) return err;
+            pf.mark(st, kStPhase);
+            nl += 1;
+          }
+          GemmArgs g{};
+          g.M = n; g.N = n; g.K = n;
+          g.lda = n; g.ldb = n; g.ldc = n; g.ldd = n;
+          g.batch = k;
+          g.gammaI = mkc(0, 0);
+          // F = IE + IE waveRud ; G = IH - IH waveRud   (:440-443)
+          g.A = cpa(ofA); g.B = cpa(ofB); g.C = cpa(ofC); g.D = pa(ofD);
+          g.alpha = mkc(1, 0); g.beta = mkc(1, 0);
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          g.A = cpa(ogA); g.B = cpa(ogB); g.C = cpa(ogC); g.D = pa(ogD);
+          g.alpha = mkc(-1, 0); g.beta = mkc(1, 0);
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          pf.mark(st, kStCascadeGemm);
+          // tau = (F + G)^-1  (:451-453)
+          if ((err = zaxpby_batched(cpa(osF), cpa(osG), pa(osD), mkc(1, 0), mkc(1, 0), n, k, st)) != cudaSuccess)
+            return err;
+          if ((err = zgetrf_batched(pa(oSp), n, n, pipiv, pinfo, k, st)) != cudaSuccess) return err;
+          if ((err = fold_info(pinfo, (const int*)(m + osp), k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
+            return err;
+          if ((err = zset_identity_batched(pa(otau), n, n, k, st)) != cudaSuccess) return err;
+          if ((err = zgetrs_batched(cpa(oSp), n, n, pipiv, pa(otau), n, n, k, st)) != cudaSuccess) return err;
+          pf.mark(st, kStTau);
+          // Rud = I - 2 G tau ; Tdd = 2 waveTdd tau  (:457-460)
+          g.A = cpa(otG); g.B = cpa(otTau); g.C = nullptr; g.D = pa(orD);
+          g.alpha = mkc(-2, 0); g.beta = mkc(0, 0); g.gammaI = mkc(1, 0);
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          g.A = cpa(otT); g.B = cpa(otTau); g.C = nullptr; g.D = pa(otD);
+          g.alpha = mkc(2, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
+          nl += 9;
+          err = zgemm_batched(g, st);
+          pf.mark(st, kStCascadeGemm);
+          return err;
+        });
+      }
+      // ---------------- scatter
+      std::vector<ScatterItem> sc;
+      for (int lp = 0; lp < np; ++lp) {
+        const int p = c.points[lp], s = pts[p].stack;
+        const size_t cells = (size_t)(si[s].ncx - 1) * (si[s].ncy - 1);
+        for (int x = 0; x < n_exc; ++x) {
+          ScatterItem it;
+          it.Rud = rud[lp];
+          it.Tdd = tdd[lp];
+          it.ab = (const cplx*)(inb + ab_off[p]);
+          it.eps_ref = si[s].eps[0];
+          it.eps_trn = si[s].eps[(size_t)(si[s].L - 1) * cells];
+          it.k0 = 2 * kPi / pts[p].lambda;
+          const rcwa_cplx px = pxy[((size_t)p * n_exc + x) * 2], py = pxy[((size_t)p * n_exc + x) * 2 + 1];
+          it.px = mkc(px.re, px.im);
+          it.py = mkc(py.re, py.im);
+          it.ref = P->dRef + P->order_offset[p] + (size_t)x * N;
+          it.trn = P->dTrn + P->order_offset[p] + (size_t)x * N;
+          it.R = P->dR + (size_t)p * n_exc + x;
+          it.T = P->dT + (size_t)p * n_exc + x;
+          it.point = p;
+          sc.push_back(it);
+        }
+      }
+      const size_t osc = meta.add_vec(sc);
+      const int nsc = (int)sc.size();
+      int* status = P->dStatus;
+      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+        nl += 1;
+        cudaError_t err = scatter_efficiencies((const ScatterItem*)((char*)plan->meta.p + osc), nsc, N, nx, ny, status,
+                                               st);
+        pf.mark(st, kStScatter);
+        return err;
+      });
+    }
+  }
+  if (cudaMalloc(&P->meta.p, std::max<size_t>(meta.bytes.size(), 16)) != cudaSuccess)
+    return fail(e, RCWA_ERR_NOMEM, "metadata allocation failed");
+  P->meta.bytes = meta.bytes.size();
+  if (!meta.bytes.empty() &&
+      cudaMemcpy(P->meta.p, meta.bytes.data(), meta.bytes.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+    return fail(e, RCWA_ERR_CUDA, "metadata upload failed");
+  *out = P.release();
+  return RCWA_OK;
+}
+
+extern "C" int rcwa_plan_execute(rcwa_plan* p, void* stream) {
+  if (!p) return RCWA_ERR_INVALID;
+  cudaStream_t st = stream ? (cudaStream_t)stream : p->e->stream;
+  if (cudaSetDevice(p->e->device) != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, "cudaSetDevice failed");
+  long long nl = 0;
+  cudaError_t err = cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st);
+  p->prof->begin(st);
+  for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, nl, *p->prof);
+  p->launches = nl;
+  if (err != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, std::string("launch failed: ") + cudaGetErrorString(err));
+  return RCWA_OK;
+}
+
+extern "C" long long rcwa_plan_launch_count(const rcwa_plan* p) { return p ? p->launches : 0; }
+
+extern "C" int rcwa_plan_set_profiling(rcwa_plan* p, int on) {
+  if (!p) return RCWA_ERR_INVALID;
+  p->prof->on = on != 0;
+  return RCWA_OK;
+}
+
+extern "C" int rcwa_plan_stage_times(rcwa_plan* p, double* ms, int max_stages) {
+  if (!p || !ms) return RCWA_ERR_INVALID;
+  // the events were recorded on whichever stream executed the plan
+  if (p->prof->used > 0 && cudaEventSynchronize(p->prof->ev[p->prof->used - 1]) != cudaSuccess) return RCWA_ERR_CUDA;
+  double t[kStCount];
+  p->prof->collect(t);
+  for (int i = 0; i < max_stages; ++i) ms[i] = i < kStCount ? t[i] : 0.0;
+  return kStCount;
+}
+
+extern "C" const char* rcwa_stage_name(int stage) {
+  static const char* names[kStCount] = {"conv_tables", "conv_gather", "conv_inverse", "pq_gemm", "assemble_pq",
+                                        "hessenberg", "schur_qr", "trevc", "eig_backtransform", "eig_normalize",
+                                        "modes_v", "halfspace", "interface_lu_solve", "phase", "cascade_gemm",
+                                        "tau_inverse", "scatter"};
+  return (stage >= 0 && stage < kStCount) ? names[stage] : "";
+}
+
+extern "C" int rcwa_plan_results(rcwa_plan* p, double* R, double* T, double* ref_orders, double* trn_orders,
+                                 int* status) {
+  if (!p) return RCWA_ERR_INVALID;
+  if (cudaDeviceSynchronize() != cudaSuccess)
+    return fail(p->e, RCWA_ERR_CUDA, std::string("execution failed: ") + cudaGetErrorString(cudaGetLastError()));
+  const size_t ne = (size_t)p->n_pts * p->n_exc;
+  if (R && cudaMemcpy(R, p->dR, sizeof(double) * ne, cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
+  if (T && cudaMemcpy(T, p->dT, sizeof(double) * ne, cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
+  if (ref_orders &&
+      cudaMemcpy(ref_orders, p->dRef, sizeof(double) * p->total_orders, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return RCWA_ERR_CUDA;
+  if (trn_orders &&
+      cudaMemcpy(trn_orders, p->dTrn, sizeof(double) * p->total_orders, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return RCWA_ERR_CUDA;
+  std::vector<int> hs(p->n_pts);
+  if (cudaMemcpy(hs.data(), p->dStatus, sizeof(int) * p->n_pts, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return RCWA_ERR_CUDA;
+  if (status) std::memcpy(status, hs.data(), sizeof(int) * p->n_pts);
+  for (int v : hs)
+    if (v) return v;
+  return RCWA_OK;
+}
+
+extern "C" void rcwa_plan_destroy(rcwa_plan* p) {
+  if (!p) return;
+  cudaSetDevice(p->e->device);
+  delete p;
+}
+
+extern "C" int rcwa_engine_solve_batch(rcwa_engine* e, const rcwa_stack* stacks, int n_stacks, const rcwa_point* pts,
+                                       int n_pts, int n_exc, const rcwa_cplx* pxy, int precision, double* R,
+                                       double* T, double* ref_orders, double* trn_orders, int* status) {
+  rcwa_plan* p = nullptr;
+  int rc = rcwa_plan_create(e, stacks, n_stacks, pts, n_pts, n_exc, pxy, precision, &p);
+  if (rc) return rc;
+  rc = rcwa_plan_execute(p, nullptr);
+  if (rc == RCWA_OK) rc = rcwa_plan_results(p, R, T, ref_orders, trn_orders, status);
+  rcwa_plan_destroy(p);
+  return rc;
+}

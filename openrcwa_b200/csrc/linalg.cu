@@ -1,0 +1,277 @@
+// Batched complex-FP64 GEMM, LU (getrf) and LU solve (getrs).
+//
+// GEMM: 64x64 output tiles, 256 threads, every thread owns a 4x4 block of
+// complex accumulators in registers; operand tiles are staged in shared memory
+// (K-slab of 16).  The same tile routine drives the trailing updates of the
+// one-CTA-per-matrix blocked LU and of the blocked triangular solves, so the
+// O(n^3) part of every factorisation runs as register-blocked FP64 FMAs.
+#include "linalg.cuh"
+#include "tile.cuh"
+
+namespace {
+
+__global__ void __launch_bounds__(kTileThreads) zgemm_kernel(GemmArgs g) {
+  __shared__ TileSmem sm;
+  const int b = blockIdx.z;
+  const cplx* A = g.A ? g.A[b] : g.A0 + b * g.sA;
+  const cplx* B = g.B ? g.B[b] : g.B0 + b * g.sB;
+  const cplx* s = g.s ? g.s[b] : nullptr;
+  const int m0 = blockIdx.y * kTBM, n0 = blockIdx.x * kTBN;
+  cplx acc[4][4];
+  tile_zero(acc);
+  if (g.transA) {
+    if (g.transB) tile_mma<true, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
+    else tile_mma<true, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
+  } else {
+    if (g.transB) tile_mma<false, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
+    else tile_mma<false, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
+  }
+  const cplx* C = (g.beta.x != 0.0 || g.beta.y != 0.0) ? g.C[b] : nullptr;
+  tile_store(acc, g.D ? g.D[b] : g.D0 + b * g.sD, g.ldd, C, g.ldc, g.alpha, g.beta, g.gammaI, g.M, g.N, m0, n0);
+}
+
+// One CTA per matrix: right-looking blocked LU with partial pivoting, panel
+// width 32.  Panel columns are factorised in global memory (L1/L2 resident),
+// the U12 block row by a shared-memory triangular solve, and the trailing
+// matrix by the register-blocked tile GEMM.
+__global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr, int n, int lda,
+                                                             int* ipiv_all, int* info_all) {
+  // the triangular block and the GEMM slabs are used in separate phases
+  __shared__ __align__(16) unsigned char smem_raw[sizeof(TileSmem)];
+  TileSmem& sm = *reinterpret_cast<TileSmem*>(smem_raw);
+  cplx (*Lsm)[33] = reinterpret_cast<cplx (*)[33]>(smem_raw);
+  __shared__ double red_v[kTileThreads / 32];
+  __shared__ int red_i[kTileThreads / 32];
+  __shared__ int s_piv;
+  const int tid = threadIdx.x;
+  const int b = blockIdx.x;
+  cplx* A = Aarr[b];
+  int* ipiv = ipiv_all + (size_t)b * n;
+  int info = 0;
+  for (int kb = 0; kb < n; kb += 32) {
+    const int jb = min(32, n - kb);
+    for (int j = kb; j < kb + jb; ++j) {
+      // pivot: largest |re|+|im| in column j, rows j..n-1 (first index on ties)
+      double best = -1.0;
+      int bi = j;
+      for (int i = j + tid; i < n; i += kTileThreads) {
+        double v = cabs1(A[(size_t)i * lda + j]);
+        if (v > best) { best = v; bi = i; }
+      }
+      for (int off = 16; off > 0; off >>= 1) {
+        double ov = __shfl_down_sync(0xffffffffu, best, off);
+        int oi = __shfl_down_sync(0xffffffffu, bi, off);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+      }
+      if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
+      __syncthreads();
+      if (tid == 0) {
+        double bv = red_v[0];
+        int bix = red_i[0];
+        for (int w = 1; w < kTileThreads / 32; ++w)
+          if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bix)) { bv = red_v[w]; bix = red_i[w]; }
+        s_piv = bix;
+        ipiv[j] = bix;
+      }
+      __syncthreads();
+      const int p = s_piv;
+      if (p != j) {
+        for (int c = tid; c < n; c += kTileThreads) {
+          cplx t = A[(size_t)j * lda + c];
+          A[(size_t)j * lda + c] = A[(size_t)p * lda + c];
+          A[(size_t)p * lda + c] = t;
+        }
+      }
+      __syncthreads();
+      const cplx piv = A[(size_t)j * lda + j];
+      if (piv.x == 0.0 && piv.y == 0.0) {
+        if (info == 0) info = j + 1;
+      } else {
+        const cplx inv = cdiv(mkc(1.0, 0.0), piv);
+        for (int i = j + 1 + tid; i < n; i += kTileThreads)
+          A[(size_t)i * lda + j] = cmul(A[(size_t)i * lda + j], inv);
+      }
+      __syncthreads();
+      const int w = kb + jb - j - 1;
+      if (w > 0) {
+        const int rows = n - j - 1;
+        for (int idx = tid; idx < rows * w; idx += kTileThreads) {
+          const int i = j + 1 + idx / w, c = j + 1 + idx % w;
+          A[(size_t)i * lda + c] =
+              cfma(cneg(A[(size_t)i * lda + j]), A[(size_t)j * lda + c], A[(size_t)i * lda + c]);
+        }
+      }
+      __syncthreads();
+    }
+    if (kb + jb < n) {
+      // U12 = L11^-1 A12 (L11 unit lower, staged in shared memory); the
+      // panel's row interchanges were applied to whole rows above.
+      for (int idx = tid; idx < jb * jb; idx += kTileThreads) {
+        const int r = idx / jb, q = idx % jb;
+        Lsm[r][q] = A[(size_t)(kb + r) * lda + kb + q];
+      }
+      __syncthreads();
+      for (int c = kb + jb + tid; c < n; c += kTileThreads) {
+        for (int r = 1; r < jb; ++r) {
+          cplx x = A[(size_t)(kb + r) * lda + c];
+          for (int q = 0; q < r; ++q) x = cfma(cneg(Lsm[r][q]), A[(size_t)(kb + q) * lda + c], x);
+          A[(size_t)(kb + r) * lda + c] = x;
+        }
+      }
+      __syncthreads();
+      const int m2 = n - kb - jb;
+      const int tiles_m = (m2 + kTBM - 1) / kTBM, tiles_n = (m2 + kTBN - 1) / kTBN;
+      const cplx* L21 = A + (size_t)(kb + jb) * lda + kb;
+      const cplx* U12 = A + (size_t)kb * lda + kb + jb;
+      cplx* A22 = A + (size_t)(kb + jb) * lda + kb + jb;
+      for (int t = 0; t < tiles_m * tiles_n; ++t) {
+        const int tm = (t / tiles_n) * kTBM, tn = (t % tiles_n) * kTBN;
+        cplx acc[4][4];
+        tile_zero(acc);
+        tile_mma<false, false>(sm, acc, L21, lda, U12, lda, nullptr, m2, m2, jb, tm, tn);
+        tile_store(acc, A22, lda, A22, lda, mkc(-1.0, 0.0), mkc(1.0, 0.0), mkc(0.0, 0.0), m2, m2, tm, tn);
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) info_all[b] = info;
+}
+
+// Blocked LU solve: one CTA per (matrix, 64-column block of B).
+__global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const* LUarr, int n, int lda,
+                                                             const int* ipiv_all, cplx* const* Barr,
+                                                             int nrhs, int ldb) {
+  __shared__ __align__(16) unsigned char smem_raw[sizeof(TileSmem)];
+  TileSmem& sm = *reinterpret_cast<TileSmem*>(smem_raw);
+  cplx (*Tsm)[33] = reinterpret_cast<cplx (*)[33]>(smem_raw);
+  const int tid = threadIdx.x;
+  const int b = blockIdx.y;
+  const int c0 = blockIdx.x * 64;
+  const int cw = min(64, nrhs - c0);
+  const cplx* LU = LUarr[b];
+  const int* ipiv = ipiv_all + (size_t)b * n;
+  cplx* B = Barr[b] + c0;
+  if (tid < cw) {
+    for (int j = 0; j < n; ++j) {
+      const int p = ipiv[j];
+      if (p != j) {
+        cplx t = B[(size_t)j * ldb + tid];
+        B[(size_t)j * ldb + tid] = B[(size_t)p * ldb + tid];
+        B[(size_t)p * ldb + tid] = t;
+      }
+    }
+  }
+  __syncthreads();
+  // forward substitution with the unit lower factor
+  for (int rb = 0; rb < n; rb += 32) {
+    const int rw = min(32, n - rb);
+    for (int idx = tid; idx < rw * rw; idx += kTileThreads)
+      Tsm[idx / rw][idx % rw] = LU[(size_t)(rb + idx / rw) * lda + rb + idx % rw];
+    __syncthreads();
+    if (tid < cw) {
+      for (int r = 1; r < rw; ++r) {
+        cplx x = B[(size_t)(rb + r) * ldb + tid];
+        for (int q = 0; q < r; ++q) x = cfma(cneg(Tsm[r][q]), B[(size_t)(rb + q) * ldb + tid], x);
+        B[(size_t)(rb + r) * ldb + tid] = x;
+      }
+    }
+    __syncthreads();
+    const int m2 = n - rb - rw;
+    if (m2 > 0) {
+      const cplx* L21 = LU + (size_t)(rb + rw) * lda + rb;
+      const cplx* X = B + (size_t)rb * ldb;
+      cplx* B2 = B + (size_t)(rb + rw) * ldb;
+      for (int tm = 0; tm < m2; tm += kTBM) {
+        cplx acc[4][4];
+        tile_zero(acc);
+        tile_mma<false, false>(sm, acc, L21, lda, X, ldb, nullptr, m2, cw, rw, tm, 0);
+        tile_store(acc, B2, ldb, B2, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0), mkc(0.0, 0.0), m2, cw, tm, 0);
+      }
+    }
+    __syncthreads();
+  }
+  // back substitution with the upper factor
+  for (int rb = ((n - 1) / 32) * 32; rb >= 0; rb -= 32) {
+    const int rw = min(32, n - rb);
+    for (int idx = tid; idx < rw * rw; idx += kTileThreads)
+      Tsm[idx / rw][idx % rw] = LU[(size_t)(rb + idx / rw) * lda + rb + idx % rw];
+    __syncthreads();
+    if (tid < cw) {
+      for (int r = rw - 1; r >= 0; --r) {
+        cplx x = B[(size_t)(rb + r) * ldb + tid];
+        for (int q = r + 1; q < rw; ++q) x = cfma(cneg(Tsm[r][q]), B[(size_t)(rb + q) * ldb + tid], x);
+        B[(size_t)(rb + r) * ldb + tid] = cdiv(x, Tsm[r][r]);
+      }
+    }
+    __syncthreads();
+    if (rb > 0) {
+      const cplx* U01 = LU + rb;
+      const cplx* X = B + (size_t)rb * ldb;
+      for (int tm = 0; tm < rb; tm += kTBM) {
+        cplx acc[4][4];
+        tile_zero(acc);
+        tile_mma<false, false>(sm, acc, U01, lda, X, ldb, nullptr, rb, cw, rw, tm, 0);
+        tile_store(acc, B, ldb, B, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0), mkc(0.0, 0.0), rb, cw, tm, 0);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void identity_kernel(cplx* const* Barr, int n, int ldb) {
+  cplx* B = Barr[blockIdx.y];
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)n * n;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / n), c = (int)(idx % n);
+    B[(size_t)r * ldb + c] = mkc(r == c ? 1.0 : 0.0, 0.0);
+  }
+}
+
+__global__ void copy_kernel(const cplx* const* S, int lds, cplx* const* Dd, int ldd, int rows, int cols) {
+  const cplx* s = S[blockIdx.y];
+  cplx* d = Dd[blockIdx.y];
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)rows * cols;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(idx / cols), c = (int)(idx % cols);
+    d[(size_t)r * ldd + c] = s[(size_t)r * lds + c];
+  }
+}
+
+}  // namespace
+
+cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st) {
+  if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
+  dim3 grid((g.N + kTBN - 1) / kTBN, (g.M + kTBM - 1) / kTBM, g.batch);
+  zgemm_kernel<<<grid, kTileThreads, 0, st>>>(g);
+  return cudaGetLastError();
+}
+
+cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
+                           cudaStream_t st) {
+  if (batch <= 0 || n <= 0) return cudaSuccess;
+  zgetrf_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, ipiv, info);
+  return cudaGetLastError();
+}
+
+cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipiv, cplx* const* B,
+                           int nrhs, int ldb, int batch, cudaStream_t st) {
+  if (batch <= 0 || n <= 0 || nrhs <= 0) return cudaSuccess;
+  dim3 grid((nrhs + 63) / 64, batch);
+  zgetrs_kernel<<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, B, nrhs, ldb);
+  return cudaGetLastError();
+}
+
+cudaError_t zset_identity_batched(cplx* const* B, int n, int ldb, int batch, cudaStream_t st) {
+  if (batch <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid(min(1024, (n * n + 255) / 256), batch);
+  identity_kernel<<<grid, 256, 0, st>>>(B, n, ldb);
+  return cudaGetLastError();
+}
+
+cudaError_t zcopy_batched(const cplx* const* src, int lds, cplx* const* dst, int ldd, int rows, int cols,
+                          int batch, cudaStream_t st) {
+  if (batch <= 0 || rows <= 0 || cols <= 0) return cudaSuccess;
+  dim3 grid(min(1024, (rows * cols + 255) / 256), batch);
+  copy_kernel<<<grid, 256, 0, st>>>(src, lds, dst, ldd, rows, cols);
+  return cudaGetLastError();
+}

@@ -1,0 +1,43 @@
+// Batched complex-FP64 dense linear algebra used by the RCWA engine.
+// Matrices are row-major double2 with a leading dimension; a batch is given
+// as a device array of per-item pointers so that items may live anywhere.
+#pragma once
+#include "common.cuh"
+
+struct GemmArgs {
+  const cplx* const* A;   // op(A) is M x K
+  const cplx* const* B;   // op(B) is K x N
+  const cplx* const* C;   // may be null when beta == 0
+  cplx* const* D;         // D = alpha*op(A)*diag(s)*op(B) + beta*C + gammaI*I
+  const cplx* const* s;   // optional diagonal between op(A) and op(B) (length K)
+  int M, N, K;
+  int lda, ldb, ldc, ldd;
+  int transA, transB;     // 0: as stored, 1: transposed
+  cplx alpha, beta, gammaI;
+  int batch;
+  // strided batches: used for an operand whose pointer array above is null
+  const cplx* A0 = nullptr;
+  const cplx* B0 = nullptr;
+  cplx* D0 = nullptr;
+  size_t sA = 0, sB = 0, sD = 0;
+};
+
+// D = alpha*op(A)*diag(s)*op(B) + beta*C + gammaI*I for every batch item.
+cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st);
+
+// In-place LU with partial pivoting (row interchanges, LAPACK getrf
+// convention, 0-based pivots) of square n x n matrices.  info[b] = 0, or k+1
+// when U(k,k) is exactly zero.
+cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
+                           cudaStream_t st);
+
+// Solve A X = B in place of B (n x nrhs) from the factors of zgetrf_batched.
+cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipiv,
+                           cplx* const* B, int nrhs, int ldb, int batch, cudaStream_t st);
+
+// B = I (n x n) for every batch item.
+cudaError_t zset_identity_batched(cplx* const* B, int n, int ldb, int batch, cudaStream_t st);
+
+// Copy src -> dst (rows x cols) for every batch item.
+cudaError_t zcopy_batched(const cplx* const* src, int lds, cplx* const* dst, int ldd, int rows,
+                          int cols, int batch, cudaStream_t st);

@@ -1,0 +1,66 @@
+// Element-wise and reduction kernels specific to the RCWA solve.
+#pragma once
+#include "common.cuh"
+
+// One patterned-layer job: the wave-equation matrix of one layer at one point.
+struct LayerItem {
+  const cplx* fe11;   // N x N  DiscontinuousX
+  const cplx* fe22;   // N x N  DiscontinuousY
+  const cplx* X1;     // N x N  E * diag(alpha) * fe11, E = fe33^-1
+  const cplx* X2;     // N x N  E * diag(beta)  * fe22
+  const cplx* ab;     // alpha[N] then beta[N] (complex, imaginary part 0)
+  cplx* M;            // n x n  (P*Q)/k0^2
+  cplx* W;            // n x n  eigenvectors (row-major)
+  cplx* V;            // n x n  on input rows [0,N) = fe22 Wb, rows [N,2N) = fe11 Wt
+  const cplx* mu;     // n eigenvalues of M
+  cplx* gamma;        // n  Layer::gamma()
+  double k0;
+  int point;
+};
+
+// Uniform half-space of one point.
+struct HalfItem {
+  const cplx* ab;
+  cplx eps;
+  double k0;
+  cplx* W;            // n x n  (identity)
+  cplx* V;            // n x n  Q*W/keff, 2x2 blocks per harmonic
+  cplx* gamma;        // n
+  int point;
+};
+
+struct PhaseItem {
+  cplx* Rud;
+  cplx* Tdd;
+  const cplx* gamma;
+  double thick;
+};
+
+struct ScatterItem {
+  const cplx* Rud;
+  const cplx* Tdd;
+  const cplx* ab;
+  cplx eps_ref, eps_trn;
+  double k0;
+  cplx px, py;
+  double* ref;        // N (device)
+  double* trn;        // N (device)
+  double* R;          // scalar (device)
+  double* T;
+  int point;
+};
+
+cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st);
+cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st);
+cudaError_t halfspace_modes(const HalfItem* items, int count, int N, int* status, cudaStream_t st);
+cudaError_t apply_phase(const PhaseItem* items, int count, int n, cudaStream_t st);
+cudaError_t scatter_efficiencies(const ScatterItem* items, int count, int N, int nx, int ny, int* status,
+                                 cudaStream_t st);
+// D = a*X + b*Y (n x n) for every item
+cudaError_t zaxpby_batched(const cplx* const* X, const cplx* const* Y, cplx* const* D, cplx a, cplx b, int n,
+                           int count, cudaStream_t st);
+// zero (n x n) the Rud and set Tdd = I
+cudaError_t cascade_init(cplx* const* Rud, cplx* const* Tdd, int n, int count, cudaStream_t st);
+// status[item_point[b]] <- code when info[b] != 0 (first error wins)
+cudaError_t fold_info(const int* info, const int* item_point, int count, int code_if_nonzero, int* status,
+                      cudaStream_t st);

@@ -1,0 +1,92 @@
+"""Seeded synthetic workloads with the shapes of the engine's benchmark configurations.
+
+Each builder returns (stacks, points, pxy) for Engine.solve_batch / Engine.plan:
+points rows are (stack index, wavelength, kx0, ky0) and pxy holds the TE and TM
+transverse polarisation vectors of each point (as sol/rcwa_bridge.cpp:187-196
+defines them).  Lengths are in metres.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .abi import Stack
+
+PI = 3.1415926535897932
+
+
+def pol_vectors(theta_deg, phi_deg):
+    th, ph = math.radians(theta_deg), math.radians(phi_deg)
+    if abs(math.sin(th)) < 1e-9:
+        return (0.0, 1.0), (1.0, 0.0)
+    return (-math.sin(ph), math.cos(ph)), (math.cos(th) * math.cos(ph), math.cos(th) * math.sin(ph))
+
+
+def _edges(period, fills):
+    e = sorted([0.0] + [f * period for f in fills if f < 1.0] + [period])
+    u = []
+    for v in e:
+        if not u or v - u[-1] > 1e-12 * period:
+            u.append(v)
+    return np.array(u)
+
+
+def rect_stack(nHx, nHy, px, py, layers, eps_sup=1.0, eps_sub=2.25):
+    """layers: list of (eps1, eps2, fill_x, fill_y, thickness); one eps1
+    rectangle [0, fx*px] x [0, fy*py] per layer on the merged edge grid."""
+    xe = _edges(px, [l[2] for l in layers])
+    ye = _edges(py, [l[3] for l in layers])
+    xc = 0.5 * (xe[1:] + xe[:-1])
+    yc = 0.5 * (ye[1:] + ye[:-1])
+    eps = [np.full((ye.size - 1, xe.size - 1), eps_sup, dtype=complex)]
+    for (e1, e2, fx, fy, _) in layers:
+        inside = (yc[:, None] < fy * py) & (xc[None, :] < fx * px)
+        eps.append(np.where(inside, e1, e2).astype(complex))
+    eps.append(np.full((ye.size - 1, xe.size - 1), eps_sub, dtype=complex))
+    thick = [0.0] + [l[4] for l in layers] + [0.0]
+    return Stack(nHx, nHy, xe, ye, np.array(eps), thick)
+
+
+def grating_1d(n_freq=16, nH=5):
+    """The 1D lamellar grating: period 300 nm, eps 4/1 fill 0.5, 200 nm, on
+    glass, normal incidence, n_freq frequencies 4.3e14-7.5e14 Hz."""
+    st = rect_stack(nH, 0, 3e-7, 3e-7, [(4.0, 1.0, 0.5, 1.0, 2e-7)])
+    freqs = np.linspace(4.3e14, 7.5e14, n_freq)
+    lam = 2.99792458e8 / freqs
+    pts = np.array([(0, l, 0.0, 0.0) for l in lam])
+    te, tm = pol_vectors(0.0, 0.0)
+    pxy = np.array([[te, tm]] * len(lam), dtype=complex)
+    return [st], pts, pxy
+
+
+def pillars_2d(seed=0, nH=10, n_lambda=256, n_angle=8, n_layers=5):
+    """2D rectangular-pillar grating: Nx=Ny=nH, period 400 x 400 nm, n_layers
+    patterned layers with fills ~U(0.2, 0.8), thickness ~U(50, 300) nm,
+    eps1 = U(2, 12) + i U(0, 0.5), eps2 = 1, superstrate 1, substrate 2.25;
+    n_lambda wavelengths 400-800 nm x n_angle (theta ~ U(0, 60), phi ~ U(0, 90))
+    conical incidences.  Points are ordered angle-major within each wavelength."""
+    rng = np.random.default_rng(seed)
+    layers = []
+    for _ in range(n_layers):
+        fx, fy = rng.uniform(0.2, 0.8, 2)
+        d = rng.uniform(50e-9, 300e-9)
+        e1 = complex(rng.uniform(2, 12), rng.uniform(0, 0.5))
+        layers.append((e1, 1.0, fx, fy, d))
+    st = rect_stack(nH, nH, 4e-7, 4e-7, layers)
+    th = rng.uniform(0, 60, n_angle)
+    ph = rng.uniform(0, 90, n_angle)
+    lam = np.linspace(400e-9, 800e-9, n_lambda)
+    pts, pxy = [], []
+    for l in lam:
+        k0 = 2 * PI / l
+        for a in range(n_angle):
+            t, p = math.radians(th[a]), math.radians(ph[a])
+            pts.append((0, l, k0 * math.sin(t) * math.cos(p), k0 * math.sin(t) * math.sin(p)))
+            pxy.append(pol_vectors(th[a], ph[a]))
+    return [st], np.array(pts), np.array(pxy, dtype=complex)
+
+
+def batch_slice(points, pxy, start, count):
+    idx = (np.arange(count) + start) % len(points)
+    return points[idx], pxy[idx]
