@@ -159,6 +159,30 @@ int rcwa_layer_solve(rcwa_engine* e, const double* cx, int ncx, const double* cy
 int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
                        rcwa_cplx* w, rcwa_cplx* VR, int* info);
 
+/* ---- eigensolver without device allocation ---------------------------------
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (code running inside another framework's memory pool, real-time loops where
+ * an allocation may stall, hosts that fix their device footprint up front):
+ * the same batched eigensolver as rcwa_zgeev_batched, on caller-owned DEVICE
+ * buffers, with its scratch in a static device array of the library that every
+ * GPU loading it holds until exit (about 8.7 MB).  Allocates nothing.
+ *   A     device [batch][n*n] row-major, overwritten (Schur form on return)
+ *   w     device [batch][n] eigenvalues
+ *   VR    device [batch][n*n] row-major unit-norm right eigenvectors
+ *   info  device [batch] per-matrix status (0 or RCWA_ERR_NOCONV/NONFINITE)
+ *   stream  cudaStream_t (NULL = legacy default stream); the call is
+ *           asynchronous on it.
+ * Limits: n <= RCWA_NOALLOC_MAX_N and batch <= RCWA_NOALLOC_MAX_BATCH, else
+ * RCWA_ERR_UNSUPPORTED.  The first call on a device looks up the scratch
+ * array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  All calls share the one
+ * scratch array, so calls whose work overlaps on the GPU (other streams,
+ * other threads) race: serialise them. */
+#define RCWA_NOALLOC_MAX_N 64
+#define RCWA_NOALLOC_MAX_BATCH 64
+int rcwa_zgeev_batched_noalloc(int n, int batch, rcwa_cplx* A, rcwa_cplx* w,
+                               rcwa_cplx* VR, int* info, void* stream);
+
 /* ---- the .ofd RCWA mode (sol/rcwa_bridge.cpp) --------------------------- */
 
 /* rcwalayer_t, same fields and order (include/orcwa_rcwa.h:33-41). */

@@ -34,7 +34,7 @@ EXPORTS = [
     "rcwa_engine_solve_batch", "rcwa_plan_create", "rcwa_plan_execute", "rcwa_plan_results",
     "rcwa_plan_launch_count", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
-    "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_ofd_solve",
+    "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -105,6 +105,8 @@ def load() -> C.CDLL:
     lib.rcwa_layer_solve.argtypes = [C.c_void_p, _DP, C.c_int, _DP, C.c_int, C.c_void_p, C.c_int, C.c_int, _DP, _DP,
                                      C.c_double, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
     lib.rcwa_zgeev_batched.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, _IP]
+    lib.rcwa_zgeev_batched_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                C.c_void_p]
     lib.rcwa_ofd_solve.argtypes = [C.c_void_p, C.POINTER(rcwa_ofd_setup), _DP, _DP, _DP, _DP, _IP]
     _lib = lib
     return lib
