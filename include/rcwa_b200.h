@@ -165,7 +165,7 @@ int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
  * an allocation may stall, hosts that fix their device footprint up front):
  * the same batched eigensolver as rcwa_zgeev_batched, on caller-owned DEVICE
  * buffers, with its scratch in a static device array of the library that every
- * GPU loading it holds until exit (about 8.7 MB).  Allocates nothing.
+ * GPU loading it holds until exit (about 22 MB).  Allocates nothing.
  *   A     device [batch][n*n] row-major, overwritten (Schur form on return)
  *   w     device [batch][n] eigenvalues
  *   VR    device [batch][n*n] row-major unit-norm right eigenvectors

@@ -123,3 +123,12 @@ struct StageProf {
       for (int i = 0; i < 8192; ++i) cudaEventDestroy(ev[i]);
   }
 };
+
+// Asynchronous 16-byte global->shared copies (cp.async, bypassing L1); many
+// can be in flight per thread.  cp_async_wait_all() waits for the calling
+// thread's copies; a barrier then publishes them to the other threads.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }

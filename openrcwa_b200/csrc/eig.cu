@@ -20,24 +20,29 @@ constexpr int kEigThreads = kTileThreads;  // 256
 constexpr int kWin = 32;
 constexpr int kItsPerEig = 300;
 
-__host__ __device__ inline size_t workspace_bytes(int n) {
-  const size_t nn = (size_t)n * n;
-  size_t bytes = (2 * nn + 4 * (size_t)n) * sizeof(cplx) + (size_t)n * sizeof(double);
-  return (bytes + 255) & ~(size_t)255;
-}
+constexpr int kHb = kEigPanel;
+
+__host__ __device__ inline size_t workspace_bytes(int n) { return zgeev_workspace_bytes(n); }
 
 struct Scratch {
   cplx* Z;     // n*n, column-major: Z(r, c) = Z[c*n + r]
   cplx* X;     // n*n, row-major upper-triangular eigenvector matrix of T
-  cplx* v;     // n: current Householder vector
+  cplx* v;     // n: current Householder vector / work column
   cplx* wv;    // n
   cplx* uv;    // n
   cplx* v0;    // n: leading element of each stored reflector
+  cplx* Vb;    // n x kHb  panel reflectors, explicit (row-major)
+  cplx* VH;    // kHb x n  their conjugate transposes (or n x kHb conj(V))
+  cplx* Yb;    // n x kHb  A V T  (also kHb x n work)
+  cplx* Wb;    // kHb x n  (also n x kHb work)
+  cplx* Vt;    // kHb x n  V^T (first kHb x kHb: T^H / T^T)
+  cplx* Tall;  // (ceil(n/kHb)+1) x kHb x kHb  triangular factors of all panels
   double* tau; // n
 };
 
 __device__ Scratch scratch_for(void* work, int n, int b) {
   const size_t nn = (size_t)n * n;
+  const size_t nk = (size_t)n * kHb;
   char* base = (char*)work + (size_t)b * workspace_bytes(n);
   Scratch s;
   s.Z = (cplx*)base;
@@ -46,7 +51,13 @@ __device__ Scratch scratch_for(void* work, int n, int b) {
   s.wv = s.v + n;
   s.uv = s.wv + n;
   s.v0 = s.uv + n;
-  s.tau = (double*)(s.v0 + n);
+  s.Vb = s.v0 + n;
+  s.VH = s.Vb + nk;
+  s.Yb = s.VH + nk;
+  s.Wb = s.Yb + nk;
+  s.Vt = s.Wb + nk;
+  s.Tall = s.Vt + (size_t)(n > kHb ? n : kHb) * kHb;
+  s.tau = (double*)(s.Tall + ((size_t)(n + kHb - 1) / kHb + 1) * kHb * kHb);
   return s;
 }
 
@@ -61,11 +72,6 @@ __device__ double block_sum(double v, double* red) {
   return t;
 }
 
-__device__ cplx block_sum_c(cplx v, double* red) {
-  const double re = block_sum(v.x, red);
-  const double im = block_sum(v.y, red);
-  return mkc(re, im);
-}
 
 __device__ int block_max_int(int v, int* red) {
   for (int off = 16; off > 0; off >>= 1) v = max(v, __shfl_down_sync(0xffffffffu, v, off));
@@ -78,99 +84,206 @@ __device__ int block_max_int(int v, int* red) {
   return t;
 }
 
-__device__ __forceinline__ cplx& at(cplx* M, int ld, int r, int c) { return M[(size_t)r * ld + c]; }
 
-// ---------------------------------------------------------------- Hessenberg
-__device__ void hessenberg(cplx* A, int n, int lda, const Scratch& s, double* red) {
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-  for (int k = 0; k + 2 < n; ++k) {
-    double sig = 0.0;
-    for (int i = k + 2 + tid; i < n; i += blockDim.x) sig += cnorm2(at(A, lda, i, k));
-    sig = block_sum(sig, red);
-    const cplx alpha = at(A, lda, k + 1, k);
-    if (sig == 0.0) {
-      if (tid == 0) { s.tau[k] = 0.0; s.v0[k] = mkc(1.0, 0.0); }
-      __syncthreads();
-      continue;
-    }
-    const double aa = cabs(alpha);
-    const double xnorm = sqrt(aa * aa + sig);
-    const cplx ph = aa > 0.0 ? cscale(alpha, 1.0 / aa) : mkc(1.0, 0.0);
-    const cplx beta = cscale(ph, -xnorm);
-    const cplx v0 = cscale(ph, aa + xnorm);
-    const double tau = 2.0 / (cnorm2(v0) + sig);
-    for (int i = k + 1 + tid; i < n; i += blockDim.x) s.v[i] = (i == k + 1) ? v0 : at(A, lda, i, k);
-    __syncthreads();
-    // w_j = sum_{i>k} conj(v_i) A(i,j), j > k   (thread per column)
-    for (int j = k + 1 + tid; j < n; j += blockDim.x) {
-      cplx acc = mkc(0.0, 0.0);
-      for (int i = k + 1; i < n; ++i) acc = cfmaconj(s.v[i], at(A, lda, i, j), acc);
-      s.wv[j] = acc;
-    }
-    // u_i = sum_{j>k} A(i,j) v_j, all rows   (warp per row)
-    for (int i = wid; i < n; i += nw) {
-      cplx acc = mkc(0.0, 0.0);
-      for (int j = k + 1 + lane; j < n; j += 32) acc = cfma(at(A, lda, i, j), s.v[j], acc);
-      for (int off = 16; off > 0; off >>= 1) {
-        acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
-        acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
-      }
-      if (lane == 0) s.uv[i] = acc;
-    }
-    __syncthreads();
-    cplx wdotv = mkc(0.0, 0.0);
-    for (int j = k + 1 + tid; j < n; j += blockDim.x) wdotv = cfma(s.wv[j], s.v[j], wdotv);
-    wdotv = block_sum_c(wdotv, red);
-    // A <- H A H, H = I - tau v v^H (rows/cols > k), column k handled below
-    const int ncol = n - k - 1;
-    for (size_t idx = tid; idx < (size_t)n * ncol; idx += blockDim.x) {
-      const int i = (int)(idx / ncol), j = k + 1 + (int)(idx % ncol);
-      cplx u = s.uv[i];
-      cplx a = at(A, lda, i, j);
-      if (i > k) {
-        u = cfma(cscale(s.v[i], -tau), wdotv, u);
-        a = cfma(cscale(s.v[i], -tau), s.wv[j], a);
-      }
-      a = cfma(cscale(u, -tau), cconj(s.v[j]), a);
-      at(A, lda, i, j) = a;
-    }
-    if (tid == 0) {
-      at(A, lda, k + 1, k) = beta;  // rows k+2.. keep the reflector tail v_i = x_i
-      s.tau[k] = tau;
-      s.v0[k] = v0;
-    }
-    __syncthreads();
+// In-CTA GEMM over 64x64 tiles: D = alpha*op(A)*op(B) + beta*C (C may alias D).
+template <bool TA, bool TB>
+__device__ void cta_gemm(TileSmem& sm, int M, int N, int K, const cplx* A, int lda, const cplx* B, int ldb,
+                         cplx* D, int ldd, const cplx* C, int ldc, cplx alpha, cplx beta) {
+  if (M <= 0 || N <= 0) return;
+  const int tm = (M + kTBM - 1) / kTBM, tn = (N + kTBN - 1) / kTBN;
+  for (int t = 0; t < tm * tn; ++t) {
+    const int m0 = (t / tn) * kTBM, n0 = (t % tn) * kTBN;
+    cplx acc[4][4];
+    tile_zero(acc);
+    if (K > 0) tile_mma<TA, TB>(sm, acc, A, lda, B, ldb, nullptr, M, N, K, m0, n0);
+    tile_store(acc, D, ldd, C, ldc, alpha, beta, mkc(0.0, 0.0), M, N, m0, n0);
   }
-  // Z = H_0 H_1 ... H_{n-3}, accumulated backwards (column-major Z)
+  __syncthreads();
+}
+
+// Blocked Householder reduction to Hessenberg form in compact WY form, the
+// scheme of LAPACK's gehrd/lahr2 (Quintana-Orti and van de Geijn, ACM TOMS
+// 32(2), 2006).  For panel columns k..k+jb-1 the reflectors are generated one
+// column at a time from A0 (the matrix at the panel start) corrected by
+// Y = A0 V T; each column needs one product A0(:, j+1:) v_j, the only O(n^2)
+// memory traffic per column.  The trailing matrix is then updated by
+// A <- (I - V T^H V^H)(A - Y V^H) with tile GEMMs, and Q = prod(I - V T V^H)
+// is formed backwards with tile GEMMs.  Reflectors H = I - tau v v^H are
+// Hermitian with real tau; column j stores beta at (j+1, j) and the tail of
+// v_j below it, v_j(j+1) = v0[j].
+__device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, double* red, TileSmem& tsm) {
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+  const int nb = kHb;
+  cplx* a = s.v;    // work column, then v_j
+  __shared__ cplx z[2 * kHb];
+  cplx* u = s.uv;   // n
+  for (int k = 0; k + 2 < n; k += nb) {
+    const int jb = min(nb, n - 2 - k);
+    cplx* T = s.Tall + (size_t)(k / nb) * nb * nb;
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) T[idx] = mkc(0.0, 0.0);
+    for (int jj = 0; jj < jb; ++jj) {
+      const int j = k + jj;
+      // a = A0(:, j) - Y(:, :jj) conj(V(j, :jj))
+      for (int i = tid; i < n; i += blockDim.x) {
+        cplx acc = A[(size_t)i * lda + j];
+        for (int q = 0; q < jj; ++q) acc = cfma(cneg(s.Yb[(size_t)i * nb + q]), cconj(s.Vb[(size_t)j * nb + q]), acc);
+        a[i] = acc;
+      }
+      __syncthreads();
+      if (jj > 0) {
+        // a(k+1:) <- (I - V T^H V^H) a(k+1:):  z = V^H a, z = T^H z, a -= V z
+        for (int q = wid; q < jj; q += nw) {
+          cplx acc = mkc(0.0, 0.0);
+          for (int i = k + 1 + q + lane; i < n; i += 32) acc = cfmaconj(s.Vb[(size_t)i * nb + q], a[i], acc);
+          for (int off = 16; off > 0; off >>= 1) {
+            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+          }
+          if (lane == 0) z[q] = acc;
+        }
+        __syncthreads();
+        if (tid < jj) {
+          cplx acc = mkc(0.0, 0.0);
+          for (int q = 0; q <= tid; ++q) acc = cfmaconj(T[q * nb + tid], z[q], acc);  // (T^H z)_tid
+          z[nb + tid] = acc;
+        }
+        __syncthreads();
+        for (int i = k + 1 + tid; i < n; i += blockDim.x) {
+          cplx acc = a[i];
+          for (int q = 0; q < jj; ++q) acc = cfma(cneg(s.Vb[(size_t)i * nb + q]), z[nb + q], acc);
+          a[i] = acc;
+        }
+        __syncthreads();
+      }
+      // reflector from a(j+1:)
+      double sig = 0.0;
+      for (int i = j + 2 + tid; i < n; i += blockDim.x) sig += cnorm2(a[i]);
+      sig = block_sum(sig, red);
+      const cplx alpha = a[j + 1];
+      double tau = 0.0;
+      cplx beta = alpha, v0 = mkc(1.0, 0.0);
+      if (sig != 0.0) {
+        const double aa = cabs(alpha);
+        const double xnorm = sqrt(aa * aa + sig);
+        const cplx ph = aa > 0.0 ? cscale(alpha, 1.0 / aa) : mkc(1.0, 0.0);
+        beta = cscale(ph, -xnorm);
+        v0 = cscale(ph, aa + xnorm);
+        tau = 2.0 / (cnorm2(v0) + sig);
+      }
+      // column j of the result; explicit v_j in V(:, jj) and V^H(jj, :)
+      for (int i = tid; i < n; i += blockDim.x) {
+        cplx vi = mkc(0.0, 0.0);
+        if (i <= j) A[(size_t)i * lda + j] = a[i];
+        else if (i == j + 1) { A[(size_t)i * lda + j] = beta; vi = v0; }
+        else { A[(size_t)i * lda + j] = a[i]; vi = a[i]; }
+        if (tau == 0.0) vi = mkc(0.0, 0.0);
+        s.Vb[(size_t)i * nb + jj] = vi;
+        s.VH[(size_t)jj * n + i] = cconj(vi);
+        a[i] = vi;
+      }
+      if (tid == 0) { s.tau[j] = tau; s.v0[j] = v0; }
+      __syncthreads();
+      // u = A0(:, j+1:) v_j (one pass over the trailing columns), z = V(:, :jj)^H v_j
+      for (int i = wid; i < n; i += nw) {
+        const cplx* row = A + (size_t)i * lda;
+        cplx acc0 = mkc(0.0, 0.0), acc1 = mkc(0.0, 0.0);
+        int c = j + 1 + lane;
+        for (; c + 32 < n; c += 64) {
+          acc0 = cfma(row[c], a[c], acc0);
+          acc1 = cfma(row[c + 32], a[c + 32], acc1);
+        }
+        if (c < n) acc0 = cfma(row[c], a[c], acc0);
+        acc0 = cadd(acc0, acc1);
+        for (int off = 16; off > 0; off >>= 1) {
+          acc0.x += __shfl_xor_sync(0xffffffffu, acc0.x, off);
+          acc0.y += __shfl_xor_sync(0xffffffffu, acc0.y, off);
+        }
+        if (lane == 0) u[i] = acc0;
+      }
+      for (int q = wid; q < jj; q += nw) {
+        cplx acc = mkc(0.0, 0.0);
+        for (int i = j + 1 + lane; i < n; i += 32) acc = cfmaconj(s.Vb[(size_t)i * nb + q], s.Vb[(size_t)i * nb + jj], acc);
+        for (int off = 16; off > 0; off >>= 1) {
+          acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+          acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+        }
+        if (lane == 0) z[q] = acc;
+      }
+      __syncthreads();
+      // Y(:, jj) = tau (u - Y(:, :jj) z); T(:jj, jj) = -tau T(:jj, :jj) z; T(jj, jj) = tau
+      for (int i = tid; i < n; i += blockDim.x) {
+        cplx acc = u[i];
+        for (int q = 0; q < jj; ++q) acc = cfma(cneg(s.Yb[(size_t)i * nb + q]), z[q], acc);
+        s.Yb[(size_t)i * nb + jj] = cscale(acc, tau);
+      }
+      if (tid < jj) {
+        cplx acc = mkc(0.0, 0.0);
+        for (int q = tid; q < jj; ++q) acc = cfma(T[tid * nb + q], z[q], acc);
+        T[tid * nb + jj] = cscale(acc, -tau);
+      }
+      if (tid == 0) T[jj * nb + jj] = mkc(tau, 0.0);
+      __syncthreads();
+    }
+    // trailing columns c0..n-1
+    const int c0 = k + jb;
+    const int m2 = n - c0;
+    if (m2 > 0) {
+      // A(:, c0:) -= Y V(c0:, :)^H
+      cta_gemm<false, false>(tsm, n, m2, jb, s.Yb, nb, s.VH + c0, n, A + c0, lda, A + c0, lda, mkc(-1.0, 0.0),
+                             mkc(1.0, 0.0));
+      // W = V(k+1:, :)^H A(k+1:, c0:)  (jb x m2), W2 = T^H W, A(k+1:, c0:) -= V(k+1:, :) W2
+      cta_gemm<false, false>(tsm, jb, m2, n - k - 1, s.VH + k + 1, n, A + (size_t)(k + 1) * lda + c0, lda, s.Wb + c0, n,
+                             nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
+      for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx / nb, c = idx % nb;
+        s.Vt[idx] = (r < jb && c < jb) ? cconj(T[c * nb + r]) : mkc(0.0, 0.0);  // T^H in Vt
+      }
+      __syncthreads();
+      cta_gemm<false, false>(tsm, jb, m2, jb, s.Vt, nb, s.Wb + c0, n, s.Yb + c0, n, nullptr, 0, mkc(1.0, 0.0),
+                             mkc(0.0, 0.0));
+      cta_gemm<false, false>(tsm, n - k - 1, m2, jb, s.Vb + (size_t)(k + 1) * nb, nb, s.Yb + c0, n,
+                             A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
+                             mkc(-1.0, 0.0), mkc(1.0, 0.0));
+    }
+  }
+  // Z (column-major, i.e. Zt = Z^T row-major) = Q, accumulated backwards:
+  // Zt(k+1:, k+1:) -= (Zt conj(V)) T^T V^T
   for (size_t idx = tid; idx < (size_t)n * n; idx += blockDim.x)
     s.Z[idx] = mkc((idx / n) == (idx % n) ? 1.0 : 0.0, 0.0);
   __syncthreads();
-  for (int k = n - 3; k >= 0; --k) {
-    const double tau = s.tau[k];
-    if (tau == 0.0) continue;
-    const cplx v0 = s.v0[k];
-    for (int j = k + 1 + wid; j < n; j += nw) {
-      cplx* zc = s.Z + (size_t)j * n;
-      cplx d = mkc(0.0, 0.0);
-      for (int i = k + 1 + lane; i < n; i += 32) {
-        const cplx vi = (i == k + 1) ? v0 : at(A, lda, i, k);
-        d = cfmaconj(vi, zc[i], d);
-      }
-      for (int off = 16; off > 0; off >>= 1) {
-        d.x += __shfl_xor_sync(0xffffffffu, d.x, off);
-        d.y += __shfl_xor_sync(0xffffffffu, d.y, off);
-      }
-      d = cscale(d, -tau);
-      for (int i = k + 1 + lane; i < n; i += 32) {
-        const cplx vi = (i == k + 1) ? v0 : at(A, lda, i, k);
-        zc[i] = cfma(vi, d, zc[i]);
+  const int npan = (n >= 3) ? (n - 3) / nb + 1 : 0;
+  for (int pnl = npan - 1; pnl >= 0; --pnl) {
+    const int k = pnl * nb;
+    const int jb = min(nb, n - 2 - k);
+    const cplx* T = s.Tall + (size_t)pnl * nb * nb;
+    // conj(V) (n x nb, in Wb) and V^T (nb x n, in VH) from the stored reflectors
+    for (int i = tid; i < n; i += blockDim.x) {
+      for (int q = 0; q < nb; ++q) {
+        const int j = k + q;
+        cplx vi = mkc(0.0, 0.0);
+        if (q < jb && s.tau[j] != 0.0) {
+          if (i == j + 1) vi = s.v0[j];
+          else if (i > j + 1) vi = A[(size_t)i * lda + j];
+        }
+        s.Wb[(size_t)i * nb + q] = cconj(vi);
+        s.VH[(size_t)q * n + i] = vi;
       }
     }
+    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+      const int r = idx / nb, c = idx % nb;
+      s.Vt[idx] = T[c * nb + r];  // T^T
+    }
     __syncthreads();
+    const int m = n - k - 1;
+    cplx* Zs = s.Z + (size_t)(k + 1) * n + (k + 1);
+    cta_gemm<false, false>(tsm, m, jb, m, Zs, n, s.Wb + (size_t)(k + 1) * nb, nb, s.Yb, nb, nullptr, 0,
+                           mkc(1.0, 0.0), mkc(0.0, 0.0));
+    cta_gemm<false, false>(tsm, m, jb, jb, s.Yb, nb, s.Vt, nb, s.Vb, nb, nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
+    cta_gemm<false, false>(tsm, m, m, jb, s.Vb, nb, s.VH + k + 1, n, Zs, n, Zs, n, mkc(-1.0, 0.0), mkc(1.0, 0.0));
   }
   for (size_t idx = tid; idx < (size_t)n * n; idx += blockDim.x) {
     const int i = (int)(idx / n), j = (int)(idx % n);
-    if (i > j + 1) at(A, lda, i, j) = mkc(0.0, 0.0);
+    if (i > j + 1) A[(size_t)i * lda + j] = mkc(0.0, 0.0);
   }
   __syncthreads();
 }
@@ -185,6 +298,24 @@ __device__ __forceinline__ void givens(cplx x, cplx y, double& c, cplx& s) {
     c = ax / nrm;
     s = cscale(cmul(cscale(x, 1.0 / ax), cconj(y)), 1.0 / nrm);
   }
+}
+
+// Rotation [c s; -conj(s) c] (c real) with G [x; y] = [r; 0], evaluated
+// with two reciprocal square roots after scaling both inputs by a power of
+// two: c = |x| / |(x, y)|, s = x conj(y) / (|x| |(x, y)|).
+__device__ __forceinline__ void givens_fast(cplx x, cplx y, double& c, cplx& s) {
+  const double m = fmax(fmax(fabs(x.x), fabs(x.y)), fmax(fabs(y.x), fabs(y.y)));
+  if (m == 0.0 || (y.x == 0.0 && y.y == 0.0)) { c = 1.0; s = mkc(0.0, 0.0); return; }
+  int e;
+  frexp(m, &e);
+  const double sc = ldexp(1.0, -e);
+  x = cscale(x, sc);
+  y = cscale(y, sc);
+  const double ax2 = cnorm2(x), ay2 = cnorm2(y);
+  if (ax2 == 0.0) { c = 0.0; s = mkc(1.0, 0.0); return; }
+  const double ra = rsqrt(ax2), rr = rsqrt(ax2 + ay2);
+  c = ax2 * ra * rr;
+  s = cscale(cmul(x, cconj(y)), ra * rr);
 }
 
 // Negligible subdiagonal T(k,k-1) inside the active block [l, i]:
@@ -362,6 +493,426 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
   return 0;
 }
 
+#ifdef RCWA_EIG_STATS
+// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles
+__device__ unsigned long long g_eig_stats[8];
+#define STAT_ADD(i, v) do { if (threadIdx.x == 0) atomicAdd(&g_eig_stats[i], (unsigned long long)(v)); } while (0)
+#else
+#define STAT_ADD(i, v) do { } while (0)
+#endif
+
+// ---------------------------------------------------------------- multishift QR
+// Small-bulge multishift QR (the scheme of Braman, Byers and Mathias, SIAM J.
+// Matrix Anal. Appl. 23(4), 2002) for complex Hessenberg matrices.  A sweep
+// chases a chain of s single-shift bulges, three rows apart, from the top to
+// the bottom of the active block.  The chain advances inside a 64 x 64 window
+// held in shared memory, all bulges of one chain step in parallel (their row
+// pairs and column pairs are disjoint).  Every rotation is logged; after a
+// window pass the log is applied to the rest of T (the rows right of the
+// window, the columns above it) and to Z by the warps, each streaming a
+// 32-column (or 32-row) tile through shared memory bulge by bulge, so an
+// element of T or Z crosses DRAM once per pass instead of once per rotation.
+constexpr int kMsW = 64;           // window order
+constexpr int kMsShifts = 10;      // bulges per sweep
+constexpr int kMsMin = 64;         // smaller active blocks use single-shift sweeps
+constexpr int kMsThreads = 128;    // four warps
+constexpr int kMsTileElems = 2112 + 66; // max(64 x 33, 32 x 65) + a dummy row pair
+
+struct MsSmem {
+  cplx* Wt;      // [kMsW][kMsW + 1]
+  cplx* tiles;   // [kMsThreads / 32][kMsTileElems]
+  double* lc;    // [kMsShifts][kMsW]  rotation cosines, bulge-major
+  cplx* ls;      // [kMsShifts][kMsW]  rotation sines
+  int* firstp;   // [kMsShifts] first rotation position of each bulge in the pass
+  int* cnt;      // [kMsShifts] rotations of each bulge in the pass
+  int* tfirst;   // [kMsShifts] pass step of each bulge's first rotation
+  cplx* shifts;  // [kMsShifts]
+  int* redi;     // [kMsThreads / 32]
+};
+
+constexpr size_t kMsSmemBytes = sizeof(cplx) * kMsW * (kMsW + 1) + sizeof(cplx) * (kMsThreads / 32) * kMsTileElems +
+                                sizeof(double) * kMsShifts * kMsW + sizeof(cplx) * kMsShifts * kMsW +
+                                sizeof(int) * 3 * kMsShifts + sizeof(cplx) * kMsShifts + sizeof(int) * 8;
+
+__device__ MsSmem carve_ms_smem(unsigned char* base) {
+  MsSmem sm;
+  sm.Wt = (cplx*)base;
+  sm.tiles = sm.Wt + kMsW * (kMsW + 1);
+  sm.ls = sm.tiles + (kMsThreads / 32) * kMsTileElems;
+  sm.shifts = sm.ls + kMsShifts * kMsW;
+  sm.lc = (double*)(sm.shifts + kMsShifts);
+  sm.firstp = (int*)(sm.lc + kMsShifts * kMsW);
+  sm.cnt = sm.firstp + kMsShifts;
+  sm.tfirst = sm.cnt + kMsShifts;
+  sm.redi = sm.tfirst + kMsShifts;
+  return sm;
+}
+
+#define MSW(r, c) sm.Wt[(r) * (kMsW + 1) + (c)]
+
+// Eigenvalues of the s x s upper Hessenberg matrix B (row stride ldb) by
+// single-shift QR without vectors; one warp.  Unconverged remainders after
+// the iteration budget are returned as their diagonal entries.
+__device__ void small_eigs_warp(cplx* B, int ldb, int s, cplx* out) {
+  const int lane = threadIdx.x & 31;
+  const double ulp = 2.0 * RCWA_DBL_EPS;
+  int hi = s - 1, its = 0;
+  while (hi >= 0) {
+    int lo = 0;
+    for (int k = hi; k >= 1; --k) {
+      const double h = cabs1(B[k * ldb + k - 1]);
+      if (h <= ulp * (cabs1(B[(k - 1) * ldb + k - 1]) + cabs1(B[k * ldb + k])) || h < RCWA_DBL_MIN) {
+        lo = k;
+        break;
+      }
+    }
+    if (lo == hi || its > 60) {
+      for (int k = lo + lane; k <= hi; k += 32) out[k] = B[k * ldb + k];
+      __syncwarp();
+      hi = lo - 1;
+      its = 0;
+      continue;
+    }
+    cplx sh;
+    if (its == 10 || its == 20) sh = cadd(B[hi * ldb + hi], mkc(0.75 * cabs1(B[hi * ldb + hi - 1]), 0.0));
+    else sh = wilkinson_shift(B[(hi - 1) * ldb + hi - 1], B[(hi - 1) * ldb + hi], B[hi * ldb + hi - 1], B[hi * ldb + hi]);
+    for (int r = lo; r < hi; ++r) {
+      cplx x, y;
+      if (r == lo) { x = csub(B[lo * ldb + lo], sh); y = B[(lo + 1) * ldb + lo]; }
+      else { x = B[r * ldb + r - 1]; y = B[(r + 1) * ldb + r - 1]; }
+      double c;
+      cplx sn;
+      givens(x, y, c, sn);
+      __syncwarp();
+      const int j = ((r == lo) ? r : r - 1) + lane;
+      if (j <= hi) {
+        const cplx a = B[r * ldb + j], b = B[(r + 1) * ldb + j];
+        B[r * ldb + j] = cfma(sn, b, cscale(a, c));
+        B[(r + 1) * ldb + j] = cfma(cneg(cconj(sn)), a, cscale(b, c));
+      }
+      __syncwarp();
+      if (r > lo && lane == 0) B[(r + 1) * ldb + r - 1] = mkc(0.0, 0.0);
+      const int row = lo + lane;
+      if (row <= min(r + 2, hi)) {
+        const cplx a = B[row * ldb + r], b = B[row * ldb + r + 1];
+        B[row * ldb + r] = cfma(cconj(sn), b, cscale(a, c));
+        B[row * ldb + r + 1] = cfma(cneg(sn), a, cscale(b, c));
+      }
+      __syncwarp();
+    }
+    ++its;
+  }
+}
+
+// One multishift sweep over the active block [l, i] with sm.shifts[0..s).
+// Bulge b sits at position p = l + t - 3b at chain step t; it is active while
+// l <= p <= i-1 and its rotation acts on rows/columns (p, p+1).
+__device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, const MsSmem& sm) {
+  const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
+  const int tend = (i - l) + 3 * (s - 1);
+  int t = 0;
+  while (t < tend) {
+    const int bmax0 = min(s - 1, t / 3);
+    const int pmin = l + t - 3 * bmax0;
+    // while bulges are still being introduced at l the window starts at l
+    const int ws = (t < 3 * (s - 1) || pmin == l) ? l : pmin - 1;
+    const int we = min(i, ws + kMsW - 1);
+    const int w = we - ws + 1;
+    int t1 = t;
+    while (t1 < tend) {
+      const int over = l + t1 - (i - 1);
+      const int b0 = over > 0 ? (over + 2) / 3 : 0;
+      if (we != i && l + t1 - 3 * b0 + 2 > we) break;
+      ++t1;
+    }
+    STAT_ADD(2, 1);
+#ifdef RCWA_EIG_STATS
+    const long long c_start = clock64();
+#endif
+    if (tid < s) { sm.firstp[tid] = -1; sm.cnt[tid] = 0; }
+    for (int idx = tid; idx < w * w; idx += nthr)
+      cp_async16(&MSW(idx / w, idx % w), &T[(size_t)(ws + idx / w) * ldt + ws + idx % w]);
+    cp_async_wait_all();
+    __syncthreads();
+    for (int tt = t; tt < t1; ++tt) {
+      const int over = l + tt - (i - 1);
+      const int bA = over > 0 ? (over + 2) / 3 : 0;
+      const int bB = min(s - 1, tt / 3);
+      if (tid >= bA && tid <= bB) {
+        const int b = tid, p = l + tt - 3 * b;
+        cplx x, y;
+        if (p == l) { x = csub(MSW(p - ws, p - ws), sm.shifts[b]); y = MSW(p + 1 - ws, p - ws); }
+        else { x = MSW(p - ws, p - 1 - ws); y = MSW(p + 1 - ws, p - 1 - ws); }
+        double c;
+        cplx sn;
+        givens_fast(x, y, c, sn);
+        if (sm.firstp[b] < 0) { sm.firstp[b] = p; sm.tfirst[b] = tt - t; }
+        const int k = p - sm.firstp[b];
+        sm.lc[b * kMsW + k] = c;
+        sm.ls[b * kMsW + k] = sn;
+        sm.cnt[b] = k + 1;
+      }
+      __syncthreads();
+      // row operations: bulge b on rows (p, p+1), columns max(p-1, l) .. we
+      const int nact = bB - bA + 1;
+      for (int idx = tid; idx < nact * kMsW; idx += nthr) {
+        const int b = bA + idx / kMsW;
+        const int p = l + tt - 3 * b;
+        const int j = ((p == l) ? l : p - 1) + idx % kMsW;
+        if (j > we) continue;
+        const int k = p - sm.firstp[b];
+        const double c = sm.lc[b * kMsW + k];
+        const cplx sn = sm.ls[b * kMsW + k];
+        const cplx a = MSW(p - ws, j - ws), bb = MSW(p + 1 - ws, j - ws);
+        MSW(p - ws, j - ws) = cfma(sn, bb, cscale(a, c));
+        MSW(p + 1 - ws, j - ws) = cfma(cneg(cconj(sn)), a, cscale(bb, c));
+      }
+      __syncthreads();
+      if (tid >= bA && tid <= bB) {
+        const int p = l + tt - 3 * tid;
+        if (p > l) MSW(p + 1 - ws, p - 1 - ws) = mkc(0.0, 0.0);
+      }
+      // column operations: bulge b on columns (p, p+1), rows ws .. min(p+2, i)
+      for (int idx = tid; idx < nact * kMsW; idx += nthr) {
+        const int b = bA + idx / kMsW;
+        const int p = l + tt - 3 * b;
+        const int r = ws + idx % kMsW;
+        if (r > min(p + 2, i)) continue;
+        const int k = p - sm.firstp[b];
+        const double c = sm.lc[b * kMsW + k];
+        const cplx sn = sm.ls[b * kMsW + k];
+        const cplx a = MSW(r - ws, p - ws), bb = MSW(r - ws, p + 1 - ws);
+        MSW(r - ws, p - ws) = cfma(cconj(sn), bb, cscale(a, c));
+        MSW(r - ws, p + 1 - ws) = cfma(cneg(sn), a, cscale(bb, c));
+      }
+      __syncthreads();
+    }
+#ifdef RCWA_EIG_STATS
+    const long long c_mid = clock64();
+    STAT_ADD(3, c_mid - c_start);
+#endif
+    for (int idx = tid; idx < w * w; idx += nthr) T[(size_t)(ws + idx / w) * ldt + ws + idx % w] = MSW(idx / w, idx % w);
+    // rows/columns touched in this pass
+    int rlo = i + 1, rhi = -1;
+    for (int b = 0; b < s; ++b)
+      if (sm.cnt[b] > 0) { rlo = min(rlo, sm.firstp[b]); rhi = max(rhi, sm.firstp[b] + sm.cnt[b]); }
+    const int nr = rhi - rlo + 1;
+    const int nR = (n - 1 - we + 31) / 32, nU = (ws + 31) / 32, nZ = (n + 31) / 32;
+    cplx* tile = sm.tiles + warp * kMsTileElems;
+    const int nsteps = t1 - t;
+    for (int task = warp; task < nR + nU + nZ; task += nwarp) {
+      if (task < nR) {
+        // T(rlo..rhi, j): row rotations, lane = column, chain order
+        const int j = we + 1 + 32 * task + lane;
+#ifdef RCWA_EIG_STATS
+        long long q0c = clock64();
+#endif
+        if (j < n) {
+          for (int r = 0; r < nr; ++r) cp_async16(&tile[r * 33 + lane], &T[(size_t)(rlo + r) * ldt + j]);
+          cp_async_wait_all();
+#ifdef RCWA_EIG_STATS
+          if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[5], (unsigned long long)(q1c - q0c)); q0c = q1c; }
+#endif
+          // chain-order replay, branch free: inactive bulges rotate a dummy
+          // row pair by the identity, so the ten chains interleave freely
+          int tf[kMsShifts], cn[kMsShifts], fq[kMsShifts];
+#pragma unroll
+          for (int b = 0; b < kMsShifts; ++b) {
+            tf[b] = b < s ? sm.tfirst[b] : 0;
+            cn[b] = b < s ? sm.cnt[b] : 0;
+            fq[b] = b < s ? sm.firstp[b] - rlo : 0;
+          }
+          cplx* dummy = tile + 2112;
+          cplx xc[kMsShifts];
+#pragma unroll
+          for (int b = 0; b < kMsShifts; ++b) xc[b] = mkc(0.0, 0.0);
+          for (int sg = 0; sg < nsteps; ++sg) {
+            cplx yv[kMsShifts];
+            cplx* ptr[kMsShifts];
+#pragma unroll
+            for (int b = 0; b < kMsShifts; ++b) {
+              const int k = sg - tf[b];
+              const bool act = (unsigned)k < (unsigned)cn[b];
+              ptr[b] = act ? tile + (fq[b] + k) * 33 + lane : dummy + lane;
+              if (k == 0) xc[b] = ptr[b][0];
+              yv[b] = ptr[b][33];
+            }
+#pragma unroll
+            for (int b = 0; b < kMsShifts; ++b) {
+              const int k = sg - tf[b];
+              const bool act = (unsigned)k < (unsigned)cn[b];
+              const int kk = act ? k : 0;
+              const double c = act ? sm.lc[b * kMsW + kk] : 1.0;
+              const cplx ls = sm.ls[b * kMsW + kk];
+              const cplx sn = act ? ls : mkc(0.0, 0.0);
+              const cplx xn = cfma(sn, yv[b], cscale(xc[b], c));
+              const cplx yn = cfma(cneg(cconj(sn)), xc[b], cscale(yv[b], c));
+              ptr[b][0] = xn;
+              if (k == cn[b] - 1) ptr[b][33] = yn;
+              xc[b] = act ? yn : xc[b];
+            }
+          }
+#ifdef RCWA_EIG_STATS
+          if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[6], (unsigned long long)(q1c - q0c)); q0c = q1c; }
+#endif
+          for (int r = 0; r < nr; ++r) T[(size_t)(rlo + r) * ldt + j] = tile[r * 33 + lane];
+#ifdef RCWA_EIG_STATS
+          if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[7], (unsigned long long)(q1c - q0c)); }
+#endif
+        }
+      } else {
+        // column rotations on T(rows above the window, rlo..rhi) or Z(:, rlo..rhi); lane = row
+        const bool isZ = task >= nR + nU;
+        const int r0 = 32 * (isZ ? task - nR - nU : task - nR);
+        const int rows = isZ ? n : ws;
+        if (!isZ) {
+          for (int rr = 0; rr < 32 && r0 + rr < rows; ++rr)
+            for (int c = lane; c < nr; c += 32) cp_async16(&tile[rr * 65 + c], &T[(size_t)(r0 + rr) * ldt + rlo + c]);
+        } else {
+          if (r0 + lane < rows)
+            for (int c = 0; c < nr; ++c) cp_async16(&tile[lane * 65 + c], &Z[(size_t)(rlo + c) * n + r0 + lane]);
+        }
+        cp_async_wait_all();
+        __syncwarp();
+        if (r0 + lane < rows) {
+          cplx* row = tile + lane * 65;
+          int tf[kMsShifts], cn[kMsShifts], fq[kMsShifts];
+#pragma unroll
+          for (int b = 0; b < kMsShifts; ++b) {
+            tf[b] = b < s ? sm.tfirst[b] : 0;
+            cn[b] = b < s ? sm.cnt[b] : 0;
+            fq[b] = b < s ? sm.firstp[b] - rlo : 0;
+          }
+          cplx* dummy = tile + 2112 + 2 * lane;
+          cplx xc[kMsShifts];
+#pragma unroll
+          for (int b = 0; b < kMsShifts; ++b) xc[b] = mkc(0.0, 0.0);
+          for (int sg = 0; sg < nsteps; ++sg) {
+            cplx yv[kMsShifts];
+            cplx* ptr[kMsShifts];
+#pragma unroll
+            for (int b = 0; b < kMsShifts; ++b) {
+              const int k = sg - tf[b];
+              const bool act = (unsigned)k < (unsigned)cn[b];
+              ptr[b] = act ? row + fq[b] + k : dummy;
+              if (k == 0) xc[b] = ptr[b][0];
+              yv[b] = ptr[b][1];
+            }
+#pragma unroll
+            for (int b = 0; b < kMsShifts; ++b) {
+              const int k = sg - tf[b];
+              const bool act = (unsigned)k < (unsigned)cn[b];
+              const int kk = act ? k : 0;
+              const double c = act ? sm.lc[b * kMsW + kk] : 1.0;
+              const cplx ls = sm.ls[b * kMsW + kk];
+              const cplx sn = act ? ls : mkc(0.0, 0.0);
+              const cplx xn = cfma(cconj(sn), yv[b], cscale(xc[b], c));
+              const cplx yn = cfma(cneg(sn), xc[b], cscale(yv[b], c));
+              ptr[b][0] = xn;
+              if (k == cn[b] - 1) ptr[b][1] = yn;
+              xc[b] = act ? yn : xc[b];
+            }
+          }
+        }
+        __syncwarp();
+        if (!isZ) {
+          for (int rr = 0; rr < 32 && r0 + rr < rows; ++rr)
+            for (int c = lane; c < nr; c += 32) T[(size_t)(r0 + rr) * ldt + rlo + c] = tile[rr * 65 + c];
+        } else {
+          if (r0 + lane < rows)
+            for (int c = 0; c < nr; ++c) Z[(size_t)(rlo + c) * n + r0 + lane] = tile[lane * 65 + c];
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
+#ifdef RCWA_EIG_STATS
+    STAT_ADD(4, clock64() - c_mid);
+#endif
+    t = t1;
+  }
+}
+
+// Schur form by multishift sweeps on large active blocks and single-shift
+// sweeps on small ones.  Returns 0 or RCWA_ERR_NOCONV.
+__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
+  const double ulp = 2.0 * RCWA_DBL_EPS;
+  const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
+  const int tid = threadIdx.x;
+  int i = n - 1;
+  long long sweeps = 0;
+  const long long budget = 30LL * max(10, n);
+  int stall = 0, last_i = -1, last_l = -1;
+  while (i >= 0) {
+    int best = 0;
+    for (int k = 1 + tid; k <= i; k += blockDim.x)
+      if (negligible(T, ldt, k, 0, i, ulp, smlnum)) best = max(best, k);
+    const int l = block_max_int(best, sm.redi);
+    if (l > 0 && tid == 0) T[(size_t)l * ldt + l - 1] = mkc(0.0, 0.0);
+    __syncthreads();
+    if (l >= i) {
+      --i;
+      stall = 0;
+      continue;
+    }
+    stall = (i == last_i && l == last_l) ? stall + 1 : 0;
+    last_i = i;
+    last_l = l;
+    const int m = i - l + 1;
+    if (m < kMsMin) {
+      // small blocks: single-shift sweeps whose off-window updates stream
+      // only the rotated pairs (cheaper than full tiles for few rotations)
+      cplx shift;
+      if (stall == 10 || stall == 30)
+        shift = cadd(T[(size_t)l * ldt + l], mkc(0.75 * cabs1(T[(size_t)(l + 1) * ldt + l]), 0.0));
+      else if (stall == 20 || stall == 40)
+        shift = cadd(T[(size_t)i * ldt + i], mkc(0.75 * cabs1(T[(size_t)i * ldt + i - 1]), 0.0));
+      else
+        shift = wilkinson_shift(T[(size_t)(i - 1) * ldt + i - 1], T[(size_t)(i - 1) * ldt + i],
+                                T[(size_t)i * ldt + i - 1], T[(size_t)i * ldt + i]);
+      __syncthreads();
+      STAT_ADD(1, 1);
+      qr_sweep(T, ldt, Z, n, l, i, shift, reinterpret_cast<cplx(*)[kWin + 1]>(sm.Wt), sm.lc, sm.ls);
+      if (++sweeps > budget) return RCWA_ERR_NOCONV;
+      continue;
+    }
+    const int s = kMsShifts;
+    {
+      STAT_ADD(0, 1);
+      if (tid < 32) {
+        cplx* B = sm.tiles;  // s x s, stride s + 1
+        const int o = i - s + 1;
+        for (int idx = tid; idx < s * s; idx += 32)
+          B[(idx / s) * (s + 1) + idx % s] = T[(size_t)(o + idx / s) * ldt + o + idx % s];
+        __syncwarp();
+        if (stall > 0 && stall % 6 == 0) {
+          for (int k = tid; k < s; k += 32)
+            sm.shifts[k] = cadd(B[k * (s + 1) + k],
+                                mkc(0.75 * cabs1(T[(size_t)(o + k) * ldt + o + k - 1]), 0.0));
+        } else {
+          small_eigs_warp(B, s + 1, s, sm.shifts);
+        }
+      }
+    }
+    __syncthreads();
+    ms_sweep(T, ldt, Z, n, l, i, s, sm);
+    if (++sweeps > budget) return RCWA_ERR_NOCONV;
+  }
+  return 0;
+}
+
+__global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr, int n, int lda, cplx* w_all,
+                                                             void* work, int* info_all) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  const MsSmem sm = carve_ms_smem(dsm);
+  cplx* A = Aarr[blockIdx.x];
+  const Scratch s = scratch_for(work, n, blockIdx.x);
+  const int status = schur_ms(A, lda, s.Z, n, sm);
+  cplx* w = w_all + (size_t)blockIdx.x * n;
+  for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = A[(size_t)k * lda + k];
+  if (threadIdx.x == 0) info_all[blockIdx.x] = status;
+}
+
 // ---------------------------------------------------------------- eigenvectors
 __device__ void trevc(const cplx* T, int ldt, cplx* X, int n) {
   const double ulp = 2.0 * RCWA_DBL_EPS;
@@ -391,8 +942,9 @@ __device__ void trevc(const cplx* T, int ldt, cplx* X, int n) {
 
 __global__ void __launch_bounds__(kEigThreads) hessenberg_kernel(cplx* const* Aarr, int n, int lda, void* work) {
   __shared__ double red[kEigThreads / 32];
+  __shared__ TileSmem tsm;
   const Scratch s = scratch_for(work, n, blockIdx.x);
-  hessenberg(Aarr[blockIdx.x], n, lda, s, red);
+  hessenberg_blocked(Aarr[blockIdx.x], n, lda, s, red, tsm);
 }
 
 __global__ void __launch_bounds__(kEigThreads) schur_kernel(cplx* const* Aarr, int n, int lda, cplx* w_all,
@@ -431,7 +983,6 @@ __global__ void normalize_kernel(cplx* const* VRarr, int n, int ldv, const cplx*
 
 }  // namespace
 
-size_t zgeev_workspace_bytes(int n) { return workspace_bytes(n); }
 
 cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* VR, int ldv, void* work,
                           int* info, int batch, cudaStream_t st, StageProf* prof) {
@@ -440,7 +991,20 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   StageProf& P = prof ? *prof : none;
   hessenberg_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, work);
   P.mark(st, kStHessenberg);
-  schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info);
+  if (n < kMsMin) {
+    schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info);
+  } else {
+    static bool attr_set[64] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      cudaError_t e = cudaFuncSetAttribute(schur_ms_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kMsSmemBytes);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+    schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info);
+  }
   P.mark(st, kStSchur);
   trevc_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, work);
   P.mark(st, kStTrevc);
@@ -466,3 +1030,16 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   P.mark(st, kStNormalize);
   return cudaGetLastError();
 }
+
+#ifdef RCWA_EIG_STATS
+extern "C" int rcwa_debug_eig_stats(unsigned long long* out, int reset) {
+  unsigned long long h[8];
+  if (cudaMemcpyFromSymbol(h, g_eig_stats, sizeof(h)) != cudaSuccess) return 2;
+  for (int i = 0; i < 8; ++i) out[i] = h[i];
+  if (reset) {
+    unsigned long long z[8] = {};
+    cudaMemcpyToSymbol(g_eig_stats, z, sizeof(z));
+  }
+  return 0;
+}
+#endif

@@ -2,8 +2,18 @@
 #pragma once
 #include "common.cuh"
 
-// Workspace bytes per matrix for zgeev_batched at order n.
-size_t zgeev_workspace_bytes(int n);
+constexpr int kEigPanel = 32;  // Hessenberg panel width
+
+// Workspace bytes per matrix for zgeev_batched at order n: Schur vectors and
+// eigenvector matrix (2 n^2), work vectors (4 n), panel buffers (4 n x 32 and
+// max(n, 32) x 32), the triangular factors of all panels, and the reflector
+// scalars.
+__host__ __device__ constexpr size_t zgeev_workspace_bytes(int n) {
+  return ((2 * (size_t)n * n + 4 * (size_t)n + 4 * (size_t)n * kEigPanel +
+           (size_t)(n > kEigPanel ? n : kEigPanel) * kEigPanel +
+           ((size_t)(n + kEigPanel - 1) / kEigPanel + 1) * kEigPanel * kEigPanel) * 16 +
+          (size_t)n * 8 + 255) & ~(size_t)255;
+}
 
 // For every batch item: A (n x n row-major, destroyed: holds the Schur form on
 // return) -> w (n eigenvalues), VR (n x n row-major, column k the unit-norm

@@ -63,7 +63,7 @@ def _match_eigs(a, b):
     return worst
 
 
-@pytest.mark.parametrize("n", [1, 2, 3, 7, 22, 33, 64, 100, 130])
+@pytest.mark.parametrize("n", [1, 2, 3, 7, 22, 33, 63, 64, 65, 100, 130, 257])
 def test_zgeev_random(eng, n):
     rng = np.random.default_rng(n)
     A = rng.normal(size=(3, n, n)) + 1j * rng.normal(size=(3, n, n))
