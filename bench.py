@@ -217,7 +217,7 @@ def main():
     n = 2 * N
     B = args.batch
     eng = o.Engine(local)
-    bpts, bpxy = workloads.batch_slice(pts, pxy, rank * B, B)
+    bpts, bpxy = workloads.batch_slice(pts, pxy, workloads.shard_start(rank, world, B, 0), B)
     plan = eng.plan(stacks, bpts, bpxy)
     stream = torch.cuda.Stream()
     for _ in range(args.warmup):
@@ -252,7 +252,7 @@ def main():
     h2d = d2h = 0
     t0 = time.perf_counter()
     for k in range(args.steps):
-        p2, x2 = workloads.batch_slice(pts, pxy, (rank + world * (k + 1)) * B, B)
+        p2, x2 = workloads.batch_slice(pts, pxy, workloads.shard_start(rank, world, B, k + 1), B)
         R2, T2, _, _, st2 = eng.solve_batch(stacks, p2, x2, orders=False)
         st = stacks[0]
         h2d += st.eps.nbytes + st.cx.nbytes + st.cy.nbytes + st.thickness.nbytes + p2.nbytes + x2.nbytes

@@ -1,0 +1,187 @@
+// RCWASolver (rcwa/RCWASolver.h:14-233 of the reference) on the B200 engine.
+//
+// The public calls the reference's callers make keep their signatures:
+// RCWASolver(nX, nY), addLayer, disablePML, setBlochWavevector, solve,
+// generateHorizontalPlaneWave and scatterPlaneWave (sol/rcwa_bridge.cpp:273-318,
+// rcwa/RCWADriver.cpp:284-339).  solve() runs the whole layer / interface /
+// cascade computation on the device through the C ABI and keeps the
+// scattering matrices there; every scatterPlaneWave after it only re-evaluates
+// the efficiencies for the new incident vector.  The modal basis of the
+// uniform half-spaces is the identity here, so the amplitude vector c of
+// generateHorizontalPlaneWave is [px delta; py delta].
+//
+// Outside this engine (they report on std::cerr and leave outputs empty):
+// PML (enablePML), layer translations, magnetic layers, non-uniform
+// half-spaces, incident vectors other than generateHorizontalPlaneWave's, the
+// field images (saveFieldImage, saveDeviceImage) and host copies of Tdd/Rud.
+#pragma once
+#include <algorithm>
+#include <cmath>
+#include <iostream>
+#include <string>
+#include <vector>
+
+#include "Layer.h"
+#include "defns.h"
+#include "engine_handle.h"
+
+class RCWASolver {
+ public:
+  RCWASolver(int nX, int nY) : nx_(2 * nX + 1), ny_(2 * nY + 1), nX_(nX), nY_(nY) {}
+  ~RCWASolver() { release(); }
+  RCWASolver(const RCWASolver&) = delete;
+  RCWASolver& operator=(const RCWASolver&) = delete;
+
+  // rcwa/RCWASolver.cpp:108-137: layers must share the boundary cells
+  void addLayer(const Layer& layer) {
+    if (!layers_.empty()) {
+      const Layer& a = layers_.front();
+      if (a.Lx() != layer.Lx() || a.Ly() != layer.Ly() || a.b0() != layer.b0() || a.b1() != layer.b1() ||
+          a.u0() != layer.u0() || a.u1() != layer.u1() || a.l0() != layer.l0() || a.l1() != layer.l1() ||
+          a.r0() != layer.r0() || a.r1() != layer.r1()) {
+        std::cerr << "The new layer does not match layers before!\n";
+        return;
+      }
+    }
+    layers_.push_back(layer);
+  }
+  int nLayerTypes() const { return (int)layers_.size(); }
+  void enablePML() { pml_ = true; }
+  void disablePML() { pml_ = false; }
+  void setBlochWavevector(scalar kx0, scalar ky0) { kx0_ = kx0; ky0_ = ky0; }
+  int nx() const { return nx_; }
+  int ny() const { return ny_; }
+
+  void solve(scalar lambda, const std::vector<int>& layerStack, const std::vector<scalar>& thickness,
+             const std::vector<scalar>* translation = nullptr) {
+    release();
+    if (pml_ || translation || layerStack.size() < 2 || thickness.size() != layerStack.size()) {
+      std::cerr << "[rcwa_b200] solve: PML, translations and stacks of fewer than 2 layers are not supported\n";
+      return;
+    }
+    rcwa_engine* e = rcwa_b200::engine();
+    if (!e) return;
+    for (int li : layerStack)
+      if (li < 0 || li >= (int)layers_.size() || layers_[(size_t)li].isMagnetic()) {
+        std::cerr << "[rcwa_b200] solve: invalid or magnetic layer in the stack\n";
+        return;
+      }
+    // common cell grid over every layer of the stack; subdividing a
+    // piecewise-constant cell does not change its Fourier coefficients
+    cx_ = merged(true, layerStack);
+    cy_ = merged(false, layerStack);
+    const size_t ncx = cx_.size(), ncy = cy_.size(), cells = (ncx - 1) * (ncy - 1);
+    eps_.assign(cells * layerStack.size(), rcwa_cplx{1.0, 0.0});
+    for (size_t l = 0; l < layerStack.size(); ++l) {
+      const Layer& L = layers_[(size_t)layerStack[l]];
+      for (size_t j = 0; j + 1 < ncy; ++j)
+        for (size_t i = 0; i + 1 < ncx; ++i) {
+          const scalex v = L.eps(0.5 * (cx_[i] + cx_[i + 1]), 0.5 * (cy_[j] + cy_[j + 1]));
+          eps_[l * cells + j * (ncx - 1) + i] = rcwa_cplx{v.real(), v.imag()};
+        }
+    }
+    thick_.assign(thickness.begin(), thickness.end());
+    rcwa_stack st{nX_, nY_, (int)ncx, (int)ncy, cx_.data(), cy_.data(), (int)layerStack.size(), eps_.data(),
+                  thick_.data()};
+    rcwa_point pt{0, lambda, kx0_, ky0_};
+    rcwa_cplx pxy[2] = {{1.0, 0.0}, {0.0, 0.0}};
+    int rc = rcwa_plan_create(e, &st, 1, &pt, 1, 1, pxy, RCWA_PREC_FP64, &plan_);
+    if (rc == RCWA_OK) rc = rcwa_plan_execute(plan_, nullptr);
+    double R, T;
+    int status = 0;
+    if (rc == RCWA_OK) rc = rcwa_plan_results(plan_, &R, &T, nullptr, nullptr, &status);
+    if (rc != RCWA_OK && rc != RCWA_ERR_GRAZING) {
+      std::cerr << "[rcwa_b200] solve: " << rcwa_status_string(rc) << " " << rcwa_engine_last_error(e) << "\n";
+      release();
+      return;
+    }
+    stack_ = layerStack;
+  }
+
+  // generateHorizontalPlaneWave (rcwa/RCWASolver.cpp:1778-1789)
+  void generateHorizontalPlaneWave(scalex px, scalex py, int layerType, Eigen::VectorXcs& c) {
+    const int N = nx_ * ny_;
+    c.resize(2 * N);
+    c.setZero();
+    if (!plan_ || stack_.empty() || layerType != stack_.front()) {
+      std::cerr << "[rcwa_b200] generateHorizontalPlaneWave: solve() the stack and use its incidence layer\n";
+      return;
+    }
+    const int k0 = ny_ * ((nx_ - 1) / 2) + (ny_ - 1) / 2;
+    c[k0] = px;
+    c[N + k0] = py;
+  }
+
+  // scatterPlaneWave (rcwa/RCWASolver.cpp:1792-1908)
+  void scatterPlaneWave(const Eigen::VectorXcs& cInc, int refLayerType, int trnLayerType, scalar /*k0*/,
+                        Eigen::VectorXs& REF, Eigen::VectorXs& TRN) {
+    const int N = nx_ * ny_;
+    const int k0i = ny_ * ((nx_ - 1) / 2) + (ny_ - 1) / 2;
+    if (!plan_ || stack_.empty() || refLayerType != stack_.front() || trnLayerType != stack_.back() ||
+        (int)cInc.size() != 2 * N) {
+      std::cerr << "The scatter matrix has not been solved!\n";
+      return;
+    }
+    for (int i = 0; i < 2 * N; ++i)
+      if (i != k0i && i != N + k0i && std::abs(cInc[i]) != 0.0) {
+        std::cerr << "[rcwa_b200] scatterPlaneWave: only plane waves of generateHorizontalPlaneWave\n";
+        return;
+      }
+    const rcwa_cplx pxy[2] = {{cInc[k0i].real(), cInc[k0i].imag()}, {cInc[N + k0i].real(), cInc[N + k0i].imag()}};
+    int rc = rcwa_plan_rescatter(plan_, pxy);
+    double R, T;
+    std::vector<double> ref((size_t)N), trn((size_t)N);
+    int status = 0;
+    if (rc == RCWA_OK) rc = rcwa_plan_results(plan_, &R, &T, ref.data(), trn.data(), &status);
+    if (rc != RCWA_OK) {
+      if (rc == RCWA_ERR_GRAZING) std::cerr << "Warning: incident kz is near zero (grazing incidence?)\n";
+      else std::cerr << "[rcwa_b200] scatterPlaneWave: " << rcwa_status_string(rc) << "\n";
+      return;
+    }
+    REF.resize(N);
+    TRN.resize(N);
+    for (int i = 0; i < N; ++i) {
+      REF[i] = ref[(size_t)i];
+      TRN[i] = trn[(size_t)i];
+    }
+  }
+
+  // Not materialised on the host by this engine.
+  const Eigen::MatrixXcs& Tdd() const { return empty_; }
+  const Eigen::MatrixXcs& Rud() const { return empty_; }
+
+  template <class... A>
+  void saveFieldImage(A&&...) { std::cerr << "[rcwa_b200] saveFieldImage is not provided by this engine\n"; }
+  template <class... A>
+  void saveDeviceImage(A&&...) { std::cerr << "[rcwa_b200] saveDeviceImage is not provided by this engine\n"; }
+
+ private:
+  std::vector<double> merged(bool xaxis, const std::vector<int>& stack) const {
+    std::vector<double> e;
+    for (int li : stack) {
+      const Layer& L = layers_[(size_t)li];
+      const int nc = xaxis ? L.nCx() : L.nCy();
+      for (int i = 0; i < nc; ++i) e.push_back(xaxis ? L.coordX(i) : L.coordY(i));
+    }
+    std::sort(e.begin(), e.end());
+    const double span = e.back() - e.front();
+    std::vector<double> u;
+    for (double v : e)
+      if (u.empty() || v - u.back() > 1e-12 * span) u.push_back(v);
+    return u;
+  }
+  void release() {
+    if (plan_) rcwa_plan_destroy(plan_);
+    plan_ = nullptr;
+  }
+
+  int nx_, ny_, nX_, nY_;
+  bool pml_ = true;
+  scalar kx0_ = 0.0, ky0_ = 0.0;
+  std::vector<Layer> layers_;
+  std::vector<int> stack_;
+  std::vector<double> cx_, cy_, thick_;
+  std::vector<rcwa_cplx> eps_;
+  rcwa_plan* plan_ = nullptr;
+  Eigen::MatrixXcs empty_;
+};

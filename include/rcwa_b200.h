@@ -115,6 +115,15 @@ int rcwa_plan_create(rcwa_engine* e,
 int rcwa_plan_execute(rcwa_plan* p, void* stream);
 int rcwa_plan_results(rcwa_plan* p, double* R, double* T,
                       double* ref_orders, double* trn_orders, int* status);
+/* Re-evaluate the efficiencies of an executed plan for new incident
+ * polarisation vectors pxy [n_pts][n_exc][2] without solving again (the
+ * scattering matrices stay on the device): the second and later
+ * generateHorizontalPlaneWave + scatterPlaneWave pairs of one solve
+ * (rcwa/RCWASolver.cpp:1778-1908).  Plans whose points needed more than one
+ * device-memory chunk return RCWA_ERR_UNSUPPORTED.  Read the results with
+ * rcwa_plan_results. */
+int rcwa_plan_rescatter(rcwa_plan* p, const rcwa_cplx* pxy);
+
 /* Number of engine kernel launches the last plan_execute enqueued. */
 long long rcwa_plan_launch_count(const rcwa_plan* p);
 /* Per-stage device time: with profiling on, plan_execute records CUDA events

@@ -32,7 +32,7 @@ RCWA_PREC_FP64 = 0
 EXPORTS = [
     "rcwa_status_string", "rcwa_engine_create", "rcwa_engine_destroy", "rcwa_engine_last_error",
     "rcwa_engine_solve_batch", "rcwa_plan_create", "rcwa_plan_execute", "rcwa_plan_results",
-    "rcwa_plan_launch_count", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
+    "rcwa_plan_launch_count", "rcwa_plan_rescatter", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
 ]
@@ -93,6 +93,7 @@ def load() -> C.CDLL:
     lib.rcwa_plan_results.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _IP]
     lib.rcwa_plan_launch_count.argtypes = [C.c_void_p]
     lib.rcwa_plan_launch_count.restype = C.c_longlong
+    lib.rcwa_plan_rescatter.argtypes = [C.c_void_p, C.c_void_p]
     lib.rcwa_plan_set_profiling.argtypes = [C.c_void_p, C.c_int]
     lib.rcwa_plan_stage_times.argtypes = [C.c_void_p, _DP, C.c_int]
     lib.rcwa_stage_name.argtypes = [C.c_int]
@@ -265,7 +266,7 @@ class Engine:
         return w, VR, info
 
     def ofd_solve(self, setup, orders=True):
-        """The rcwa_run computation for an oracle-style setup object with the
+        """The rcwa_run computation for a setup object with the
         fields of rcwa_ofd_setup (layers with eps1..thickness, poles, freqs)."""
         L = len(setup.layers)
         lay = (rcwa_layer_spec * L)(*[rcwa_layer_spec(l.eps1, l.eps2, l.eps1i, l.eps2i, l.fill, l.fill_y,

@@ -90,6 +90,11 @@ struct rcwa_plan {
   std::vector<std::function<cudaError_t(cudaStream_t, long long&, StageProf&)>> steps;
   long long launches = 0;
   std::unique_ptr<StageProf> prof{new StageProf()};
+  // scatter items of a single-chunk plan, kept for rcwa_plan_rescatter
+  int chunks = 0;
+  std::vector<ScatterItem> scatter_items;
+  size_t scatter_meta = 0;
+  int scatter_N = 0, scatter_nx = 0, scatter_ny = 0;
 };
 
 namespace {
@@ -805,6 +810,11 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       }
       const size_t osc = meta.add_vec(sc);
       const int nsc = (int)sc.size();
+      P->scatter_items = sc;
+      P->scatter_meta = osc;
+      P->scatter_N = N;
+      P->scatter_nx = nx;
+      P->scatter_ny = ny;
       int* status = P->dStatus;
       P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
         nl += 1;
@@ -815,6 +825,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       });
     }
   }
+  P->chunks = (int)chunks.size();
   if (cudaMalloc(&P->meta.p, std::max<size_t>(meta.bytes.size(), 16)) != cudaSuccess)
     return fail(e, RCWA_ERR_NOMEM, "metadata allocation failed");
   P->meta.bytes = meta.bytes.size();
@@ -836,6 +847,32 @@ extern "C" int rcwa_plan_execute(rcwa_plan* p, void* stream) {
   p->launches = nl;
   if (err != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, std::string("launch failed: ") + cudaGetErrorString(err));
   return RCWA_OK;
+}
+
+extern "C" int rcwa_plan_rescatter(rcwa_plan* p, const rcwa_cplx* pxy) {
+  if (!p || !pxy) return RCWA_ERR_INVALID;
+  if (p->chunks != 1) return fail(p->e, RCWA_ERR_UNSUPPORTED, "rescatter needs a single-chunk plan");
+  if (cudaSetDevice(p->e->device) != cudaSuccess) return RCWA_ERR_CUDA;
+  std::vector<ScatterItem> sc = p->scatter_items;
+  for (size_t k = 0; k < sc.size(); ++k) {
+    ScatterItem& it = sc[k];
+    const size_t e = k % (size_t)p->n_exc;
+    const rcwa_cplx px = pxy[((size_t)it.point * p->n_exc + e) * 2], py = pxy[((size_t)it.point * p->n_exc + e) * 2 + 1];
+    it.px = mkc(px.re, px.im);
+    it.py = mkc(py.re, py.im);
+  }
+  // the previous execution may still run on another stream
+  if (cudaDeviceSynchronize() != cudaSuccess) return RCWA_ERR_CUDA;
+  cudaStream_t st = p->e->stream;
+  if (cudaMemcpyAsync((char*)p->meta.p + p->scatter_meta, sc.data(), sizeof(ScatterItem) * sc.size(),
+                      cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st) != cudaSuccess)
+    return RCWA_ERR_CUDA;
+  if (scatter_efficiencies((const ScatterItem*)((char*)p->meta.p + p->scatter_meta), (int)sc.size(), p->scatter_N,
+                           p->scatter_nx, p->scatter_ny, p->dStatus, st) != cudaSuccess)
+    return RCWA_ERR_CUDA;
+  // the host copy must outlive the asynchronous upload
+  return cudaStreamSynchronize(st) == cudaSuccess ? RCWA_OK : RCWA_ERR_CUDA;
 }
 
 extern "C" long long rcwa_plan_launch_count(const rcwa_plan* p) { return p ? p->launches : 0; }

@@ -27,7 +27,7 @@ size_t scratch_bytes_needed(int n, int batch) { return kPtrBytes + zgeev_workspa
 // sized for the largest accepted call: n = 64, batch = 64 (about 22 MB)
 constexpr size_t kScratchBytes = kPtrBytes + zgeev_workspace_bytes(kMaxN) * kMaxBatch;
 
-__device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // Device address of g_noalloc_scratch per device.  In host code the symbol
 // name is only a stand-in, so the address is looked up once per device with

@@ -90,3 +90,9 @@ def pillars_2d(seed=0, nH=10, n_lambda=256, n_angle=8, n_layers=5):
 def batch_slice(points, pxy, start, count):
     idx = (np.arange(count) + start) % len(points)
     return points[idx], pxy[idx]
+
+
+def shard_start(rank: int, world: int, batch: int, step: int) -> int:
+    """First sweep index of the batch a rank solves at a step: ranks take
+    disjoint consecutive batches (weak scaling, no data exchange)."""
+    return (step * world + rank) * batch

@@ -1,0 +1,25 @@
+#!/bin/sh
+# Builds the reference-side test binary into oracle/_ref/ (kept out of git,
+# shipped with the tree to the GPU box).  Needs the reference sources at
+# $REF (default /root/reference) and the engine library already built.
+#
+#   rcwa_bridge_dropin : the reference's sol/rcwa_bridge.cpp, unmodified,
+#                        compiled against include/openrcwa_b200/rcwa/*.h and
+#                        linked with librcwa_b200.so plus dropin_harness.cpp.
+#
+# The reference's RCWA core (rcwa/*.cpp) itself is not built: it needs Eigen3
+# and LAPACKE, which this image does not have.
+set -e
+HERE=$(cd "$(dirname "$0")" && pwd)
+ROOT=$(dirname "$HERE")
+REF=${REF:-/root/reference}
+OUT="$HERE/_ref"
+mkdir -p "$OUT"
+[ -f "$REF/sol/rcwa_bridge.cpp" ] || { echo "reference sources not found at $REF"; exit 1; }
+CXXFLAGS="-std=c++17 -O2 -DRCWA_B200_NO_EIGEN -I$ROOT/include/openrcwa_b200 -I$REF/include"
+g++ $CXXFLAGS -c "$REF/sol/rcwa_bridge.cpp" -o "$OUT/rcwa_bridge.o"
+g++ $CXXFLAGS -c "$HERE/dropin_harness.cpp" -o "$OUT/dropin_harness.o"
+g++ "$OUT/rcwa_bridge.o" "$OUT/dropin_harness.o" -L"$ROOT/openrcwa_b200/lib" -lrcwa_b200 \
+    -Wl,-rpath,'$ORIGIN/../../openrcwa_b200/lib' -o "$OUT/rcwa_bridge_dropin"
+rm -f "$OUT/rcwa_bridge.o" "$OUT/dropin_harness.o"
+echo "$OUT/rcwa_bridge_dropin"

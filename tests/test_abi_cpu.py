@@ -1,0 +1,103 @@
+"""C ABI and host-side checks that need no GPU."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rcwa_b200.h")
+
+
+def _lib():
+    from openrcwa_b200 import build
+    if not os.path.exists(build.LIB):
+        build.build()
+    import openrcwa_b200 as o
+    return o, o.load()
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(rcwa_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    o, lib = _lib()
+    decl = declared_functions()
+    assert len(decl) >= 15
+    out = subprocess.run(["nm", "-D", "--defined-only", o.abi.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if " T " in l)
+    missing = [d for d in decl if d not in exported]
+    assert not missing, missing
+    assert set(decl) <= set(o.EXPORTS)
+    for d in decl:
+        getattr(lib, d)
+
+
+def test_status_strings_and_argument_checks():
+    o, lib = _lib()
+    for code in range(10):
+        assert lib.rcwa_status_string(code)
+    h = ctypes.c_void_p()
+    rc = lib.rcwa_engine_create(0, ctypes.byref(h))
+    if rc == 0:
+        lib.rcwa_engine_destroy(h)
+        pytest.skip("a GPU is present")
+    assert rc == o.abi.RCWA_ERR_NODEVICE
+    assert lib.rcwa_engine_create(0, None) == o.abi.RCWA_ERR_INVALID
+    assert lib.rcwa_plan_execute(None, None) == o.abi.RCWA_ERR_INVALID
+    assert lib.rcwa_plan_rescatter(None, None) == o.abi.RCWA_ERR_INVALID
+    assert lib.rcwa_zgeev_batched_noalloc(0, 1, None, None, None, None, None) == o.abi.RCWA_ERR_INVALID
+
+
+def test_product_fails_loudly_without_its_library(monkeypatch):
+    import openrcwa_b200.abi as abi
+    monkeypatch.setattr(abi, "_lib", None)
+    monkeypatch.setattr(abi, "LIB_PATH", "/nonexistent/librcwa_b200.so")
+    with pytest.raises(RuntimeError):
+        abi.load()
+
+
+def test_c_header_is_plain_c():
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-fsyntax-only", "-x", "c", HEADER], check=True)
+
+
+def test_cpp_adapters_compile_without_eigen():
+    src = os.path.join(ROOT, "tests", "cpp", "adapter_grating.cpp")
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-DRCWA_B200_NO_EIGEN", "-fsyntax-only",
+                    "-I", os.path.join(ROOT, "include", "openrcwa_b200"), src], check=True)
+
+
+REF = "/root/reference"
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "sol", "rcwa_bridge.cpp")),
+                    reason="reference sources not mounted")
+def test_reference_bridge_compiles_unmodified_against_adapters(tmp_path):
+    subprocess.run(["g++", "-std=c++17", "-DRCWA_B200_NO_EIGEN", "-c", os.path.join(REF, "sol", "rcwa_bridge.cpp"),
+                    "-I", os.path.join(ROOT, "include", "openrcwa_b200"), "-I", os.path.join(REF, "include"),
+                    "-o", str(tmp_path / "b.o")], check=True)
+
+
+def test_product_code_never_touches_the_oracle():
+    for base in ("openrcwa_b200", "include"):
+        for dirpath, _, files in os.walk(os.path.join(ROOT, base)):
+            for f in files:
+                if f.endswith((".py", ".cu", ".cuh", ".h", ".hpp", ".cpp")):
+                    text = open(os.path.join(dirpath, f), errors="ignore").read()
+                    assert "oracle" not in text.lower(), os.path.join(dirpath, f)
+
+
+def test_workload_shapes():
+    from openrcwa_b200 import workloads
+    st, pts, pxy = workloads.pillars_2d(seed=0)
+    assert st[0].N == 441 and pts.shape == (2048, 4) and pxy.shape == (2048, 2, 2)
+    assert st[0].eps.shape[0] == 7 and np.all(st[0].thickness[1:-1] > 0)
+    st, pts, pxy = workloads.grating_1d()
+    assert st[0].N == 11 and pts.shape == (16, 4)
+    starts = {workloads.shard_start(r, 4, 32, k) for r in range(4) for k in range(3)}
+    assert len(starts) == 12

@@ -1,0 +1,74 @@
+"""Drop-in checks on the GPU.
+
+* The reference's own sol/rcwa_bridge.cpp, unmodified, compiled against this
+  engine's RCWASolver/Layer headers (oracle/_ref/rcwa_bridge_dropin, built by
+  oracle/build_ref.sh), writes rcwa_efficiency.csv / rcwa_orders.csv that must
+  agree with the oracle's rcwa_run.
+* The header-only C++ API (tests/cpp/adapter_grating.cpp) reproduces the
+  grating known answer.
+"""
+import csv
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle.rcwa_oracle import OfdSetup, RcwaLayerSpec as L, rcwa_run
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DROPIN = os.path.join(ROOT, "oracle", "_ref", "rcwa_bridge_dropin")
+
+OFD = """OpenRCWA 4 2
+title = drop-in check
+rcwa = 5 3.0e-7 2 3.0e-7
+rcwalayer = 1.0 1.0 0.5 0
+rcwalayer = 4.0 1.0 0.5 2.0e-7 0.1 0 0.7
+rcwalayer = 2.25 2.25 0.5 0
+rcwaincidence = 20 30
+frequency1 = 4.3e14 7.5e14 4
+end
+"""
+
+
+@pytest.mark.skipif(not os.path.exists(DROPIN), reason="oracle/_ref not built (oracle/build_ref.sh)")
+def test_reference_bridge_unmodified_on_engine(tmp_path):
+    (tmp_path / "in.ofd").write_text(OFD)
+    out = subprocess.run([DROPIN, "in.ofd"], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    rows = list(csv.DictReader(open(tmp_path / "rcwa_efficiency.csv")))
+    setup = OfdSetup(nHx=5, period_x=3e-7, nHy=2, period_y=3e-7,
+                     layers=[L(1, 1, .5, 0), L(4, 1, .5, 2e-7, 0.1, 0, 0.7), L(2.25, 2.25, .5, 0)],
+                     freqs=[4.3e14 + k * 0.8e14 for k in range(5)], theta=20.0, phi=30.0)
+    ref = rcwa_run(setup)
+    assert len(rows) == len(ref)
+    for row, r in zip(rows, ref):
+        got = np.array([float(row["R_TE"]), float(row["T_TE"]), float(row["R_TM"]), float(row["T_TM"])])
+        want = np.array([r["R"][0], r["T"][0], r["R"][1], r["T"][1]])
+        assert np.max(np.abs(got - want)) < 2e-8, (got, want)
+    orders = list(csv.DictReader(open(tmp_path / "rcwa_orders.csv")))
+    assert len(orders) > 0
+    for o in orders:
+        f = [i for i, r in enumerate(ref) if abs(r["freq"] - float(o["frequency[Hz]"])) < 1e3][0]
+        pol = 0 if o["pol"] == "TE" else 1
+        k = (int(o["m"]) + 5) * 5 + (int(o["n"]) + 2)
+        assert abs(float(o["R"]) - ref[f]["ordR"][pol][k]) < 2e-8
+        assert abs(float(o["T"]) - ref[f]["ordT"][pol][k]) < 2e-8
+
+
+def test_cpp_api_adapter(tmp_path):
+    exe = tmp_path / "adapter_grating"
+    lib = os.path.join(ROOT, "openrcwa_b200", "lib")
+    subprocess.run(["g++", "-std=c++17", "-O1", "-DRCWA_B200_NO_EIGEN", "-I",
+                    os.path.join(ROOT, "include", "openrcwa_b200"),
+                    os.path.join(ROOT, "tests", "cpp", "adapter_grating.cpp"), "-L", lib, "-lrcwa_b200",
+                    f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    vals = [list(map(float, ln.split())) for ln in out.stdout.strip().splitlines()]
+    ref = rcwa_run(OfdSetup(nHx=5, period_x=3e-7, layers=[L(1, 1, .5, 0), L(4, 1, .5, 2e-7), L(2.25, 2.25, .5, 0)],
+                            freqs=[6.5e14]))[0]
+    assert abs(vals[0][0] - ref["R"][0]) < 1e-9 and abs(vals[1][0] - ref["R"][1]) < 1e-9
+    assert abs(vals[0][1] - ref["T"][0]) < 1e-9 and abs(vals[1][1] - ref["T"][1]) < 1e-9
+    assert abs(vals[0][0] - 0.138130) < 1e-6 and abs(vals[1][0] - 0.204841) < 1e-6
