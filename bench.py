@@ -41,10 +41,28 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=32, help="solve points per step per GPU")
+    ap.add_argument("--batch", type=int, default=29, help="solve points per step per GPU (29 x 5 layers = 145 "
+                    "eigensolves, one wave on 148 SMs)")
     ap.add_argument("--nh", type=int, default=10, help="harmonics per axis (Nx=Ny)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
+                    help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
+
+
+def run_eig_only(spec):
+    """One rcwa_zgeev_batched call on seeded random matrices (the kernels of the
+    per-layer eigenproblem alone), for counter captures of those kernels."""
+    import openrcwa_b200 as o
+    n, b = (int(x) for x in spec.split(","))
+    rng = np.random.default_rng(0)
+    A = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
+    eng = o.Engine(0)
+    w, V, info = eng.zgeev(A)
+    res = np.abs(A[0] @ V[0] - V[0] * w[0][None, :]).max() / np.abs(A[0]).max()
+    print(json.dumps({"eig_only": {"n": n, "batch": b, "info_max": int(info.max()), "residual": float(res)}}))
+    eng.close()
+    return 0 if info.max() == 0 else 1
 
 
 class ClockSampler:
@@ -184,6 +202,8 @@ def run_reference(args):
 
 def main():
     args = parse()
+    if args.eig_only:
+        return run_eig_only(args.eig_only)
     if args.impl == "reference":
         return run_reference(args)
     import torch
