@@ -168,6 +168,34 @@ int rcwa_layer_solve(rcwa_engine* e, const double* cx, int ncx, const double* cy
 int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
                        rcwa_cplx* w, rcwa_cplx* VR, int* info);
 
+/* ---- slab S-matrices and the Redheffer star product -------------------------
+ * Batched, FP64, host buffers; every matrix row-major [batch][n*n].
+ *
+ * rcwa_slab_smatrix_batched: dtmm::RCWAScatterMatrix::compute_v2
+ * (rcwa/RCWAScatterMatrix.cpp:90-146) -- the S-matrix of one z-uniform slab
+ * with modes W, V, gamma[batch][n] seen from a reference medium W0, V0, over a
+ * thickness wz at wavelength lambda (X = exp(i gamma wz lambda/2pi)).  The
+ * slab S-matrix is symmetric: Rdu = Rud and Tdd = Tuu
+ * (rcwa/RCWAScatterMatrix.h:40-47), so only Rud and Tuu are returned.
+ *
+ * rcwa_star_product_batched: the cascade update of the z-integrators
+ * (core/RCWAIntegrator.cpp:57-67, core/RedhefferIntegrator.cpp:136-146):
+ * the running S-matrix (Rud, Rdu, Tdd, Tuu), updated in place, absorbs the
+ * slab (rud, rdu, tdd, tuu) below it.  Start from Tdd = Tuu = I,
+ * Rud = Rdu = 0 (core/RCWAIntegrator.cpp:36-39).
+ *
+ * status[batch] (optional): 0 or RCWA_ERR_SINGULAR per item; the return value
+ * is the first nonzero status. */
+int rcwa_slab_smatrix_batched(rcwa_engine* e, int n, int batch,
+                              const rcwa_cplx* W, const rcwa_cplx* V, const rcwa_cplx* gamma,
+                              const rcwa_cplx* W0, const rcwa_cplx* V0,
+                              const double* lambda, const double* wz,
+                              rcwa_cplx* Rud, rcwa_cplx* Tuu, int* status);
+int rcwa_star_product_batched(rcwa_engine* e, int n, int batch,
+                              rcwa_cplx* Rud, rcwa_cplx* Rdu, rcwa_cplx* Tdd, rcwa_cplx* Tuu,
+                              const rcwa_cplx* rud, const rcwa_cplx* rdu,
+                              const rcwa_cplx* tdd, const rcwa_cplx* tuu, int* status);
+
 /* ---- eigensolver without device allocation ---------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (code running inside another framework's memory pool, real-time loops where

@@ -35,6 +35,7 @@ EXPORTS = [
     "rcwa_plan_launch_count", "rcwa_plan_rescatter", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
+    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -109,6 +110,9 @@ def load() -> C.CDLL:
     lib.rcwa_zgeev_batched_noalloc.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                                 C.c_void_p]
     lib.rcwa_ofd_solve.argtypes = [C.c_void_p, C.POINTER(rcwa_ofd_setup), _DP, _DP, _DP, _DP, _IP]
+    lib.rcwa_slab_smatrix_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5 + [_DP, _DP] + \
+        [C.c_void_p, C.c_void_p, _IP]
+    lib.rcwa_star_product_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 8 + [_IP]
     _lib = lib
     return lib
 
@@ -264,6 +268,43 @@ class Engine:
         if rc and not np.any(info):
             self._check(rc, "zgeev")
         return w, VR, info
+
+    @staticmethod
+    def _batch3(*mats):
+        out = [np.ascontiguousarray(m, dtype=np.complex128) for m in mats]
+        return [m[None] if m.ndim == 2 else m for m in out]
+
+    def slab_smatrix(self, W, V, gamma, W0, V0, lam, wz):
+        """(Rud, Tuu) of z-uniform slabs: dtmm::RCWAScatterMatrix::compute_v2
+        (rcwa/RCWAScatterMatrix.cpp:90-146).  Matrices (batch, n, n) or (n, n);
+        gamma (batch, n); lam and wz scalars or (batch,)."""
+        W, V, W0, V0 = self._batch3(W, V, W0, V0)
+        b, n, _ = W.shape
+        g = np.ascontiguousarray(np.broadcast_to(gamma, (b, n)), dtype=np.complex128)
+        lam = np.ascontiguousarray(np.broadcast_to(np.asarray(lam, dtype=np.float64), (b,)))
+        wz = np.ascontiguousarray(np.broadcast_to(np.asarray(wz, dtype=np.float64), (b,)))
+        Rud = np.zeros((b, n, n), dtype=np.complex128)
+        Tuu = np.zeros((b, n, n), dtype=np.complex128)
+        st = np.zeros(b, dtype=np.int32)
+        rc = self.lib.rcwa_slab_smatrix_batched(self.h, n, b, _v(W), _v(V), _v(g), _v(W0), _v(V0), _d(lam), _d(wz),
+                                                _v(Rud), _v(Tuu), _i(st))
+        if rc and not np.any(st):
+            self._check(rc, "slab_smatrix")
+        return Rud, Tuu, st
+
+    def star_product(self, S, s):
+        """Redheffer update of the running S-matrix ``S`` (dict Rud, Rdu, Tdd,
+        Tuu) with slab ``s`` (dict rud, rdu, tdd, tuu) below it
+        (core/RCWAIntegrator.cpp:57-67).  Returns the new dict and statuses."""
+        Rud, Rdu, Tdd, Tuu = [m.copy() for m in self._batch3(S["Rud"], S["Rdu"], S["Tdd"], S["Tuu"])]
+        rud, rdu, tdd, tuu = self._batch3(s["rud"], s["rdu"], s["tdd"], s["tuu"])
+        b, n, _ = Rud.shape
+        st = np.zeros(b, dtype=np.int32)
+        rc = self.lib.rcwa_star_product_batched(self.h, n, b, _v(Rud), _v(Rdu), _v(Tdd), _v(Tuu), _v(rud), _v(rdu),
+                                                _v(tdd), _v(tuu), _i(st))
+        if rc and not np.any(st):
+            self._check(rc, "star_product")
+        return {"Rud": Rud, "Rdu": Rdu, "Tdd": Tdd, "Tuu": Tuu}, st
 
     def ofd_solve(self, setup, orders=True):
         """The rcwa_run computation for a setup object with the

@@ -832,6 +832,9 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   if (!meta.bytes.empty() &&
       cudaMemcpy(P->meta.p, meta.bytes.data(), meta.bytes.size(), cudaMemcpyHostToDevice) != cudaSuccess)
     return fail(e, RCWA_ERR_CUDA, "metadata upload failed");
+  // the uploads above ran on the legacy stream, which the plan's (non-blocking)
+  // stream does not wait for
+  if (cudaStreamSynchronize(cudaStreamLegacy) != cudaSuccess) return fail(e, RCWA_ERR_CUDA, "upload failed");
   *out = P.release();
   return RCWA_OK;
 }

@@ -36,9 +36,13 @@ bool ascending(const double* x, int n) {
   return n >= 2 && x[n - 1] > x[0];
 }
 
+// A pageable host-to-device cudaMemcpy may return before its DMA lands, and the
+// engine's stream does not wait for the legacy stream, so each upload waits
+// for the legacy stream before kernels on the engine's stream read the data.
 template <class T>
 bool up(void* dst, const T* src, size_t count) {
-  return cudaMemcpy(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice) == cudaSuccess;
+  return cudaMemcpy(dst, src, sizeof(T) * count, cudaMemcpyHostToDevice) == cudaSuccess &&
+         cudaStreamSynchronize(cudaStreamLegacy) == cudaSuccess;
 }
 
 // Convolution matrices of one layer into device buffers fe11/fe22/fe33 (N x N).
