@@ -73,6 +73,13 @@ RCWA_HD cplx gamma_sqrt(cplx g) {
 #define RCWA_DBL_EPS 1.1102230246251565e-16   // unit roundoff 2^-53
 #define RCWA_DBL_MIN 2.2250738585072014e-308
 
+// Kernel launches issued by the calling host thread; plan execution reports
+// the difference over its launch sequence.
+inline long long& launch_counter() {
+  static thread_local long long count = 0;
+  return count;
+}
+
 // Host-side launch check used by the engine.
 #define RCWA_CUDA_TRY(expr)                                   \
   do {                                                        \

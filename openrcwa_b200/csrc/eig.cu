@@ -990,9 +990,11 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   StageProf none;
   StageProf& P = prof ? *prof : none;
   hessenberg_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, work);
+  ++launch_counter();
   P.mark(st, kStHessenberg);
   if (n < kMsMin) {
     schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info);
+    ++launch_counter();
   } else {
     static bool attr_set[64] = {};
     int dev = 0;
@@ -1004,9 +1006,11 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
       if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
     schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info);
+    ++launch_counter();
   }
   P.mark(st, kStSchur);
   trevc_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, work);
+  ++launch_counter();
   P.mark(st, kStTrevc);
   // VR = Z X for every matrix (Z column-major == transposed operand)
   GemmArgs g{};
@@ -1027,6 +1031,7 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   P.mark(st, kStBackTransform);
   dim3 grid((n + 127) / 128, batch);
   normalize_kernel<<<grid, 128, 0, st>>>(VR, n, ldv, w, info);
+  ++launch_counter();
   P.mark(st, kStNormalize);
   return cudaGetLastError();
 }

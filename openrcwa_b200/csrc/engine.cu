@@ -503,7 +503,6 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         cudaError_t err;
         if ((err = zgetrf_batched(a, N, N, cipiv, cinfo, nconv, st)) != cudaSuccess) return err;
         if ((err = zset_identity_batched(b, N, N, nconv, st)) != cudaSuccess) return err;
-        nl += 3;
         err = zgetrs_batched(a, N, N, cipiv, b, N, N, nconv, st);
         pf.mark(st, kStConvInverse);
         return err;
@@ -596,7 +595,6 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         v.alpha = mkc(1, 0); v.beta = mkc(0, 0); v.gammaI = mkc(0, 0);
         v.batch = 2 * nj;
         if ((err = zgemm_batched(v, st)) != cudaSuccess) return err;
-        nl += 10;
         err = finish_modes(it, nj, N, status, st);
         pf.mark(st, kStModes);
         return err;
@@ -624,7 +622,6 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       int* status = P->dStatus;
       const int cnt = 2 * np;
       P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
-        nl += 1;
         cudaError_t err = halfspace_modes((const HalfItem*)((char*)plan->meta.p + oh), cnt, N, status, st);
         pf.mark(st, kStHalfspace);
         return err;
@@ -641,7 +638,6 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       }
       const size_t oR0 = meta.add_vec(rud), oT0 = meta.add_vec(tdd);
       P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
-        nl += 1;
         cudaError_t err = cascade_init((cplx* const*)((char*)plan->meta.p + oR0),
                                        (cplx* const*)((char*)plan->meta.p + oT0), n, np, st);
         pf.mark(st, kStPhase);
@@ -744,11 +740,9 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
             return err;
           if ((err = zgetrs_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * k, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
-          nl += 4;
           if (nph > 0) {
             if ((err = apply_phase((const PhaseItem*)(m + oph), nph, n, st)) != cudaSuccess) return err;
             pf.mark(st, kStPhase);
-            nl += 1;
           }
           GemmArgs g{};
           g.M = n; g.N = n; g.K = n;
@@ -778,7 +772,6 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
           g.A = cpa(otT); g.B = cpa(otTau); g.C = nullptr; g.D = pa(otD);
           g.alpha = mkc(2, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
-          nl += 9;
           err = zgemm_batched(g, st);
           pf.mark(st, kStCascadeGemm);
           return err;
@@ -817,7 +810,6 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       P->scatter_ny = ny;
       int* status = P->dStatus;
       P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
-        nl += 1;
         cudaError_t err = scatter_efficiencies((const ScatterItem*)((char*)plan->meta.p + osc), nsc, N, nx, ny, status,
                                                st);
         pf.mark(st, kStScatter);
@@ -844,10 +836,11 @@ extern "C" int rcwa_plan_execute(rcwa_plan* p, void* stream) {
   cudaStream_t st = stream ? (cudaStream_t)stream : p->e->stream;
   if (cudaSetDevice(p->e->device) != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, "cudaSetDevice failed");
   long long nl = 0;
+  const long long launches0 = launch_counter();
   cudaError_t err = cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st);
   p->prof->begin(st);
   for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, nl, *p->prof);
-  p->launches = nl;
+  p->launches = launch_counter() - launches0;
   if (err != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, std::string("launch failed: ") + cudaGetErrorString(err));
   return RCWA_OK;
 }

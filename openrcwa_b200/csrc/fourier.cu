@@ -183,8 +183,10 @@ cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st, long long* launc
   if (P.njobs <= 0) return cudaSuccess;
   const int mys = P.max_ncy - 1, mxs = P.max_ncx - 1;
   conv_tables_kernel<<<P.njobs, 256, 0, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy);
+  ++launch_counter();
   fill_table_ptrs<<<(P.njobs * max(mys, mxs) + 255) / 256, 256, 0, st>>>(
       P.jobs, P.njobs, P.nx, P.ny, P.max_ncx, P.max_ncy, P.tx_ptrs, P.txinv_ptrs, P.ty_ptrs, P.tyinv_ptrs);
+  ++launch_counter();
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return err;
   *launches += 2;
@@ -201,11 +203,13 @@ cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st, long long* launc
   const size_t nblk = (NN + 255) / 256;
   dim3 grid((unsigned)(nblk < 2048 ? nblk : 2048), P.njobs);
   conv_gather_kernel<<<grid, 256, 0, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy);
+  ++launch_counter();
   *launches += 1;
   return cudaGetLastError();
 }
 
 cudaError_t fourier1d_device(const double* x, int nxe, double d, const cplx* f, int M, cplx* Ff, cudaStream_t st) {
   fourier1d_kernel<<<1, 256, 0, st>>>(x, nxe, d, f, M, Ff);
+  ++launch_counter();
   return cudaGetLastError();
 }

@@ -13,8 +13,8 @@ namespace {
 __global__ void __launch_bounds__(kTileThreads) zgemm_kernel(GemmArgs g) {
   __shared__ TileSmem sm;
   const int b = blockIdx.z;
-  const cplx* A = g.A ? g.A[b] : g.A0 + b * g.sA;
-  const cplx* B = g.B ? g.B[b] : g.B0 + b * g.sB;
+  const cplx* A = (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
+  const cplx* B = (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB;
   const cplx* s = g.s ? g.s[b] : nullptr;
   const int m0 = blockIdx.y * kTBM, n0 = blockIdx.x * kTBN;
   cplx acc[4][4];
@@ -26,14 +26,85 @@ __global__ void __launch_bounds__(kTileThreads) zgemm_kernel(GemmArgs g) {
     if (g.transB) tile_mma<false, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
     else tile_mma<false, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
   }
-  const cplx* C = (g.beta.x != 0.0 || g.beta.y != 0.0) ? g.C[b] : nullptr;
-  tile_store(acc, g.D ? g.D[b] : g.D0 + b * g.sD, g.ldd, C, g.ldc, g.alpha, g.beta, g.gammaI, g.M, g.N, m0, n0);
+  const cplx* C = (g.beta.x != 0.0 || g.beta.y != 0.0) ? g.C[b] + g.offC : nullptr;
+  tile_store(acc, (g.D ? g.D[b] : g.D0 + b * g.sD) + g.offD, g.ldd, C, g.ldc, g.alpha, g.beta, g.gammaI, g.M, g.N,
+             m0, n0);
 }
 
-// One CTA per matrix: right-looking blocked LU with partial pivoting, panel
-// width 32.  Panel columns are factorised in global memory (L1/L2 resident),
-// the U12 block row by a shared-memory triangular solve, and the trailing
-// matrix by the register-blocked tile GEMM.
+// Factorise panel columns kb .. kb+jb-1 of the n x n matrix A in place (rows
+// kb .. n-1), LAPACK getf2 order: pivot = largest |re|+|im| in the column
+// (first index on ties), the pivot rows are interchanged across all n columns,
+// the column is scaled by the reciprocal pivot and the rest of the panel gets
+// the rank-1 update.  Whole CTA; info keeps the first exactly-zero pivot.
+__device__ void lu_panel(cplx* A, int n, int lda, int kb, int jb, int* ipiv, int& info, double* red_v, int* red_i,
+                         int* s_piv) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  for (int j = kb; j < kb + jb; ++j) {
+    double best = -1.0;
+    int bi = j;
+    for (int i = j + tid; i < n; i += nthr) {
+      double v = cabs1(A[(size_t)i * lda + j]);
+      if (v > best) { best = v; bi = i; }
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      double ov = __shfl_down_sync(0xffffffffu, best, off);
+      int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+    }
+    if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double bv = red_v[0];
+      int bix = red_i[0];
+      for (int w = 1; w < nthr / 32; ++w)
+        if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bix)) { bv = red_v[w]; bix = red_i[w]; }
+      *s_piv = bix;
+      ipiv[j] = bix;
+    }
+    __syncthreads();
+    const int p = *s_piv;
+    if (p != j) {
+      for (int c = tid; c < n; c += nthr) {
+        cplx t = A[(size_t)j * lda + c];
+        A[(size_t)j * lda + c] = A[(size_t)p * lda + c];
+        A[(size_t)p * lda + c] = t;
+      }
+    }
+    __syncthreads();
+    const cplx piv = A[(size_t)j * lda + j];
+    if (piv.x == 0.0 && piv.y == 0.0) {
+      if (info == 0) info = j + 1;
+    } else {
+      const cplx inv = cdiv(mkc(1.0, 0.0), piv);
+      for (int i = j + 1 + tid; i < n; i += nthr) A[(size_t)i * lda + j] = cmul(A[(size_t)i * lda + j], inv);
+    }
+    __syncthreads();
+    const int w = kb + jb - j - 1;
+    if (w > 0) {
+      const int rows = n - j - 1;
+      for (int idx = tid; idx < rows * w; idx += nthr) {
+        const int i = j + 1 + idx / w, c = j + 1 + idx % w;
+        A[(size_t)i * lda + c] = cfma(cneg(A[(size_t)i * lda + j]), A[(size_t)j * lda + c], A[(size_t)i * lda + c]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// U12(:, c) = L11^-1 A12(:, c) for columns c = c0 + tid (L11 unit lower,
+// jb x jb at (kb, kb), staged in Lsm); threads with c >= n idle.
+__device__ void lu_trsm_cols(cplx* A, int n, int lda, int kb, int jb, int c, cplx (*Lsm)[33]) {
+  if (c >= n) return;
+  for (int r = 1; r < jb; ++r) {
+    cplx x = A[(size_t)(kb + r) * lda + c];
+    for (int q = 0; q < r; ++q) x = cfma(cneg(Lsm[r][q]), A[(size_t)(kb + q) * lda + c], x);
+    A[(size_t)(kb + r) * lda + c] = x;
+  }
+}
+
+// One CTA per matrix: right-looking blocked LU, panel width 32; the U12 block
+// row by a shared-memory triangular solve and the trailing matrix by the
+// register-blocked tile GEMM.
 __global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr, int n, int lda,
                                                              int* ipiv_all, int* info_all) {
   // the triangular block and the GEMM slabs are used in separate phases
@@ -50,74 +121,14 @@ __global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr,
   int info = 0;
   for (int kb = 0; kb < n; kb += 32) {
     const int jb = min(32, n - kb);
-    for (int j = kb; j < kb + jb; ++j) {
-      // pivot: largest |re|+|im| in column j, rows j..n-1 (first index on ties)
-      double best = -1.0;
-      int bi = j;
-      for (int i = j + tid; i < n; i += kTileThreads) {
-        double v = cabs1(A[(size_t)i * lda + j]);
-        if (v > best) { best = v; bi = i; }
-      }
-      for (int off = 16; off > 0; off >>= 1) {
-        double ov = __shfl_down_sync(0xffffffffu, best, off);
-        int oi = __shfl_down_sync(0xffffffffu, bi, off);
-        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-      }
-      if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
-      __syncthreads();
-      if (tid == 0) {
-        double bv = red_v[0];
-        int bix = red_i[0];
-        for (int w = 1; w < kTileThreads / 32; ++w)
-          if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bix)) { bv = red_v[w]; bix = red_i[w]; }
-        s_piv = bix;
-        ipiv[j] = bix;
-      }
-      __syncthreads();
-      const int p = s_piv;
-      if (p != j) {
-        for (int c = tid; c < n; c += kTileThreads) {
-          cplx t = A[(size_t)j * lda + c];
-          A[(size_t)j * lda + c] = A[(size_t)p * lda + c];
-          A[(size_t)p * lda + c] = t;
-        }
-      }
-      __syncthreads();
-      const cplx piv = A[(size_t)j * lda + j];
-      if (piv.x == 0.0 && piv.y == 0.0) {
-        if (info == 0) info = j + 1;
-      } else {
-        const cplx inv = cdiv(mkc(1.0, 0.0), piv);
-        for (int i = j + 1 + tid; i < n; i += kTileThreads)
-          A[(size_t)i * lda + j] = cmul(A[(size_t)i * lda + j], inv);
-      }
-      __syncthreads();
-      const int w = kb + jb - j - 1;
-      if (w > 0) {
-        const int rows = n - j - 1;
-        for (int idx = tid; idx < rows * w; idx += kTileThreads) {
-          const int i = j + 1 + idx / w, c = j + 1 + idx % w;
-          A[(size_t)i * lda + c] =
-              cfma(cneg(A[(size_t)i * lda + j]), A[(size_t)j * lda + c], A[(size_t)i * lda + c]);
-        }
-      }
-      __syncthreads();
-    }
+    lu_panel(A, n, lda, kb, jb, ipiv, info, red_v, red_i, &s_piv);
     if (kb + jb < n) {
-      // U12 = L11^-1 A12 (L11 unit lower, staged in shared memory); the
-      // panel's row interchanges were applied to whole rows above.
       for (int idx = tid; idx < jb * jb; idx += kTileThreads) {
         const int r = idx / jb, q = idx % jb;
         Lsm[r][q] = A[(size_t)(kb + r) * lda + kb + q];
       }
       __syncthreads();
-      for (int c = kb + jb + tid; c < n; c += kTileThreads) {
-        for (int r = 1; r < jb; ++r) {
-          cplx x = A[(size_t)(kb + r) * lda + c];
-          for (int q = 0; q < r; ++q) x = cfma(cneg(Lsm[r][q]), A[(size_t)(kb + q) * lda + c], x);
-          A[(size_t)(kb + r) * lda + c] = x;
-        }
-      }
+      for (int c = kb + jb + tid; c < n; c += kTileThreads) lu_trsm_cols(A, n, lda, kb, jb, c, Lsm);
       __syncthreads();
       const int m2 = n - kb - jb;
       const int tiles_m = (m2 + kTBM - 1) / kTBM, tiles_n = (m2 + kTBN - 1) / kTBN;
@@ -135,6 +146,31 @@ __global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr,
     }
   }
   if (tid == 0) info_all[b] = info;
+}
+
+// Panel step of the multi-launch LU: one CTA per matrix factorises columns
+// kb .. kb+jb-1 (the first panel also clears info).
+__global__ void __launch_bounds__(kTileThreads) getrf_panel_kernel(cplx* const* Aarr, int n, int lda, int kb, int jb,
+                                                                  int* ipiv_all, int* info_all) {
+  __shared__ double red_v[kTileThreads / 32];
+  __shared__ int red_i[kTileThreads / 32];
+  __shared__ int s_piv;
+  const int b = blockIdx.x;
+  int info = kb == 0 ? 0 : info_all[b];
+  lu_panel(Aarr[b], n, lda, kb, jb, ipiv_all + (size_t)b * n, info, red_v, red_i, &s_piv);
+  if (threadIdx.x == 0) info_all[b] = info;
+}
+
+// U12 of the multi-launch LU: one CTA per (matrix, 64 columns right of the panel).
+__global__ void __launch_bounds__(64) getrf_trsm_kernel(cplx* const* Aarr, int n, int lda, int kb, int jb) {
+  __shared__ cplx Lsm[32][33];
+  cplx* A = Aarr[blockIdx.y];
+  for (int idx = threadIdx.x; idx < jb * jb; idx += 64) {
+    const int r = idx / jb, q = idx % jb;
+    Lsm[r][q] = A[(size_t)(kb + r) * lda + kb + q];
+  }
+  __syncthreads();
+  lu_trsm_cols(A, n, lda, kb, jb, kb + jb + blockIdx.x * 64 + threadIdx.x, Lsm);
 }
 
 // Blocked LU solve: one CTA per (matrix, 64-column block of B).
@@ -243,13 +279,54 @@ cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st) {
   if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
   dim3 grid((g.N + kTBN - 1) / kTBN, (g.M + kTBM - 1) / kTBM, g.batch);
   zgemm_kernel<<<grid, kTileThreads, 0, st>>>(g);
+  ++launch_counter();
   return cudaGetLastError();
 }
+
+namespace {
+int sm_count() {
+  static int count = 0;
+  if (!count) {
+    int dev = 0, c = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&c, cudaDevAttrMultiProcessorCount, dev) ==
+                                                  cudaSuccess && c > 0)
+      count = c;
+    else
+      return 148;
+  }
+  return count;
+}
+}  // namespace
 
 cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
                            cudaStream_t st) {
   if (batch <= 0 || n <= 0) return cudaSuccess;
-  zgetrf_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, ipiv, info);
+  if (n <= 128 || batch >= sm_count()) {
+    zgetrf_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, ipiv, info);
+    ++launch_counter();
+    return cudaGetLastError();
+  }
+  for (int kb = 0; kb < n; kb += 32) {
+    const int jb = min(32, n - kb);
+    getrf_panel_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, kb, jb, ipiv, info);
+    ++launch_counter();
+    const int m2 = n - kb - jb;
+    if (m2 <= 0) break;
+    getrf_trsm_kernel<<<dim3((m2 + 63) / 64, batch), 64, 0, st>>>(A, n, lda, kb, jb);
+    ++launch_counter();
+    // A22 -= L21 U12
+    GemmArgs g{};
+    g.A = A; g.B = A; g.C = A; g.D = A;
+    g.offA = (size_t)(kb + jb) * lda + kb;
+    g.offB = (size_t)kb * lda + kb + jb;
+    g.offC = g.offD = (size_t)(kb + jb) * lda + kb + jb;
+    g.M = m2; g.N = m2; g.K = jb;
+    g.lda = g.ldb = g.ldc = g.ldd = lda;
+    g.alpha = mkc(-1.0, 0.0); g.beta = mkc(1.0, 0.0); g.gammaI = mkc(0.0, 0.0);
+    g.batch = batch;
+    cudaError_t err = zgemm_batched(g, st);
+    if (err != cudaSuccess) return err;
+  }
   return cudaGetLastError();
 }
 
@@ -258,6 +335,7 @@ cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipi
   if (batch <= 0 || n <= 0 || nrhs <= 0) return cudaSuccess;
   dim3 grid((nrhs + 63) / 64, batch);
   zgetrs_kernel<<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, B, nrhs, ldb);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
@@ -265,6 +343,7 @@ cudaError_t zset_identity_batched(cplx* const* B, int n, int ldb, int batch, cud
   if (batch <= 0 || n <= 0) return cudaSuccess;
   dim3 grid(min(1024, (n * n + 255) / 256), batch);
   identity_kernel<<<grid, 256, 0, st>>>(B, n, ldb);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
@@ -273,5 +352,6 @@ cudaError_t zcopy_batched(const cplx* const* src, int lds, cplx* const* dst, int
   if (batch <= 0 || rows <= 0 || cols <= 0) return cudaSuccess;
   dim3 grid(min(1024, (rows * cols + 255) / 256), batch);
   copy_kernel<<<grid, 256, 0, st>>>(src, lds, dst, ldd, rows, cols);
+  ++launch_counter();
   return cudaGetLastError();
 }

@@ -20,6 +20,8 @@ struct GemmArgs {
   const cplx* B0 = nullptr;
   cplx* D0 = nullptr;
   size_t sA = 0, sB = 0, sD = 0;
+  // element offsets added to every item's A, B, C and D (sub-blocks)
+  size_t offA = 0, offB = 0, offC = 0, offD = 0;
 };
 
 // D = alpha*op(A)*diag(s)*op(B) + beta*C + gammaI*I for every batch item.
@@ -27,7 +29,10 @@ cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st);
 
 // In-place LU with partial pivoting (row interchanges, LAPACK getrf
 // convention, 0-based pivots) of square n x n matrices.  info[b] = 0, or k+1
-// when U(k,k) is exactly zero.
+// when U(k,k) is exactly zero.  Batches that fill the GPU run one CTA per
+// matrix; smaller batches of large matrices run panel by panel, the panel
+// factorisation one CTA per matrix and the triangular solve and trailing
+// update spread over all SMs.
 cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
                            cudaStream_t st);
 

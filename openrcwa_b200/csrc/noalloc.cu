@@ -68,6 +68,7 @@ extern "C" int rcwa_zgeev_batched_noalloc(int n, int batch, rcwa_cplx* A, rcwa_c
   cplx** ptrV = ptrA + kMaxBatch;
   void* work = base + kPtrBytes;
   fill_ptrs_kernel<<<(batch + 127) / 128, 128, 0, st>>>((cplx*)A, (cplx*)VR, n, batch, ptrA, ptrV);
+  ++launch_counter();
   if (cudaGetLastError() != cudaSuccess) return RCWA_ERR_CUDA;
   // every scratch region is written before it is read inside the eigensolver
   // (Z starts as the identity, X is initialised by the back-substitution),

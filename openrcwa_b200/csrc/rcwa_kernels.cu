@@ -224,24 +224,28 @@ inline dim3 ew_grid(size_t elems, int count) {
 cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   assemble_m_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
 cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   finish_modes_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, status);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
 cudaError_t halfspace_modes(const HalfItem* items, int count, int N, int* status, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   halfspace_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, status);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
 cudaError_t apply_phase(const PhaseItem* items, int count, int n, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   phase_kernel<<<ew_grid((size_t)n * n, count), 256, 0, st>>>(items, n);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
@@ -249,6 +253,7 @@ cudaError_t scatter_efficiencies(const ScatterItem* items, int count, int N, int
                                  cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   scatter_kernel<<<count, 256, 0, st>>>(items, N, nx, ny, status);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
@@ -256,12 +261,14 @@ cudaError_t zaxpby_batched(const cplx* const* X, const cplx* const* Y, cplx* con
                            int count, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   axpby_kernel<<<ew_grid((size_t)n * n, count), 256, 0, st>>>(X, Y, D, a, b, n);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
 cudaError_t cascade_init(cplx* const* Rud, cplx* const* Tdd, int n, int count, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   cascade_init_kernel<<<ew_grid((size_t)n * n, count), 256, 0, st>>>(Rud, Tdd, n);
+  ++launch_counter();
   return cudaGetLastError();
 }
 
@@ -269,5 +276,6 @@ cudaError_t fold_info(const int* info, const int* item_point, int count, int cod
                       cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   fold_info_kernel<<<(count + 255) / 256, 256, 0, st>>>(info, item_point, count, code, status);
+  ++launch_counter();
   return cudaGetLastError();
 }

@@ -192,6 +192,7 @@ extern "C" int rcwa_slab_smatrix_batched(rcwa_engine* e, int n, int batch, const
   {
     dim3 grid((unsigned)std::min<size_t>(1024, (nn + 255) / 256), batch);
     slab_rhs_kernel<<<grid, 256, 0, st>>>((const SlabRhsItem*)ditems.p, n);
+    ++launch_counter();
     run(cudaGetLastError());
   }
   run(zgetrf_batched(pb.at(pA), n, n, piv, info, batch, st));

@@ -215,3 +215,17 @@ def test_invalid_setup_rejected(eng):
     import openrcwa_b200 as o
     with pytest.raises(o.RcwaError):
         eng.ofd_solve(OfdSetup(nHx=1, period_x=3e-7, layers=[L(1, 1, .5, 0)], freqs=[5e14]))
+
+
+def test_large_orders_panel_lu_path(eng):
+    # n = 162 and a small batch: the interface and tau factorisations take the
+    # multi-launch panel LU instead of one CTA per matrix
+    rng = np.random.default_rng(5)
+    layers = [L(1, 1, .5, 0)]
+    for _ in range(2):
+        layers.append(L(rng.uniform(2, 12), 1.0, rng.uniform(.2, .8), rng.uniform(50e-9, 300e-9),
+                        rng.uniform(0, .5), 0.0, rng.uniform(.2, .8)))
+    layers.append(L(2.25, 2.25, .5, 0))
+    setup = OfdSetup(nHx=4, period_x=4e-7, nHy=4, period_y=4e-7, layers=layers,
+                     freqs=orc.C0 / np.array([450e-9, 700e-9]), theta=35.0, phi=20.0)
+    _cmp_ofd(eng, setup)
