@@ -528,11 +528,12 @@ struct MsSmem {
   int* tfirst;   // [kMsShifts] pass step of each bulge's first rotation
   cplx* shifts;  // [kMsShifts]
   int* redi;     // [kMsThreads / 32]
+  int* aed;      // [4] early-deflation results: converged flag, undeflated count, shift count
 };
 
 constexpr size_t kMsSmemBytes = sizeof(cplx) * kMsW * (kMsW + 1) + sizeof(cplx) * (kMsThreads / 32) * kMsTileElems +
                                 sizeof(double) * kMsShifts * kMsW + sizeof(cplx) * kMsShifts * kMsW +
-                                sizeof(int) * 3 * kMsShifts + sizeof(cplx) * kMsShifts + sizeof(int) * 8;
+                                sizeof(int) * 3 * kMsShifts + sizeof(cplx) * kMsShifts + sizeof(int) * 12;
 
 __device__ MsSmem carve_ms_smem(unsigned char* base) {
   MsSmem sm;
@@ -545,6 +546,7 @@ __device__ MsSmem carve_ms_smem(unsigned char* base) {
   sm.cnt = sm.firstp + kMsShifts;
   sm.tfirst = sm.cnt + kMsShifts;
   sm.redi = sm.tfirst + kMsShifts;
+  sm.aed = sm.redi + kMsThreads / 32;
   return sm;
 }
 
@@ -603,6 +605,293 @@ __device__ void small_eigs_warp(cplx* B, int ldb, int s, cplx* out) {
     ++its;
   }
 }
+
+// ---------------------------------------------------------------- aggressive early deflation
+// Aggressive early deflation (Braman, Byers and Mathias, SIAM J. Matrix Anal.
+// Appl. 23(4), 2002; the complex variant of LAPACK's zlaqr3): the trailing
+// kAedW x kAedW window of the active block is brought to Schur form with its
+// unitary V; the spike s*conj(V(0,:)) that couples it to the rest tells which
+// window eigenvalues have converged.  Converged ones at the bottom are
+// deflated, the others are moved to the top by adjacent swaps and serve as
+// shifts; the spike of the undeflated part is reflected onto its first entry
+// and that part is returned to Hessenberg form by Householder reflectors.
+constexpr int kAedW = 32;        // window order (one lane per column)
+constexpr int kAedLd = kAedW + 1;
+constexpr int kAedNibble = 14;   // percent of the window deflated that skips the sweep
+
+#define AW(r, c) W[(r) * kAedLd + (c)]
+#define AV(r, c) V[(r) * kAedLd + (c)]
+
+// Schur form of the Hessenberg window W (nw x nw) with V <- V G^H for every
+// rotation G; single-shift QR by one warp.  Returns false when the iteration
+// budget runs out.
+__device__ bool aed_window_schur(cplx* W, cplx* V, int nw) {
+  const int lane = threadIdx.x & 31;
+  const double ulp = 2.0 * RCWA_DBL_EPS;
+  int hi = nw - 1, its = 0, total = 0;
+  while (hi >= 0) {
+    __syncwarp();
+    bool defl = false;
+    if (lane >= 1 && lane <= hi) {
+      const double h = cabs1(AW(lane, lane - 1));
+      defl = h <= ulp * (cabs1(AW(lane - 1, lane - 1)) + cabs1(AW(lane, lane))) || h < RCWA_DBL_MIN;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, defl);
+    const int lo = mask ? 31 - __clz(mask) : 0;
+    __syncwarp();
+    if (lo == hi) {
+      if (hi > 0 && lane == 0) AW(hi, hi - 1) = mkc(0.0, 0.0);
+      --hi;
+      its = 0;
+      continue;
+    }
+    if (lo > 0 && lane == 0) AW(lo, lo - 1) = mkc(0.0, 0.0);
+    if (++total > 30 * nw) return false;
+    cplx sh;
+    if (its == 10) sh = cadd(AW(lo, lo), mkc(0.75 * cabs1(AW(lo + 1, lo)), 0.0));
+    else if (its == 20) sh = cadd(AW(hi, hi), mkc(0.75 * cabs1(AW(hi, hi - 1)), 0.0));
+    else sh = wilkinson_shift(AW(hi - 1, hi - 1), AW(hi - 1, hi), AW(hi, hi - 1), AW(hi, hi));
+    __syncwarp();
+    for (int p = lo; p < hi; ++p) {
+      cplx x, y;
+      if (p == lo) { x = csub(AW(lo, lo), sh); y = AW(lo + 1, lo); }
+      else { x = AW(p, p - 1); y = AW(p + 1, p - 1); }
+      double c;
+      cplx sn;
+      givens(x, y, c, sn);
+      __syncwarp();
+      if (lane >= (p == lo ? p : p - 1) && lane < nw) {
+        const cplx a = AW(p, lane), b = AW(p + 1, lane);
+        AW(p, lane) = cfma(sn, b, cscale(a, c));
+        AW(p + 1, lane) = cfma(cneg(cconj(sn)), a, cscale(b, c));
+      }
+      __syncwarp();
+      if (p > lo && lane == 0) AW(p + 1, p - 1) = mkc(0.0, 0.0);
+      if (lane <= min(p + 2, hi)) {
+        const cplx a = AW(lane, p), b = AW(lane, p + 1);
+        AW(lane, p) = cfma(cconj(sn), b, cscale(a, c));
+        AW(lane, p + 1) = cfma(cneg(sn), a, cscale(b, c));
+      }
+      if (lane < nw) {
+        const cplx a = AV(lane, p), b = AV(lane, p + 1);
+        AV(lane, p) = cfma(cconj(sn), b, cscale(a, c));
+        AV(lane, p + 1) = cfma(cneg(sn), a, cscale(b, c));
+      }
+      __syncwarp();
+    }
+    ++its;
+  }
+  __syncwarp();
+  return true;
+}
+
+// Swap the adjacent eigenvalues k, k+1 of the upper triangular W (LAPACK
+// ztrexc step): G from (W(k,k+1), W(k+1,k+1) - W(k,k)) applied to rows
+// k, k+1 right of the pair, to columns k, k+1 above it and to V; the
+// diagonal entries trade places and W(k,k+1) keeps its value.  One warp.
+__device__ void aed_swap(cplx* W, cplx* V, int nw, int k) {
+  const int lane = threadIdx.x & 31;
+  const cplx t11 = AW(k, k), t22 = AW(k + 1, k + 1);
+  double c;
+  cplx sn;
+  givens(AW(k, k + 1), csub(t22, t11), c, sn);
+  __syncwarp();
+  if (lane >= k + 2 && lane < nw) {
+    const cplx a = AW(k, lane), b = AW(k + 1, lane);
+    AW(k, lane) = cfma(sn, b, cscale(a, c));
+    AW(k + 1, lane) = cfma(cneg(cconj(sn)), a, cscale(b, c));
+  }
+  if (lane < k) {
+    const cplx a = AW(lane, k), b = AW(lane, k + 1);
+    AW(lane, k) = cfma(cconj(sn), b, cscale(a, c));
+    AW(lane, k + 1) = cfma(cneg(sn), a, cscale(b, c));
+  }
+  if (lane < nw) {
+    const cplx a = AV(lane, k), b = AV(lane, k + 1);
+    AV(lane, k) = cfma(cconj(sn), b, cscale(a, c));
+    AV(lane, k + 1) = cfma(cneg(sn), a, cscale(b, c));
+  }
+  if (lane == 0) { AW(k, k) = t22; AW(k + 1, k + 1) = t11; }
+  __syncwarp();
+}
+
+// Householder reflector H = I - tau v v^H with H^H x = beta e1 for the
+// vector x[0..len) in shared memory (LAPACK zlarfg convention: v[0] = 1,
+// tau = (beta - alpha)/beta, beta = -sign(Re alpha) ||x||); v overwrites x.
+// One warp; returns tau (zero when x is already beta e1).
+__device__ cplx aed_house(cplx* x, int len) {
+  const int lane = threadIdx.x & 31;
+  double part = (lane >= 1 && lane < len) ? cnorm2(x[lane]) : 0.0;
+  for (int off = 16; off > 0; off >>= 1) part += __shfl_xor_sync(0xffffffffu, part, off);
+  const cplx alpha = x[0];
+  __syncwarp();
+  if (part == 0.0 && alpha.y == 0.0) return mkc(0.0, 0.0);
+  const double beta = -copysign(sqrt(cnorm2(alpha) + part), alpha.x);
+  const cplx tau = mkc((beta - alpha.x) / beta, -alpha.y / beta);
+  const cplx scal = cdiv(mkc(1.0, 0.0), csub(alpha, mkc(beta, 0.0)));
+  if (lane >= 1 && lane < len) x[lane] = cmul(x[lane], scal);
+  if (lane == 0) x[0] = mkc(beta, 0.0);  // beta kept in x[0]; v[0] = 1 implied
+  __syncwarp();
+  return tau;
+}
+
+// M(r0 + r, c) -= conj(tau) v[r] (v^H M(r0.., c)) for columns c in [c0, nw):
+// the left product H^H M on rows r0 .. r0+len-1; v[0] = 1.  One warp.
+__device__ void aed_left(cplx* M, const cplx* v, int len, cplx tau, int r0, int c0, int nw) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= c0 && lane < nw) {
+    cplx w = M[r0 * kAedLd + lane];
+    for (int r = 1; r < len; ++r) w = cfmaconj(v[r], M[(r0 + r) * kAedLd + lane], w);
+    const cplx f = cmul(cconj(tau), w);
+    M[r0 * kAedLd + lane] = csub(M[r0 * kAedLd + lane], f);
+    for (int r = 1; r < len; ++r) M[(r0 + r) * kAedLd + lane] = csub(M[(r0 + r) * kAedLd + lane], cmul(v[r], f));
+  }
+  __syncwarp();
+}
+
+// M(r, c0 + c) -= tau (M(r, c0..) v) conj(v[c]) for rows r < rows: the right
+// product M H on columns c0 .. c0+len-1; v[0] = 1.  One warp.
+__device__ void aed_right(cplx* M, const cplx* v, int len, cplx tau, int rows, int c0) {
+  const int lane = threadIdx.x & 31;
+  if (lane < rows) {
+    cplx w = M[lane * kAedLd + c0];
+    for (int c = 1; c < len; ++c) w = cfma(M[lane * kAedLd + c0 + c], v[c], w);
+    const cplx f = cmul(tau, w);
+    M[lane * kAedLd + c0] = csub(M[lane * kAedLd + c0], f);
+    for (int c = 1; c < len; ++c)
+      M[lane * kAedLd + c0 + c] = csub(M[lane * kAedLd + c0 + c], cmul(f, cconj(v[c])));
+  }
+  __syncwarp();
+}
+
+// Aggressive early deflation on the active block [l, i] (i - l + 1 > kAedW + 1).
+// Returns the number of deflated eigenvalues (0 when none, -1 when the window
+// did not converge and nothing was changed).  On return sm.shifts[0..cnt)
+// hold the bottom undeflated window eigenvalues, cnt <= kMsShifts, in
+// sm.aed[2].  Whole CTA.
+__device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem& sm) {
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nw = kAedW;
+  const int kw = i - nw + 1;
+  cplx* W = sm.tiles;
+  cplx* V = W + kAedW * kAedLd;
+  cplx* hv = V + kAedW * kAedLd;
+  const double ulp = 2.0 * RCWA_DBL_EPS;
+  const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
+  for (int idx = tid; idx < nw * nw; idx += nthr) {
+    const int r = idx / nw, c = idx % nw;
+    AW(r, c) = T[(size_t)(kw + r) * ldt + kw + c];
+    AV(r, c) = mkc(r == c ? 1.0 : 0.0, 0.0);
+  }
+  const cplx s = T[(size_t)kw * ldt + kw - 1];
+  __syncthreads();
+  if (tid < 32) {
+    const int lane = tid;
+    const bool ok = aed_window_schur(W, V, nw);
+    int ns = nw;
+    if (ok) {
+      // deflation test from the bottom, undeflatable eigenvalues moved up
+      int ilst = 0;
+      const double as = cabs1(s);
+      for (int knt = 0; knt < nw && ns > ilst; ++knt) {
+        double foo = cabs1(AW(ns - 1, ns - 1));
+        if (foo == 0.0) foo = as;
+        if (as * cabs1(AV(0, ns - 1)) <= fmax(smlnum, ulp * foo)) {
+          --ns;
+        } else {
+          for (int k = ns - 2; k >= ilst; --k) aed_swap(W, V, nw, k);
+          ++ilst;
+        }
+      }
+      // shifts: the bottom undeflated eigenvalues, before the reflection
+      const int cnt = min(ns, kMsShifts);
+      if (lane < cnt) sm.shifts[lane] = AW(ns - cnt + lane, ns - cnt + lane);
+      if (lane == 0) sm.aed[2] = cnt;
+      __syncwarp();
+      if (ns < nw && ns > 1 && (s.x != 0.0 || s.y != 0.0)) {
+        // reflect the spike onto its first entry
+        if (lane < ns) hv[lane] = cmul(s, cconj(AV(0, lane)));
+        __syncwarp();
+        const cplx tau = aed_house(hv, ns);
+        if (tau.x != 0.0 || tau.y != 0.0) {
+          aed_left(W, hv, ns, tau, 0, 0, nw);
+          aed_right(W, hv, ns, tau, ns, 0);
+          aed_right(V, hv, ns, tau, nw, 0);
+        }
+        // back to Hessenberg form
+        for (int j = 0; j + 2 < ns; ++j) {
+          const int len = ns - j - 1;
+          if (lane < len) hv[lane] = AW(j + 1 + lane, j);
+          __syncwarp();
+          const cplx tj = aed_house(hv, len);
+          if (tj.x != 0.0 || tj.y != 0.0) {
+            if (lane < len) AW(j + 1 + lane, j) = lane == 0 ? hv[0] : mkc(0.0, 0.0);
+            __syncwarp();
+            aed_left(W, hv, len, tj, j + 1, j + 1, nw);
+            aed_right(W, hv, len, tj, ns, j + 1);
+            aed_right(V, hv, len, tj, nw, j + 1);
+          }
+        }
+      }
+    }
+    if (lane == 0) { sm.aed[0] = ok ? 1 : 0; sm.aed[1] = ns; }
+  }
+  __syncthreads();
+  const bool ok = sm.aed[0] != 0;
+  const int ns = sm.aed[1];
+  if (!ok) return -1;
+  if (ns == nw && (s.x != 0.0 || s.y != 0.0)) return 0;
+  // window, spike and the off-window blocks
+  for (int idx = tid; idx < nw * nw; idx += nthr) {
+    const int r = idx / nw, c = idx % nw;
+    T[(size_t)(kw + r) * ldt + kw + c] = AW(r, c);
+  }
+  if (tid == 0) T[(size_t)kw * ldt + kw - 1] = cmul(s, cconj(AV(0, 0)));
+  // rows kw..i right of the window: Vh * T
+  for (int j = i + 1 + tid; j < n; j += nthr) {
+    cplx x[kAedW];
+#pragma unroll
+    for (int r = 0; r < kAedW; ++r) x[r] = T[(size_t)(kw + r) * ldt + j];
+#pragma unroll 4
+    for (int r = 0; r < kAedW; ++r) {
+      cplx acc = mkc(0.0, 0.0);
+#pragma unroll
+      for (int c = 0; c < kAedW; ++c) acc = cfmaconj(AV(c, r), x[c], acc);
+      T[(size_t)(kw + r) * ldt + j] = acc;
+    }
+  }
+  // columns kw..i above the window: T * V
+  for (int r = tid; r < kw; r += nthr) {
+    cplx x[kAedW];
+#pragma unroll
+    for (int c = 0; c < kAedW; ++c) x[c] = T[(size_t)r * ldt + kw + c];
+#pragma unroll 4
+    for (int c = 0; c < kAedW; ++c) {
+      cplx acc = mkc(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < kAedW; ++k) acc = cfma(x[k], AV(k, c), acc);
+      T[(size_t)r * ldt + kw + c] = acc;
+    }
+  }
+  // Schur vectors (column-major): Z(:, kw..i) * V
+  for (int r = tid; r < n; r += nthr) {
+    cplx x[kAedW];
+#pragma unroll
+    for (int c = 0; c < kAedW; ++c) x[c] = Z[(size_t)(kw + c) * n + r];
+#pragma unroll 4
+    for (int c = 0; c < kAedW; ++c) {
+      cplx acc = mkc(0.0, 0.0);
+#pragma unroll
+      for (int k = 0; k < kAedW; ++k) acc = cfma(x[k], AV(k, c), acc);
+      Z[(size_t)(kw + c) * n + r] = acc;
+    }
+  }
+  __syncthreads();
+  return nw - ns;
+}
+
+#undef AW
+#undef AV
 
 // One multishift sweep over the active block [l, i] with sm.shifts[0..s).
 // Bulge b sits at position p = l + t - 3b at chain step t; it is active while
@@ -876,26 +1165,45 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
       if (++sweeps > budget) return RCWA_ERR_NOCONV;
       continue;
     }
-    const int s = kMsShifts;
+    // aggressive early deflation on the trailing window; its undeflated
+    // eigenvalues are the next sweep's shifts
+    int s = kMsShifts, ib = i;
+    bool have_shifts = false;
+    {
+      const int nd = aed(T, ldt, Z, n, l, i, sm);
+      if (nd > 0) {
+        stall = 0;
+        if (100 * nd > kAedNibble * kAedW || i - nd - l + 1 < kMsMin) {
+          if (++sweeps > budget) return RCWA_ERR_NOCONV;
+          continue;
+        }
+        ib = i - nd;
+      }
+      if (nd >= 0 && sm.aed[2] >= kMsShifts / 2) {
+        s = sm.aed[2];
+        have_shifts = true;
+      }
+    }
+    __syncthreads();
     {
       STAT_ADD(0, 1);
       if (tid < 32) {
         cplx* B = sm.tiles;  // s x s, stride s + 1
-        const int o = i - s + 1;
-        for (int idx = tid; idx < s * s; idx += 32)
-          B[(idx / s) * (s + 1) + idx % s] = T[(size_t)(o + idx / s) * ldt + o + idx % s];
-        __syncwarp();
+        const int o = ib - s + 1;
         if (stall > 0 && stall % 6 == 0) {
           for (int k = tid; k < s; k += 32)
-            sm.shifts[k] = cadd(B[k * (s + 1) + k],
+            sm.shifts[k] = cadd(T[(size_t)(o + k) * ldt + o + k],
                                 mkc(0.75 * cabs1(T[(size_t)(o + k) * ldt + o + k - 1]), 0.0));
-        } else {
+        } else if (!have_shifts) {
+          for (int idx = tid; idx < s * s; idx += 32)
+            B[(idx / s) * (s + 1) + idx % s] = T[(size_t)(o + idx / s) * ldt + o + idx % s];
+          __syncwarp();
           small_eigs_warp(B, s + 1, s, sm.shifts);
         }
       }
     }
     __syncthreads();
-    ms_sweep(T, ldt, Z, n, l, i, s, sm);
+    ms_sweep(T, ldt, Z, n, l, ib, s, sm);
     if (++sweeps > budget) return RCWA_ERR_NOCONV;
   }
   return 0;
