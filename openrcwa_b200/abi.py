@@ -355,6 +355,11 @@ class Plan:
     def launch_count(self):
         return int(self.eng.lib.rcwa_plan_launch_count(self.h))
 
+    def rescatter(self, pxy):
+        """New incident polarisations (n_pts, n_exc, 2) on the kept S-matrices."""
+        pxy = np.ascontiguousarray(pxy, dtype=np.complex128).reshape(self.n_pts, self.n_exc, 2)
+        self.eng._check(self.eng.lib.rcwa_plan_rescatter(self.h, _v(pxy)), "plan_rescatter")
+
     def set_profiling(self, on=True):
         self.eng._check(self.eng.lib.rcwa_plan_set_profiling(self.h, 1 if on else 0), "set_profiling")
 

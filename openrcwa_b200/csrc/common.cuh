@@ -110,12 +110,22 @@ struct StageProf {
     }
     used = 0;
     stage[used] = -1;
-    cudaEventRecord(ev[used++], st);
+    record(ev[used++], st);
   }
   void mark(cudaStream_t st, int s) {
     if (!on || used >= 8192) return;
     stage[used] = s;
-    cudaEventRecord(ev[used++], st);
+    record(ev[used++], st);
+  }
+  // While the stream is being captured into a graph the record becomes an
+  // external event node, so stage times also come out of graph launches (the
+  // external flag is only valid during capture).
+  static void record(cudaEvent_t e, cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusActive)
+      cudaEventRecordWithFlags(e, st, cudaEventRecordExternal);
+    else
+      cudaEventRecord(e, st);
   }
   void collect(double* ms_per_stage) {
     for (int i = 0; i < kStCount; ++i) ms_per_stage[i] = 0.0;

@@ -37,7 +37,8 @@ constexpr double kPi = 3.1415926535897932;
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
-  ~DevBuf() { if (p) cudaFree(p); }
+  bool borrowed = false;  // the engine's cached workspace, not freed here
+  ~DevBuf() { if (p && !borrowed) cudaFree(p); }
 };
 
 // Bump allocator over byte offsets; turned into addresses once the base exists.
@@ -95,6 +96,17 @@ struct rcwa_plan {
   std::vector<ScatterItem> scatter_items;
   size_t scatter_meta = 0;
   int scatter_N = 0, scatter_nx = 0, scatter_ny = 0;
+  // launch sequence as a CUDA graph, captured on the second execution
+  cudaGraphExec_t graph_exec = nullptr;
+  bool graph_prof = false;   // the graph holds the stage-timing event records
+  long long graph_launches = 0;
+  long long executions = 0;
+  ~rcwa_plan() {
+    // kernels of this plan may still run on a caller's stream
+    if (graph_exec || work.borrowed) cudaDeviceSynchronize();
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (work.borrowed && e) e->work_cache_busy = false;
+  }
 };
 
 namespace {
@@ -209,6 +221,7 @@ int rcwa_engine_create(int device, rcwa_engine** out) {
 void rcwa_engine_destroy(rcwa_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
+  if (e->work_cache) cudaFree(e->work_cache);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
 }
@@ -378,6 +391,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   // ---- chunking: group by (nx, ny), then fill chunks up to the memory budget
   size_t free_b = 0, total_b = 0;
   cudaMemGetInfo(&free_b, &total_b);
+  if (!e->work_cache_busy) free_b += e->work_cache_bytes;
   const size_t budget = std::min<size_t>((size_t)(0.6 * free_b), (size_t)96 << 30);
   std::map<std::pair<int, int>, std::vector<int>> groups;
   for (int p = 0; p < n_pts; ++p) groups[{si[pts[p].stack].nx, si[pts[p].stack].ny}].push_back(p);
@@ -421,8 +435,25 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   }
   size_t wbytes = 0;
   for (size_t ci = 0; ci < chunks.size(); ++ci) wbytes = std::max(wbytes, chunk_layout(chunks[ci], si, chunk_N[ci]));
-  if (cudaMalloc(&P->work.p, std::max<size_t>(wbytes, 256)) != cudaSuccess)
+  const size_t wneed = std::max<size_t>(wbytes, 256);
+  if (!e->work_cache_busy) {
+    if (e->work_cache_bytes < wneed) {
+      if (e->work_cache) cudaFree(e->work_cache);
+      e->work_cache = nullptr;
+      e->work_cache_bytes = 0;
+      if (cudaMalloc(&e->work_cache, wneed) != cudaSuccess) {
+        e->work_cache = nullptr;
+        return fail(e, RCWA_ERR_NOMEM, "workspace allocation failed (" + std::to_string(wbytes >> 20) + " MiB)");
+      }
+      e->work_cache_bytes = wneed;
+    }
+    P->work.p = e->work_cache;
+    P->work.borrowed = true;
+    e->work_cache_busy = true;
+  } else if (cudaMalloc(&P->work.p, wneed) != cudaSuccess) {
+    P->work.p = nullptr;
     return fail(e, RCWA_ERR_NOMEM, "workspace allocation failed (" + std::to_string(wbytes >> 20) + " MiB)");
+  }
   P->work.bytes = wbytes;
   char* wb = (char*)P->work.p;
 
@@ -831,16 +862,61 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   return RCWA_OK;
 }
 
+namespace {
+// The plan's launch sequence on stream st (status reset, then every step).
+cudaError_t issue_plan(rcwa_plan* p, cudaStream_t st) {
+  long long nl = 0;
+  cudaError_t err = cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st);
+  p->prof->begin(st);
+  for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, nl, *p->prof);
+  return err;
+}
+}  // namespace
+
+// The first execution launches the kernels directly; from the second on the
+// sequence is captured once into a CUDA graph (with the stage-timing event
+// records when profiling is on) and the graph is launched, so repeated sweeps
+// pay one launch instead of thousands.
 extern "C" int rcwa_plan_execute(rcwa_plan* p, void* stream) {
   if (!p) return RCWA_ERR_INVALID;
   cudaStream_t st = stream ? (cudaStream_t)stream : p->e->stream;
   if (cudaSetDevice(p->e->device) != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, "cudaSetDevice failed");
-  long long nl = 0;
   const long long launches0 = launch_counter();
-  cudaError_t err = cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st);
-  p->prof->begin(st);
-  for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, nl, *p->prof);
-  p->launches = launch_counter() - launches0;
+  cudaError_t err = cudaSuccess;
+  const bool graph = p->executions > 0;
+  if (graph && p->graph_exec && p->graph_prof != p->prof->on) {
+    // recapture with or without the stage-timing event nodes
+    cudaDeviceSynchronize();
+    cudaGraphExecDestroy(p->graph_exec);
+    p->graph_exec = nullptr;
+  }
+  if (graph && !p->graph_exec) {
+    p->graph_prof = p->prof->on;
+    cudaGraph_t g = nullptr;
+    // the previous execution's event records must have completed
+    err = cudaStreamSynchronize(st);
+    if (err == cudaSuccess) err = cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed);
+    if (err == cudaSuccess) {
+      cudaError_t ierr = issue_plan(p, st);
+      err = cudaStreamEndCapture(st, &g);
+      if (ierr != cudaSuccess) err = ierr;
+    }
+    if (err == cudaSuccess) err = cudaGraphInstantiate(&p->graph_exec, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (err != cudaSuccess) {
+      p->graph_exec = nullptr;
+      return fail(p->e, RCWA_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(err));
+    }
+    p->graph_launches = launch_counter() - launches0;
+  }
+  if (graph) {
+    err = cudaGraphLaunch(p->graph_exec, st);
+    p->launches = p->graph_launches;
+  } else {
+    err = issue_plan(p, st);
+    p->launches = launch_counter() - launches0;
+  }
+  ++p->executions;
   if (err != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, std::string("launch failed: ") + cudaGetErrorString(err));
   return RCWA_OK;
 }

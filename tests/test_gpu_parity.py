@@ -229,3 +229,30 @@ def test_large_orders_panel_lu_path(eng):
     setup = OfdSetup(nHx=4, period_x=4e-7, nHy=4, period_y=4e-7, layers=layers,
                      freqs=orc.C0 / np.array([450e-9, 700e-9]), theta=35.0, phi=20.0)
     _cmp_ofd(eng, setup)
+
+
+def test_plan_graph_replay_and_rescatter(eng):
+    # first execution launches directly, later ones replay a captured CUDA
+    # graph (recaptured when stage profiling is switched); all bit-identical
+    import openrcwa_b200 as o
+    from openrcwa_b200 import workloads
+    stacks, pts, pxy = workloads.pillars_2d(seed=3, nH=3)
+    bp, bx = workloads.batch_slice(pts, pxy, 0, 6)
+    plan = eng.plan(stacks, bp, bx)
+    outs = []
+    for prof in (True, True, True, False, False, True, False):
+        plan.set_profiling(prof)
+        plan.execute()
+        outs.append(plan.results(orders=True))
+    for r in outs[1:]:
+        for a, b in zip(outs[0], r):
+            assert np.array_equal(a, b)
+    assert plan.launch_count() > 0
+    # rescatter: swap TE/TM and compare with a fresh solve
+    bx2 = np.ascontiguousarray(bx[:, ::-1, :])
+    plan.rescatter(bx2)
+    R, T, _, _, st = plan.results()
+    R2, T2, _, _, st2 = eng.solve_batch(stacks, bp, bx2, orders=False)
+    assert not np.any(st) and not np.any(st2)
+    assert np.max(np.abs(R - R2)) < 1e-12 and np.max(np.abs(T - T2)) < 1e-12
+    plan.close()
