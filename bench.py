@@ -269,6 +269,9 @@ def main():
     t_ms = allmax(e0.elapsed_time(e1))
     launches = plan.launch_count() * args.steps
     value = world * B * args.steps / (t_ms * 1e-3)
+    # release the plan (and with it the engine's cached workspace) so that the
+    # end-to-end calls below find the workspace free, as a caller's would
+    plan.close()
 
     # e2e: the public C ABI with host buffers, a different batch each step
     barrier()

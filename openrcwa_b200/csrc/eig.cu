@@ -183,17 +183,26 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       }
       if (tid == 0) { s.tau[j] = tau; s.v0[j] = v0; }
       __syncthreads();
-      // u = A0(:, j+1:) v_j (one pass over the trailing columns), z = V(:, :jj)^H v_j
+      // u = A0(:, j+1:) v_j (one pass over the trailing columns), z = V(:, :jj)^H v_j.
+      // The pass streams the trailing matrix from DRAM; eight independent
+      // loads per lane keep enough bytes in flight to cover the latency.
       for (int i = wid; i < n; i += nw) {
         const cplx* row = A + (size_t)i * lda;
-        cplx acc0 = mkc(0.0, 0.0), acc1 = mkc(0.0, 0.0);
+        cplx acc[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) acc[q] = mkc(0.0, 0.0);
         int c = j + 1 + lane;
-        for (; c + 32 < n; c += 64) {
-          acc0 = cfma(row[c], a[c], acc0);
-          acc1 = cfma(row[c + 32], a[c + 32], acc1);
+        for (; c + 224 < n; c += 256) {
+          cplx r[8];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) r[q] = row[c + 32 * q];
+#pragma unroll
+          for (int q = 0; q < 8; ++q) acc[q] = cfma(r[q], a[c + 32 * q], acc[q]);
         }
-        if (c < n) acc0 = cfma(row[c], a[c], acc0);
-        acc0 = cadd(acc0, acc1);
+        for (; c < n; c += 32) acc[0] = cfma(row[c], a[c], acc[0]);
+        cplx acc0 = acc[0];
+#pragma unroll
+        for (int q = 1; q < 8; ++q) acc0 = cadd(acc0, acc[q]);
         for (int off = 16; off > 0; off >>= 1) {
           acc0.x += __shfl_xor_sync(0xffffffffu, acc0.x, off);
           acc0.y += __shfl_xor_sync(0xffffffffu, acc0.y, off);
@@ -1222,30 +1231,82 @@ __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr,
 }
 
 // ---------------------------------------------------------------- eigenvectors
-__device__ void trevc(const cplx* T, int ldt, cplx* X, int n) {
+// Eigenvectors of the upper triangular T (LAPACK ztrevc, right vectors, back
+// substitution with protected divisors): column k of X solves
+// (T - t_kk I) x = 0 with x_k = 1 and x_j = 0 for j > k.  Blocked bottom-up
+// over 64-row blocks [r0, r1): the coupling to the rows already solved,
+// B = T(r0:r1, r1:) X(r1:, k), is a tile GEMM over the upper triangle of X
+// (column tile by column tile, K cut at the tile's last column); the block
+// itself is solved by one thread per column in two 32-row halves held in
+// registers.
+constexpr int kTrBlk = 64;
+
+template <int R>
+__device__ __forceinline__ void trevc_half(const cplx* T, int ldt, cplx* X, int n, int k, int h0, int hend,
+                                           cplx tkk, double ulp, double smlnum, cplx (&x)[R]) {
+  // rows h0 .. h0+R-1 (those < hend); X(i, k) holds the right-hand side
+  const double smin = fmax(ulp * cabs1(tkk), smlnum);
+#pragma unroll
+  for (int ii = R - 1; ii >= 0; --ii) {
+    const int i = h0 + ii;
+    cplx xi = mkc(0.0, 0.0);
+    if (i < hend) {
+      if (i == k) {
+        xi = mkc(1.0, 0.0);
+      } else if (i < k) {
+        cplx acc = X[(size_t)i * n + k];
+#pragma unroll
+        for (int jj = ii + 1; jj < R; ++jj) acc = cfma(__ldg(&T[(size_t)i * ldt + h0 + jj]), x[jj], acc);
+        cplx d = csub(__ldg(&T[(size_t)i * ldt + i]), tkk);
+        if (cabs1(d) < smin) d = mkc(smin, 0.0);
+        xi = cneg(cdiv(acc, d));
+      }
+      X[(size_t)i * n + k] = xi;
+    }
+    x[ii] = xi;
+  }
+}
+
+__device__ void trevc_blocked(const cplx* T, int ldt, cplx* X, int n, TileSmem& tsm) {
   const double ulp = 2.0 * RCWA_DBL_EPS;
   const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
-  for (size_t idx = threadIdx.x; idx < (size_t)n * n; idx += blockDim.x) {
-    const int i = (int)(idx / n), k = (int)(idx % n);
-    if (i >= k) X[idx] = mkc(i == k ? 1.0 : 0.0, 0.0);
-  }
+  // X = 0 everywhere but the unit diagonal; rows are overwritten block by block
+  for (size_t idx = threadIdx.x; idx < (size_t)n * n; idx += blockDim.x)
+    X[idx] = mkc((idx / n) == (idx % n) ? 1.0 : 0.0, 0.0);
   __syncthreads();
-  // column k of X is owned by thread k % blockDim.x for the whole sweep, so
-  // its earlier entries are always the thread's own writes
-  for (int i = n - 2; i >= 0; --i) {
-    const cplx tii = T[(size_t)i * ldt + i];
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-      if (k <= i) continue;
-      cplx acc = T[(size_t)i * ldt + k];
-      for (int j = i + 1; j < k; ++j) acc = cfma(T[(size_t)i * ldt + j], X[(size_t)j * n + k], acc);
-      const cplx tkk = T[(size_t)k * ldt + k];
-      const double smin = fmax(ulp * cabs1(tkk), smlnum);
-      cplx d = csub(tii, tkk);
-      if (cabs1(d) < smin) d = mkc(smin, 0.0);
-      X[(size_t)i * n + k] = cneg(cdiv(acc, d));
+  const int nblk = (n + kTrBlk - 1) / kTrBlk;
+  for (int bi = nblk - 1; bi >= 0; --bi) {
+    const int r0 = bi * kTrBlk, r1 = min(n, r0 + kTrBlk);
+    // B(r0:r1, c) = sum_{j >= r1} T(r0:r1, j) X(j, c) for columns c >= r1;
+    // X(j, c) = 0 for j > c, so the tile of columns [c0, c0+64) needs j < c0+64
+    for (int c0 = r1; c0 < n; c0 += kTBN) {
+      const int nc = min(kTBN, n - c0);
+      const int K = min(n, c0 + nc) - r1;
+      cta_gemm<false, false>(tsm, r1 - r0, nc, K, T + (size_t)r0 * ldt + r1, ldt, X + (size_t)r1 * n + c0, n,
+                             X + (size_t)r0 * n + c0, n, nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
     }
+    // columns k > r0 solve the block rows; columns inside the block start
+    // from a zero right-hand side (X(i, k) = 0 for i < k there)
+    for (int k = r0 + 1 + threadIdx.x; k < n; k += blockDim.x) {
+      const cplx tkk = __ldg(&T[(size_t)k * ldt + k]);
+      cplx xl[32], xh[32];
+      // lower half [r0+32, r1)
+      trevc_half<32>(T, ldt, X, n, k, r0 + 32, r1, tkk, ulp, smlnum, xh);
+      // the lower half's contribution to the upper half's right-hand side
+      if (k > r0) {
+        for (int ii = 0; ii < 32 && r0 + ii < min(k, r1); ++ii) {
+          const int i = r0 + ii;
+          cplx acc = X[(size_t)i * n + k];
+#pragma unroll
+          for (int jj = 0; jj < 32; ++jj)
+            if (r0 + 32 + jj < r1) acc = cfma(__ldg(&T[(size_t)i * ldt + r0 + 32 + jj]), xh[jj], acc);
+          X[(size_t)i * n + k] = acc;
+        }
+      }
+      trevc_half<32>(T, ldt, X, n, k, r0, min(r1, r0 + 32), tkk, ulp, smlnum, xl);
+    }
+    __syncthreads();
   }
-  __syncthreads();
 }
 
 __global__ void __launch_bounds__(kEigThreads) hessenberg_kernel(cplx* const* Aarr, int n, int lda, void* work) {
@@ -1270,8 +1331,9 @@ __global__ void __launch_bounds__(kEigThreads) schur_kernel(cplx* const* Aarr, i
 }
 
 __global__ void __launch_bounds__(kEigThreads) trevc_kernel(cplx* const* Aarr, int n, int lda, void* work) {
+  __shared__ TileSmem tsm;
   const Scratch s = scratch_for(work, n, blockIdx.x);
-  trevc(Aarr[blockIdx.x], lda, s.X, n);
+  trevc_blocked(Aarr[blockIdx.x], lda, s.X, n, tsm);
 }
 
 // unit 2-norm columns; non-finite eigenpairs flag the matrix

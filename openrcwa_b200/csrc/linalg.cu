@@ -173,7 +173,18 @@ __global__ void __launch_bounds__(64) getrf_trsm_kernel(cplx* const* Aarr, int n
   lu_trsm_cols(A, n, lda, kb, jb, kb + jb + blockIdx.x * 64 + threadIdx.x, Lsm);
 }
 
-// Blocked LU solve: one CTA per (matrix, 64-column block of B).
+// Blocked LU solve, left-looking: one CTA per (matrix, 64-column slab of B).
+// Each 64-row block of the slab first takes the contribution of all rows
+// already solved as one long-K tile GEMM (L(rb:, :rb) X(:rb) forward,
+// U(rb:, re:) X(re:) backward), then its diagonal block is solved in two
+// 32-row halves, one thread per column with the column in registers.
+__device__ __forceinline__ void load_block32(cplx (*Tsm)[33], const cplx* LU, int lda, int r0, int c0, int h, int w) {
+  for (int idx = threadIdx.x; idx < h * w; idx += blockDim.x) {
+    const int r = idx / w, q = idx % w;
+    Tsm[r][q] = LU[(size_t)(r0 + r) * lda + c0 + q];
+  }
+}
+
 __global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const* LUarr, int n, int lda,
                                                              const int* ipiv_all, cplx* const* Barr,
                                                              int nrhs, int ldb) {
@@ -199,58 +210,91 @@ __global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const*
   }
   __syncthreads();
   // forward substitution with the unit lower factor
-  for (int rb = 0; rb < n; rb += 32) {
-    const int rw = min(32, n - rb);
-    for (int idx = tid; idx < rw * rw; idx += kTileThreads)
-      Tsm[idx / rw][idx % rw] = LU[(size_t)(rb + idx / rw) * lda + rb + idx % rw];
-    __syncthreads();
-    if (tid < cw) {
-      for (int r = 1; r < rw; ++r) {
-        cplx x = B[(size_t)(rb + r) * ldb + tid];
-        for (int q = 0; q < r; ++q) x = cfma(cneg(Tsm[r][q]), B[(size_t)(rb + q) * ldb + tid], x);
-        B[(size_t)(rb + r) * ldb + tid] = x;
-      }
+  for (int rb = 0; rb < n; rb += 64) {
+    const int rw = min(64, n - rb);
+    if (rb > 0) {
+      cplx acc[4][4];
+      tile_zero(acc);
+      tile_mma<false, false>(sm, acc, LU + (size_t)rb * lda, lda, B, ldb, nullptr, rw, cw, rb, 0, 0);
+      tile_store(acc, B + (size_t)rb * ldb, ldb, B + (size_t)rb * ldb, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0),
+                 mkc(0.0, 0.0), rw, cw, 0, 0);
+      __syncthreads();
     }
-    __syncthreads();
-    const int m2 = n - rb - rw;
-    if (m2 > 0) {
-      const cplx* L21 = LU + (size_t)(rb + rw) * lda + rb;
-      const cplx* X = B + (size_t)rb * ldb;
-      cplx* B2 = B + (size_t)(rb + rw) * ldb;
-      for (int tm = 0; tm < m2; tm += kTBM) {
-        cplx acc[4][4];
-        tile_zero(acc);
-        tile_mma<false, false>(sm, acc, L21, lda, X, ldb, nullptr, m2, cw, rw, tm, 0);
-        tile_store(acc, B2, ldb, B2, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0), mkc(0.0, 0.0), m2, cw, tm, 0);
+    for (int h0 = rb; h0 < rb + rw; h0 += 32) {
+      const int hw = min(32, rb + rw - h0);
+      if (h0 > rb) {
+        // the first half of the block feeds the second
+        load_block32(Tsm, LU, lda, h0, rb, hw, 32);
+        __syncthreads();
+        if (tid < cw) {
+          cplx x[32];
+#pragma unroll
+          for (int q = 0; q < 32; ++q) x[q] = B[(size_t)(rb + q) * ldb + tid];
+          for (int r = 0; r < hw; ++r) {
+            cplx acc = B[(size_t)(h0 + r) * ldb + tid];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) acc = cfma(cneg(Tsm[r][q]), x[q], acc);
+            B[(size_t)(h0 + r) * ldb + tid] = acc;
+          }
+        }
+        __syncthreads();
       }
+      load_block32(Tsm, LU, lda, h0, h0, hw, hw);
+      __syncthreads();
+      if (tid < cw) {
+        // the column's solved entries are re-read from L1
+        for (int r = 1; r < hw; ++r) {
+          cplx acc = B[(size_t)(h0 + r) * ldb + tid];
+          for (int q = 0; q < r; ++q) acc = cfma(cneg(Tsm[r][q]), B[(size_t)(h0 + q) * ldb + tid], acc);
+          B[(size_t)(h0 + r) * ldb + tid] = acc;
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
   // back substitution with the upper factor
-  for (int rb = ((n - 1) / 32) * 32; rb >= 0; rb -= 32) {
-    const int rw = min(32, n - rb);
-    for (int idx = tid; idx < rw * rw; idx += kTileThreads)
-      Tsm[idx / rw][idx % rw] = LU[(size_t)(rb + idx / rw) * lda + rb + idx % rw];
-    __syncthreads();
-    if (tid < cw) {
-      for (int r = rw - 1; r >= 0; --r) {
-        cplx x = B[(size_t)(rb + r) * ldb + tid];
-        for (int q = r + 1; q < rw; ++q) x = cfma(cneg(Tsm[r][q]), B[(size_t)(rb + q) * ldb + tid], x);
-        B[(size_t)(rb + r) * ldb + tid] = cdiv(x, Tsm[r][r]);
-      }
+  for (int rb = ((n - 1) / 64) * 64; rb >= 0; rb -= 64) {
+    const int re = min(n, rb + 64), rw = re - rb;
+    if (re < n) {
+      cplx acc[4][4];
+      tile_zero(acc);
+      tile_mma<false, false>(sm, acc, LU + (size_t)rb * lda + re, lda, B + (size_t)re * ldb, ldb, nullptr, rw, cw,
+                             n - re, 0, 0);
+      tile_store(acc, B + (size_t)rb * ldb, ldb, B + (size_t)rb * ldb, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0),
+                 mkc(0.0, 0.0), rw, cw, 0, 0);
+      __syncthreads();
     }
-    __syncthreads();
-    if (rb > 0) {
-      const cplx* U01 = LU + rb;
-      const cplx* X = B + (size_t)rb * ldb;
-      for (int tm = 0; tm < rb; tm += kTBM) {
-        cplx acc[4][4];
-        tile_zero(acc);
-        tile_mma<false, false>(sm, acc, U01, lda, X, ldb, nullptr, rb, cw, rw, tm, 0);
-        tile_store(acc, B, ldb, B, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0), mkc(0.0, 0.0), rb, cw, tm, 0);
+    for (int h0 = (rw > 32) ? rb + 32 : rb; h0 >= rb; h0 -= 32) {
+      const int hw = min(32, re - h0);
+      const int tail = re - h0 - hw;  // rows of this block below the half, already solved
+      if (tail > 0) {
+        load_block32(Tsm, LU, lda, h0, h0 + hw, hw, tail);
+        __syncthreads();
+        if (tid < cw) {
+          cplx x[32];
+#pragma unroll
+          for (int q = 0; q < 32; ++q) x[q] = q < tail ? B[(size_t)(h0 + hw + q) * ldb + tid] : mkc(0.0, 0.0);
+          for (int r = 0; r < hw; ++r) {
+            cplx acc = B[(size_t)(h0 + r) * ldb + tid];
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+              if (q < tail) acc = cfma(cneg(Tsm[r][q]), x[q], acc);
+            B[(size_t)(h0 + r) * ldb + tid] = acc;
+          }
+        }
+        __syncthreads();
       }
+      load_block32(Tsm, LU, lda, h0, h0, hw, hw);
+      __syncthreads();
+      if (tid < cw) {
+        for (int r = hw - 1; r >= 0; --r) {
+          cplx acc = B[(size_t)(h0 + r) * ldb + tid];
+          for (int q = r + 1; q < hw; ++q) acc = cfma(cneg(Tsm[r][q]), B[(size_t)(h0 + q) * ldb + tid], acc);
+          B[(size_t)(h0 + r) * ldb + tid] = cdiv(acc, Tsm[r][r]);
+        }
+      }
+      __syncthreads();
     }
-    __syncthreads();
   }
 }
 
