@@ -93,7 +93,7 @@ inline long long& launch_counter() {
 enum RcwaStage {
   kStConvTables = 0, kStConvGather, kStConvInverse, kStPQGemm, kStAssemble, kStHessenberg, kStSchur,
   kStTrevc, kStBackTransform, kStNormalize, kStModes, kStHalfspace, kStInterface, kStPhase, kStCascadeGemm,
-  kStTau, kStScatter, kStCount
+  kStTau, kStScatter, kStInterfaceLU, kStTauLU, kStCount
 };
 
 struct StageProf {

@@ -766,9 +766,11 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           cudaError_t err;
           // interface matrices IE = Wa^-1 Wb, IH = Va^-1 Vb (rcwa/RCWASolver.cpp:537-543)
           if ((err = zcopy_batched(cpa(ocs), n, pa(ocd), n, n, n, 4 * k, st)) != cudaSuccess) return err;
+          pf.mark(st, kStInterface);
           if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * k, st)) != cudaSuccess) return err;
           if ((err = fold_info(pinfo, (const int*)(m + oip), 2 * k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
+          pf.mark(st, kStInterfaceLU);
           if ((err = zgetrs_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * k, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
           if (nph > 0) {
@@ -791,9 +793,11 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           // tau = (F + G)^-1  (:451-453)
           if ((err = zaxpby_batched(cpa(osF), cpa(osG), pa(osD), mkc(1, 0), mkc(1, 0), n, k, st)) != cudaSuccess)
             return err;
+          pf.mark(st, kStTau);
           if ((err = zgetrf_batched(pa(oSp), n, n, pipiv, pinfo, k, st)) != cudaSuccess) return err;
           if ((err = fold_info(pinfo, (const int*)(m + osp), k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
+          pf.mark(st, kStTauLU);
           if ((err = zset_identity_batched(pa(otau), n, n, k, st)) != cudaSuccess) return err;
           if ((err = zgetrs_batched(cpa(oSp), n, n, pipiv, pa(otau), n, n, k, st)) != cudaSuccess) return err;
           pf.mark(st, kStTau);
@@ -969,7 +973,7 @@ extern "C" const char* rcwa_stage_name(int stage) {
   static const char* names[kStCount] = {"conv_tables", "conv_gather", "conv_inverse", "pq_gemm", "assemble_pq",
                                         "hessenberg", "schur_qr", "trevc", "eig_backtransform", "eig_normalize",
                                         "modes_v", "halfspace", "interface_lu_solve", "phase", "cascade_gemm",
-                                        "tau_inverse", "scatter"};
+                                        "tau_inverse", "scatter", "interface_getrf", "tau_getrf"};
   return (stage >= 0 && stage < kStCount) ? names[stage] : "";
 }
 
