@@ -41,8 +41,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=29, help="solve points per step per GPU (29 x 5 layers = 145 "
-                    "eigensolves, one wave on 148 SMs)")
+    ap.add_argument("--batch", type=int, default=145, help="solve points per step per GPU (145 x 5 layers = 725 "
+                    "eigensolves, about five waves on 148 SMs; the interface and tau factorisations then "
+                    "fill the GPU too)")
     ap.add_argument("--nh", type=int, default=10, help="harmonics per axis (Nx=Ny)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",

@@ -503,8 +503,9 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
 }
 
 #ifdef RCWA_EIG_STATS
-// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles
-__device__ unsigned long long g_eig_stats[8];
+// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles,
+// 8 early-deflation cycles, 9 single-shift cycles, 10 Schur cycles, 11 early deflations, 12 deflated by them
+__device__ unsigned long long g_eig_stats[16];
 #define STAT_ADD(i, v) do { if (threadIdx.x == 0) atomicAdd(&g_eig_stats[i], (unsigned long long)(v)); } while (0)
 #else
 #define STAT_ADD(i, v) do { } while (0)
@@ -1170,7 +1171,13 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
                                 T[(size_t)i * ldt + i - 1], T[(size_t)i * ldt + i]);
       __syncthreads();
       STAT_ADD(1, 1);
+#ifdef RCWA_EIG_STATS
+      const long long c_ss = clock64();
+#endif
       qr_sweep(T, ldt, Z, n, l, i, shift, reinterpret_cast<cplx(*)[kWin + 1]>(sm.Wt), sm.lc, sm.ls);
+#ifdef RCWA_EIG_STATS
+      STAT_ADD(9, clock64() - c_ss);
+#endif
       if (++sweeps > budget) return RCWA_ERR_NOCONV;
       continue;
     }
@@ -1179,7 +1186,15 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
     int s = kMsShifts, ib = i;
     bool have_shifts = false;
     {
+#ifdef RCWA_EIG_STATS
+      const long long c_aed = clock64();
+#endif
       const int nd = aed(T, ldt, Z, n, l, i, sm);
+#ifdef RCWA_EIG_STATS
+      STAT_ADD(8, clock64() - c_aed);
+      STAT_ADD(11, 1);
+      STAT_ADD(12, nd > 0 ? nd : 0);
+#endif
       if (nd > 0) {
         stall = 0;
         if (100 * nd > kAedNibble * kAedW || i - nd - l + 1 < kMsMin) {
@@ -1224,7 +1239,13 @@ __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr,
   const MsSmem sm = carve_ms_smem(dsm);
   cplx* A = Aarr[blockIdx.x];
   const Scratch s = scratch_for(work, n, blockIdx.x);
+#ifdef RCWA_EIG_STATS
+  const long long c_schur = clock64();
+#endif
   const int status = schur_ms(A, lda, s.Z, n, sm);
+#ifdef RCWA_EIG_STATS
+  STAT_ADD(10, clock64() - c_schur);
+#endif
   cplx* w = w_all + (size_t)blockIdx.x * n;
   for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = A[(size_t)k * lda + k];
   if (threadIdx.x == 0) info_all[blockIdx.x] = status;
@@ -1408,11 +1429,11 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
 
 #ifdef RCWA_EIG_STATS
 extern "C" int rcwa_debug_eig_stats(unsigned long long* out, int reset) {
-  unsigned long long h[8];
+  unsigned long long h[16];
   if (cudaMemcpyFromSymbol(h, g_eig_stats, sizeof(h)) != cudaSuccess) return 2;
-  for (int i = 0; i < 8; ++i) out[i] = h[i];
+  for (int i = 0; i < 16; ++i) out[i] = h[i];
   if (reset) {
-    unsigned long long z[8] = {};
+    unsigned long long z[16] = {};
     cudaMemcpyToSymbol(g_eig_stats, z, sizeof(z));
   }
   return 0;

@@ -35,20 +35,33 @@ __global__ void __launch_bounds__(kTileThreads) zgemm_kernel(GemmArgs g) {
 // kb .. n-1), LAPACK getf2 order: pivot = largest |re|+|im| in the column
 // (first index on ties), the pivot rows are interchanged across all n columns,
 // the column is scaled by the reciprocal pivot and the rest of the panel gets
-// the rank-1 update.  Whole CTA; info keeps the first exactly-zero pivot.
+// the rank-1 update.  The update reads the pivot row from shared memory and
+// issues the loads of eight elements before their stores, so a thread keeps
+// eight L2 requests in flight instead of one; it also tracks the largest
+// entry of the next column, which is that column's pivot search.  Whole CTA;
+// info keeps the first exactly-zero pivot.
 __device__ void lu_panel(cplx* A, int n, int lda, int kb, int jb, int* ipiv, int& info, double* red_v, int* red_i,
-                         int* s_piv) {
+                         int* s_piv, cplx* prow) {
   const int tid = threadIdx.x, nthr = blockDim.x;
-  for (int j = kb; j < kb + jb; ++j) {
-    double best = -1.0;
-    int bi = j;
-    for (int i = j + tid; i < n; i += nthr) {
-      double v = cabs1(A[(size_t)i * lda + j]);
-      if (v > best) { best = v; bi = i; }
+  constexpr int kU = 8;
+  double best = -1.0;
+  int bi = kb;
+  for (int i0 = kb + tid; i0 < n; i0 += kU * nthr) {
+    double v[kU];
+#pragma unroll
+    for (int q = 0; q < kU; ++q) {
+      const int i = i0 + q * nthr;
+      v[q] = i < n ? cabs1(A[(size_t)i * lda + kb]) : -1.0;
     }
+#pragma unroll
+    for (int q = 0; q < kU; ++q)
+      if (v[q] > best) { best = v[q]; bi = i0 + q * nthr; }
+  }
+  const int ce = kb + jb;  // panel end (exclusive)
+  for (int j = kb; j < ce; ++j) {
     for (int off = 16; off > 0; off >>= 1) {
-      double ov = __shfl_down_sync(0xffffffffu, best, off);
-      int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      const double ov = __shfl_down_sync(0xffffffffu, best, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
       if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
     }
     if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
@@ -71,20 +84,57 @@ __device__ void lu_panel(cplx* A, int n, int lda, int kb, int jb, int* ipiv, int
       }
     }
     __syncthreads();
-    const cplx piv = A[(size_t)j * lda + j];
+    for (int c = j + tid; c < ce; c += nthr) prow[c - kb] = A[(size_t)j * lda + c];
+    __syncthreads();
+    const cplx piv = prow[j - kb];
     if (piv.x == 0.0 && piv.y == 0.0) {
       if (info == 0) info = j + 1;
     } else {
       const cplx inv = cdiv(mkc(1.0, 0.0), piv);
-      for (int i = j + 1 + tid; i < n; i += nthr) A[(size_t)i * lda + j] = cmul(A[(size_t)i * lda + j], inv);
+      for (int i0 = j + 1 + tid; i0 < n; i0 += kU * nthr) {
+        cplx v[kU];
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int i = i0 + q * nthr;
+          if (i < n) v[q] = A[(size_t)i * lda + j];
+        }
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int i = i0 + q * nthr;
+          if (i < n) A[(size_t)i * lda + j] = cmul(v[q], inv);
+        }
+      }
     }
     __syncthreads();
-    const int w = kb + jb - j - 1;
+    best = -1.0;
+    bi = j + 1;
+    const int w = ce - j - 1;
     if (w > 0) {
-      const int rows = n - j - 1;
-      for (int idx = tid; idx < rows * w; idx += nthr) {
-        const int i = j + 1 + idx / w, c = j + 1 + idx % w;
-        A[(size_t)i * lda + c] = cfma(cneg(A[(size_t)i * lda + j]), A[(size_t)j * lda + c], A[(size_t)i * lda + c]);
+      const int total = (n - j - 1) * w;
+      for (int base = tid; base < total; base += kU * nthr) {
+        cplx l[kU], a[kU];
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int idx = base + q * nthr;
+          if (idx < total) {
+            const int i = j + 1 + idx / w, c = j + 1 + idx % w;
+            l[q] = A[(size_t)i * lda + j];
+            a[q] = A[(size_t)i * lda + c];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int idx = base + q * nthr;
+          if (idx < total) {
+            const int i = j + 1 + idx / w, c = j + 1 + idx % w;
+            const cplx v = cfma(cneg(l[q]), prow[c - kb], a[q]);
+            A[(size_t)i * lda + c] = v;
+            if (c == j + 1) {
+              const double av = cabs1(v);
+              if (av > best) { best = av; bi = i; }
+            }
+          }
+        }
       }
     }
     __syncthreads();
@@ -114,6 +164,7 @@ __global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr,
   __shared__ double red_v[kTileThreads / 32];
   __shared__ int red_i[kTileThreads / 32];
   __shared__ int s_piv;
+  __shared__ cplx prow[32];
   const int tid = threadIdx.x;
   const int b = blockIdx.x;
   cplx* A = Aarr[b];
@@ -121,7 +172,7 @@ __global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr,
   int info = 0;
   for (int kb = 0; kb < n; kb += 32) {
     const int jb = min(32, n - kb);
-    lu_panel(A, n, lda, kb, jb, ipiv, info, red_v, red_i, &s_piv);
+    lu_panel(A, n, lda, kb, jb, ipiv, info, red_v, red_i, &s_piv, prow);
     if (kb + jb < n) {
       for (int idx = tid; idx < jb * jb; idx += kTileThreads) {
         const int r = idx / jb, q = idx % jb;
@@ -155,9 +206,10 @@ __global__ void __launch_bounds__(kTileThreads) getrf_panel_kernel(cplx* const* 
   __shared__ double red_v[kTileThreads / 32];
   __shared__ int red_i[kTileThreads / 32];
   __shared__ int s_piv;
+  __shared__ cplx prow[32];
   const int b = blockIdx.x;
   int info = kb == 0 ? 0 : info_all[b];
-  lu_panel(Aarr[b], n, lda, kb, jb, ipiv_all + (size_t)b * n, info, red_v, red_i, &s_piv);
+  lu_panel(Aarr[b], n, lda, kb, jb, ipiv_all + (size_t)b * n, info, red_v, red_i, &s_piv, prow);
   if (threadIdx.x == 0) info_all[b] = info;
 }
 
@@ -345,7 +397,7 @@ int sm_count() {
 cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
                            cudaStream_t st) {
   if (batch <= 0 || n <= 0) return cudaSuccess;
-  if (n <= 128 || batch >= sm_count()) {
+  if (n <= 128 || batch >= 4 * sm_count()) {
     zgetrf_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, ipiv, info);
     ++launch_counter();
     return cudaGetLastError();
