@@ -526,13 +526,20 @@ constexpr int kMsW = 64;           // window order
 constexpr int kMsShifts = 10;      // bulges per sweep
 constexpr int kMsMin = 64;         // smaller active blocks use single-shift sweeps
 constexpr int kMsThreads = 128;    // four warps
-constexpr int kMsTileElems = 2112 + 66; // max(64 x 33, 32 x 65) + a dummy row pair
+constexpr int kMsTileElems = 2112 + 66; // 66 rows x 33 (row tasks) or 32 rows x 67 (column tasks)
+constexpr int kMsLog = kMsW + 1;         // rotation log per bulge; slot kMsW holds the identity
+constexpr int kMsMaxSteps = kMsW + 3 * kMsShifts;  // chain steps of one window pass
+constexpr int kMsColPitch = 67;          // column-task tile row pitch (conflict-free 16-byte accesses)
+constexpr int kMsDummy = kMsW;           // tile row / column pair that absorbs inactive bulges
+// replay table entry: tile row (bits 0-7), log slot (8-15), first (16) and last (17) rotation of the bulge
+constexpr int kRepFirst = 1 << 16, kRepLast = 1 << 17;
 
 struct MsSmem {
   cplx* Wt;      // [kMsW][kMsW + 1]
   cplx* tiles;   // [kMsThreads / 32][kMsTileElems]
-  double* lc;    // [kMsShifts][kMsW]  rotation cosines, bulge-major
-  cplx* ls;      // [kMsShifts][kMsW]  rotation sines
+  double* lc;    // [kMsShifts][kMsLog]  rotation cosines, bulge-major
+  cplx* ls;      // [kMsShifts][kMsLog]  rotation sines
+  int* ix;       // [kMsMaxSteps][kMsShifts]  replay table per chain step and bulge
   int* firstp;   // [kMsShifts] first rotation position of each bulge in the pass
   int* cnt;      // [kMsShifts] rotations of each bulge in the pass
   int* tfirst;   // [kMsShifts] pass step of each bulge's first rotation
@@ -542,17 +549,20 @@ struct MsSmem {
 };
 
 constexpr size_t kMsSmemBytes = sizeof(cplx) * kMsW * (kMsW + 1) + sizeof(cplx) * (kMsThreads / 32) * kMsTileElems +
-                                sizeof(double) * kMsShifts * kMsW + sizeof(cplx) * kMsShifts * kMsW +
-                                sizeof(int) * 3 * kMsShifts + sizeof(cplx) * kMsShifts + sizeof(int) * 12;
+                                sizeof(double) * kMsShifts * kMsLog + sizeof(cplx) * kMsShifts * kMsLog +
+                                sizeof(int) * kMsMaxSteps * kMsShifts + sizeof(int) * 3 * kMsShifts +
+                                sizeof(cplx) * kMsShifts + sizeof(int) * 12;
+static_assert(kMsSmemBytes <= 232448, "multishift shared memory exceeds the per-block limit");
 
 __device__ MsSmem carve_ms_smem(unsigned char* base) {
   MsSmem sm;
   sm.Wt = (cplx*)base;
   sm.tiles = sm.Wt + kMsW * (kMsW + 1);
   sm.ls = sm.tiles + (kMsThreads / 32) * kMsTileElems;
-  sm.shifts = sm.ls + kMsShifts * kMsW;
+  sm.shifts = sm.ls + kMsShifts * kMsLog;
   sm.lc = (double*)(sm.shifts + kMsShifts);
-  sm.firstp = (int*)(sm.lc + kMsShifts * kMsW);
+  sm.ix = (int*)(sm.lc + kMsShifts * kMsLog);
+  sm.firstp = sm.ix + kMsMaxSteps * kMsShifts;
   sm.cnt = sm.firstp + kMsShifts;
   sm.tfirst = sm.cnt + kMsShifts;
   sm.redi = sm.tfirst + kMsShifts;
@@ -947,8 +957,8 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
         givens_fast(x, y, c, sn);
         if (sm.firstp[b] < 0) { sm.firstp[b] = p; sm.tfirst[b] = tt - t; }
         const int k = p - sm.firstp[b];
-        sm.lc[b * kMsW + k] = c;
-        sm.ls[b * kMsW + k] = sn;
+        sm.lc[b * kMsLog + k] = c;
+        sm.ls[b * kMsLog + k] = sn;
         sm.cnt[b] = k + 1;
       }
       __syncthreads();
@@ -960,8 +970,8 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
         const int j = ((p == l) ? l : p - 1) + idx % kMsW;
         if (j > we) continue;
         const int k = p - sm.firstp[b];
-        const double c = sm.lc[b * kMsW + k];
-        const cplx sn = sm.ls[b * kMsW + k];
+        const double c = sm.lc[b * kMsLog + k];
+        const cplx sn = sm.ls[b * kMsLog + k];
         const cplx a = MSW(p - ws, j - ws), bb = MSW(p + 1 - ws, j - ws);
         MSW(p - ws, j - ws) = cfma(sn, bb, cscale(a, c));
         MSW(p + 1 - ws, j - ws) = cfma(cneg(cconj(sn)), a, cscale(bb, c));
@@ -978,8 +988,8 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
         const int r = ws + idx % kMsW;
         if (r > min(p + 2, i)) continue;
         const int k = p - sm.firstp[b];
-        const double c = sm.lc[b * kMsW + k];
-        const cplx sn = sm.ls[b * kMsW + k];
+        const double c = sm.lc[b * kMsLog + k];
+        const cplx sn = sm.ls[b * kMsLog + k];
         const cplx a = MSW(r - ws, p - ws), bb = MSW(r - ws, p + 1 - ws);
         MSW(r - ws, p - ws) = cfma(cconj(sn), bb, cscale(a, c));
         MSW(r - ws, p + 1 - ws) = cfma(cneg(sn), a, cscale(bb, c));
@@ -996,9 +1006,24 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
     for (int b = 0; b < s; ++b)
       if (sm.cnt[b] > 0) { rlo = min(rlo, sm.firstp[b]); rhi = max(rhi, sm.firstp[b] + sm.cnt[b]); }
     const int nr = rhi - rlo + 1;
+    const int nsteps = t1 - t;
+    // replay table per chain step and bulge: the tile row of the bulge's row
+    // pair, its log slot and whether the rotation is its first or last in the
+    // pass; inactive bulges rotate the dummy pair by the identity slot, so the
+    // chains interleave without branches
+    for (int idx = tid; idx < nsteps * kMsShifts; idx += nthr) {
+      const int sg = idx / kMsShifts, b = idx % kMsShifts;
+      int v = kMsDummy | (kMsW << 8);
+      if (b < s) {
+        const int k = sg - sm.tfirst[b], cnt = sm.cnt[b];
+        if (k >= 0 && k < cnt)
+          v = (sm.firstp[b] - rlo + k) | (k << 8) | (k == 0 ? kRepFirst : 0) | (k == cnt - 1 ? kRepLast : 0);
+      }
+      sm.ix[idx] = v;
+    }
+    __syncthreads();
     const int nR = (n - 1 - we + 31) / 32, nU = (ws + 31) / 32, nZ = (n + 31) / 32;
     cplx* tile = sm.tiles + warp * kMsTileElems;
-    const int nsteps = t1 - t;
     for (int task = warp; task < nR + nU + nZ; task += nwarp) {
       if (task < nR) {
         // T(rlo..rhi, j): row rotations, lane = column, chain order
@@ -1012,43 +1037,30 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
 #ifdef RCWA_EIG_STATS
           if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[5], (unsigned long long)(q1c - q0c)); q0c = q1c; }
 #endif
-          // chain-order replay, branch free: inactive bulges rotate a dummy
-          // row pair by the identity, so the ten chains interleave freely
-          int tf[kMsShifts], cn[kMsShifts], fq[kMsShifts];
-#pragma unroll
-          for (int b = 0; b < kMsShifts; ++b) {
-            tf[b] = b < s ? sm.tfirst[b] : 0;
-            cn[b] = b < s ? sm.cnt[b] : 0;
-            fq[b] = b < s ? sm.firstp[b] - rlo : 0;
-          }
-          cplx* dummy = tile + 2112;
           cplx xc[kMsShifts];
 #pragma unroll
           for (int b = 0; b < kMsShifts; ++b) xc[b] = mkc(0.0, 0.0);
           for (int sg = 0; sg < nsteps; ++sg) {
-            cplx yv[kMsShifts];
-            cplx* ptr[kMsShifts];
+            const int* e = sm.ix + sg * kMsShifts;
+            int v[kMsShifts];
+            cplx* px[kMsShifts];
+            cplx x[kMsShifts], y[kMsShifts], sn[kMsShifts];
+            double c[kMsShifts];
 #pragma unroll
             for (int b = 0; b < kMsShifts; ++b) {
-              const int k = sg - tf[b];
-              const bool act = (unsigned)k < (unsigned)cn[b];
-              ptr[b] = act ? tile + (fq[b] + k) * 33 + lane : dummy + lane;
-              if (k == 0) xc[b] = ptr[b][0];
-              yv[b] = ptr[b][33];
+              v[b] = e[b];
+              const int k = (v[b] >> 8) & 0xff;
+              px[b] = tile + (v[b] & 0xff) * 33 + lane;
+              c[b] = sm.lc[b * kMsLog + k];
+              sn[b] = sm.ls[b * kMsLog + k];
+              y[b] = px[b][33];
+              x[b] = (v[b] & kRepFirst) ? px[b][0] : xc[b];
             }
 #pragma unroll
             for (int b = 0; b < kMsShifts; ++b) {
-              const int k = sg - tf[b];
-              const bool act = (unsigned)k < (unsigned)cn[b];
-              const int kk = act ? k : 0;
-              const double c = act ? sm.lc[b * kMsW + kk] : 1.0;
-              const cplx ls = sm.ls[b * kMsW + kk];
-              const cplx sn = act ? ls : mkc(0.0, 0.0);
-              const cplx xn = cfma(sn, yv[b], cscale(xc[b], c));
-              const cplx yn = cfma(cneg(cconj(sn)), xc[b], cscale(yv[b], c));
-              ptr[b][0] = xn;
-              if (k == cn[b] - 1) ptr[b][33] = yn;
-              xc[b] = act ? yn : xc[b];
+              px[b][0] = cfma(sn[b], y[b], cscale(x[b], c[b]));
+              xc[b] = cfma(cneg(cconj(sn[b])), x[b], cscale(y[b], c[b]));
+              if (v[b] & kRepLast) px[b][33] = xc[b];
             }
           }
 #ifdef RCWA_EIG_STATS
@@ -1066,60 +1078,50 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
         const int rows = isZ ? n : ws;
         if (!isZ) {
           for (int rr = 0; rr < 32 && r0 + rr < rows; ++rr)
-            for (int c = lane; c < nr; c += 32) cp_async16(&tile[rr * 65 + c], &T[(size_t)(r0 + rr) * ldt + rlo + c]);
+            for (int c = lane; c < nr; c += 32)
+              cp_async16(&tile[rr * kMsColPitch + c], &T[(size_t)(r0 + rr) * ldt + rlo + c]);
         } else {
           if (r0 + lane < rows)
-            for (int c = 0; c < nr; ++c) cp_async16(&tile[lane * 65 + c], &Z[(size_t)(rlo + c) * n + r0 + lane]);
+            for (int c = 0; c < nr; ++c) cp_async16(&tile[lane * kMsColPitch + c], &Z[(size_t)(rlo + c) * n + r0 + lane]);
         }
         cp_async_wait_all();
         __syncwarp();
         if (r0 + lane < rows) {
-          cplx* row = tile + lane * 65;
-          int tf[kMsShifts], cn[kMsShifts], fq[kMsShifts];
-#pragma unroll
-          for (int b = 0; b < kMsShifts; ++b) {
-            tf[b] = b < s ? sm.tfirst[b] : 0;
-            cn[b] = b < s ? sm.cnt[b] : 0;
-            fq[b] = b < s ? sm.firstp[b] - rlo : 0;
-          }
-          cplx* dummy = tile + 2112 + 2 * lane;
+          cplx* row = tile + lane * kMsColPitch;
           cplx xc[kMsShifts];
 #pragma unroll
           for (int b = 0; b < kMsShifts; ++b) xc[b] = mkc(0.0, 0.0);
           for (int sg = 0; sg < nsteps; ++sg) {
-            cplx yv[kMsShifts];
-            cplx* ptr[kMsShifts];
+            const int* e = sm.ix + sg * kMsShifts;
+            int v[kMsShifts];
+            cplx* px[kMsShifts];
+            cplx x[kMsShifts], y[kMsShifts], sn[kMsShifts];
+            double c[kMsShifts];
 #pragma unroll
             for (int b = 0; b < kMsShifts; ++b) {
-              const int k = sg - tf[b];
-              const bool act = (unsigned)k < (unsigned)cn[b];
-              ptr[b] = act ? row + fq[b] + k : dummy;
-              if (k == 0) xc[b] = ptr[b][0];
-              yv[b] = ptr[b][1];
+              v[b] = e[b];
+              const int k = (v[b] >> 8) & 0xff;
+              px[b] = row + (v[b] & 0xff);
+              c[b] = sm.lc[b * kMsLog + k];
+              sn[b] = sm.ls[b * kMsLog + k];
+              y[b] = px[b][1];
+              x[b] = (v[b] & kRepFirst) ? px[b][0] : xc[b];
             }
 #pragma unroll
             for (int b = 0; b < kMsShifts; ++b) {
-              const int k = sg - tf[b];
-              const bool act = (unsigned)k < (unsigned)cn[b];
-              const int kk = act ? k : 0;
-              const double c = act ? sm.lc[b * kMsW + kk] : 1.0;
-              const cplx ls = sm.ls[b * kMsW + kk];
-              const cplx sn = act ? ls : mkc(0.0, 0.0);
-              const cplx xn = cfma(cconj(sn), yv[b], cscale(xc[b], c));
-              const cplx yn = cfma(cneg(sn), xc[b], cscale(yv[b], c));
-              ptr[b][0] = xn;
-              if (k == cn[b] - 1) ptr[b][1] = yn;
-              xc[b] = act ? yn : xc[b];
+              px[b][0] = cfma(cconj(sn[b]), y[b], cscale(x[b], c[b]));
+              xc[b] = cfma(cneg(sn[b]), x[b], cscale(y[b], c[b]));
+              if (v[b] & kRepLast) px[b][1] = xc[b];
             }
           }
         }
         __syncwarp();
         if (!isZ) {
           for (int rr = 0; rr < 32 && r0 + rr < rows; ++rr)
-            for (int c = lane; c < nr; c += 32) T[(size_t)(r0 + rr) * ldt + rlo + c] = tile[rr * 65 + c];
+            for (int c = lane; c < nr; c += 32) T[(size_t)(r0 + rr) * ldt + rlo + c] = tile[rr * kMsColPitch + c];
         } else {
           if (r0 + lane < rows)
-            for (int c = 0; c < nr; ++c) Z[(size_t)(rlo + c) * n + r0 + lane] = tile[lane * 65 + c];
+            for (int c = 0; c < nr; ++c) Z[(size_t)(rlo + c) * n + r0 + lane] = tile[lane * kMsColPitch + c];
         }
         __syncwarp();
       }
@@ -1237,6 +1239,12 @@ __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr,
                                                              void* work, int* info_all) {
   extern __shared__ __align__(16) unsigned char dsm[];
   const MsSmem sm = carve_ms_smem(dsm);
+  // identity slot of every bulge's rotation log (inactive chain steps)
+  for (int b = threadIdx.x; b < kMsShifts; b += blockDim.x) {
+    sm.lc[b * kMsLog + kMsW] = 1.0;
+    sm.ls[b * kMsLog + kMsW] = mkc(0.0, 0.0);
+  }
+  __syncthreads();
   cplx* A = Aarr[blockIdx.x];
   const Scratch s = scratch_for(work, n, blockIdx.x);
 #ifdef RCWA_EIG_STATS
