@@ -39,6 +39,10 @@ extern "C" {
 
 /* ---- precision of the batched solve ---------------------------------------- */
 #define RCWA_PREC_FP64  0     /* every stage complex128                           */
+#define RCWA_PREC_MIXED 1     /* cascade GEMMs (F, G, Rud, Tdd) in 3xTF32 on the
+                                 tensor cores with FP32 accumulation; the
+                                 eigensolve, the interface and tau solves, the
+                                 half-spaces and the efficiency sums stay FP64  */
 
 typedef struct { double re, im; } rcwa_cplx;
 
@@ -167,6 +171,14 @@ int rcwa_layer_solve(rcwa_engine* e, const double* cx, int ncx, const double* cy
  * VR[batch][n*n] row-major (columns unit 2-norm), info[batch]. */
 int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
                        rcwa_cplx* w, rcwa_cplx* VR, int* info);
+
+/* Batched complex GEMM D = alpha*A*B + beta*C (row-major, host buffers
+ * [batch][M*K], [batch][K*N], [batch][M*N]; C may be NULL when beta = 0), the
+ * product kernel of the cascade: RCWA_PREC_FP64 on the FP64 tensor path,
+ * RCWA_PREC_MIXED as 3xTF32 on the fifth-generation tensor cores.  No
+ * counterpart in the reference (its Eigen products). */
+int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch, const rcwa_cplx* A, const rcwa_cplx* B,
+                       const rcwa_cplx* C, rcwa_cplx alpha, rcwa_cplx beta, int precision, rcwa_cplx* D);
 
 /* ---- slab S-matrices and the Redheffer star product -------------------------
  * Batched, FP64, host buffers; every matrix row-major [batch][n*n].

@@ -27,6 +27,7 @@ RCWA_ERR_NODEVICE = 8
 RCWA_ERR_UNSUPPORTED = 9
 RCWA_CONTINUOUS_XY, RCWA_DISCONTINUOUS_X, RCWA_DISCONTINUOUS_Y = 0, 1, 2
 RCWA_PREC_FP64 = 0
+RCWA_PREC_MIXED = 1
 
 # every symbol declared in include/rcwa_b200.h
 EXPORTS = [
@@ -35,11 +36,15 @@ EXPORTS = [
     "rcwa_plan_launch_count", "rcwa_plan_rescatter", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
-    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched",
+    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_zgemm_batched",
 ]
 
 _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int)
+
+
+class rcwa_cplx(C.Structure):
+    _fields_ = [("re", C.c_double), ("im", C.c_double)]
 
 
 class rcwa_stack(C.Structure):
@@ -113,6 +118,8 @@ def load() -> C.CDLL:
     lib.rcwa_slab_smatrix_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5 + [_DP, _DP] + \
         [C.c_void_p, C.c_void_p, _IP]
     lib.rcwa_star_product_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 8 + [_IP]
+    lib.rcwa_zgemm_batched.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                       C.c_void_p, rcwa_cplx, rcwa_cplx, C.c_int, C.c_void_p]
     _lib = lib
     return lib
 
@@ -268,6 +275,18 @@ class Engine:
         if rc and not np.any(info):
             self._check(rc, "zgeev")
         return w, VR, info
+
+    def zgemm(self, A, B, C=None, alpha=1.0, beta=0.0, precision=RCWA_PREC_FP64):
+        """Batched D = alpha A B + beta C; (batch, M, K) x (batch, K, N)."""
+        A, B = self._batch3(A, B)
+        b, M, K = A.shape
+        N = B.shape[2]
+        Cm = None if C is None else self._batch3(C)[0]
+        D = np.zeros((b, M, N), dtype=np.complex128)
+        al, be = complex(alpha), complex(beta)
+        self._check(self.lib.rcwa_zgemm_batched(self.h, M, N, K, b, _v(A), _v(B), _v(Cm), rcwa_cplx(al.real, al.imag),
+                                                rcwa_cplx(be.real, be.imag), precision, _v(D)), "zgemm")
+        return D
 
     @staticmethod
     def _batch3(*mats):

@@ -1,0 +1,286 @@
+// 3xTF32 complex GEMM on tcgen05.
+//
+// One CTA (four warps) computes a 128 x 128 complex output tile.  For each
+// 32-deep K slab the CTA converts its FP64 operand tiles into eight TF32
+// planes in shared memory (A: re hi/lo, im hi/lo; B likewise), laid out as
+// K-major, unswizzled UMMA core matrices (8 rows x 16 bytes; 8-row groups
+// 128 B apart, 16-byte K chunks 2048 B apart).  One thread then issues, per
+// K step of 8, twelve tcgen05.mma (M=128, N=128, K=8):
+//   Re += Ar*Br (3 terms) - Ai*Bi (3 terms, A negated in the descriptor)
+//   Im += Ar*Bi (3 terms) + Ai*Br (3 terms)
+// into two FP32 accumulators in tensor memory (256 columns), and commits to
+// an mbarrier; the next slab's conversion waits for that commit before it
+// overwrites the planes.  The epilogue reads the accumulators with
+// tcgen05.ld (warp w owns rows 32w..32w+31) and writes alpha*acc + beta*C.
+// Every wait is bounded: a wait that runs out sets the error flag, waits
+// (bounded) for the MMAs in flight, frees the tensor memory and skips the
+// tile's stores.
+#include <cstdint>
+
+#include "gemm_tc.cuh"
+
+namespace {
+
+constexpr int kTcM = 128, kTcN = 128, kTcK = 32;
+constexpr int kTcThreads = 128;
+constexpr int kPlaneFloats = kTcM * kTcK;                // 4096 floats = 16 KB
+constexpr int kLbo = 2048, kSbo = 128;                   // bytes
+constexpr size_t kTcSmem = 8 * kPlaneFloats * sizeof(float) + 64;
+constexpr uint32_t kTmemCols = 256;
+constexpr long kWaitLimit = 1L << 22;
+
+// instruction descriptor: D F32, A/B TF32, both K-major, N = 128, M = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
+                            ((uint32_t)(kTcM >> 4) << 24);
+constexpr uint32_t kIdescNegA = kIdesc | (1u << 13);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// byte offset of (row r, k) in a plane
+__device__ __forceinline__ int plane_off(int r, int k) {
+  return (k >> 2) * kLbo + (r >> 3) * kSbo + (r & 7) * 16 + (k & 3) * 4;
+}
+
+// shared-memory matrix descriptor (sm100 layout: start >> 4 at [0,14), LBO >> 4
+// at [16,30), SBO >> 4 at [32,46), version 1 at [46,48), no swizzle)
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kLbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((kSbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+  for (long it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(mbar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void split_tf32(double v, float& hi, float& lo) {
+  const float f = (float)v;
+  uint32_t h, l;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(f));
+  const float rest = f - __uint_as_float(h);
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(rest));
+  hi = __uint_as_float(h);
+  lo = __uint_as_float(l);
+}
+
+__device__ __forceinline__ void st_plane4(float* plane, int off, float a, float b, float c, float d) {
+  *reinterpret_cast<float4*>(reinterpret_cast<char*>(plane) + off) = make_float4(a, b, c, d);
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g, int* err) {
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  float* planes = reinterpret_cast<float*>(tsm);
+  float* Arh = planes;
+  float* Arl = planes + kPlaneFloats;
+  float* Aih = planes + 2 * kPlaneFloats;
+  float* Ail = planes + 3 * kPlaneFloats;
+  float* Brh = planes + 4 * kPlaneFloats;
+  float* Brl = planes + 5 * kPlaneFloats;
+  float* Bih = planes + 6 * kPlaneFloats;
+  float* Bil = planes + 7 * kPlaneFloats;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 8 * kPlaneFloats * sizeof(float));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
+
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int b = blockIdx.z;
+  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
+  const cplx* A = (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
+  const cplx* B = (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB;
+  const uint32_t mb = smem_u32(mbar);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tRe = tmem, tIm = tmem + kTcN;
+
+  uint32_t phase = 0;
+  int pending = 0;  // a commit not yet waited for (uniform across the CTA)
+  for (int k0 = 0; k0 < g.K; k0 += kTcK) {
+    if (pending) {
+      // the planes are free once the previous slab's MMAs completed
+      if (mbar_wait(mb, phase)) {
+        phase ^= 1u;
+        pending = 0;
+      } else {
+        *s_fail = 1;
+      }
+    }
+    __syncthreads();
+    if (*s_fail) break;
+    // A: row tid, K chunks q (4 consecutive k each)
+    {
+      const int gm = m0 + tid;
+#pragma unroll 2
+      for (int q = 0; q < kTcK / 4; ++q) {
+        float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int gk = k0 + 4 * q + j;
+          cplx v = mkc(0.0, 0.0);
+          if (gm < g.M && gk < g.K) v = A[(size_t)gm * g.lda + gk];
+          split_tf32(v.x, rh[j], rl[j]);
+          split_tf32(v.y, ih[j], il[j]);
+        }
+        const int off = plane_off(tid, 4 * q);
+        st_plane4(Arh, off, rh[0], rh[1], rh[2], rh[3]);
+        st_plane4(Arl, off, rl[0], rl[1], rl[2], rl[3]);
+        st_plane4(Aih, off, ih[0], ih[1], ih[2], ih[3]);
+        st_plane4(Ail, off, il[0], il[1], il[2], il[3]);
+      }
+    }
+    // B: column tid (row of the K-major plane), K chunks q
+    {
+      const int gn = n0 + tid;
+#pragma unroll 2
+      for (int q = 0; q < kTcK / 4; ++q) {
+        float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const int gk = k0 + 4 * q + j;
+          cplx v = mkc(0.0, 0.0);
+          if (gn < g.N && gk < g.K) v = B[(size_t)gk * g.ldb + gn];
+          split_tf32(v.x, rh[j], rl[j]);
+          split_tf32(v.y, ih[j], il[j]);
+        }
+        const int off = plane_off(tid, 4 * q);
+        st_plane4(Brh, off, rh[0], rh[1], rh[2], rh[3]);
+        st_plane4(Brl, off, rl[0], rl[1], rl[2], rl[3]);
+        st_plane4(Bih, off, ih[0], ih[1], ih[2], ih[3]);
+        st_plane4(Bil, off, il[0], il[1], il[2], il[3]);
+      }
+    }
+    // make the generic-proxy writes visible to the tensor cores
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+      for (int ks = 0; ks < kTcK / 8; ++ks) {
+        const uint32_t off = (uint32_t)(2 * ks * kLbo);
+        const uint64_t arh = make_desc(smem_u32(Arh) + off), arl = make_desc(smem_u32(Arl) + off);
+        const uint64_t aih = make_desc(smem_u32(Aih) + off), ail = make_desc(smem_u32(Ail) + off);
+        const uint64_t brh = make_desc(smem_u32(Brh) + off), brl = make_desc(smem_u32(Brl) + off);
+        const uint64_t bih = make_desc(smem_u32(Bih) + off), bil = make_desc(smem_u32(Bil) + off);
+        const uint32_t acc = (k0 > 0 || ks > 0) ? 1u : 0u;
+        mma_tf32(tRe, arh, brh, kIdesc, acc);
+        mma_tf32(tRe, arh, brl, kIdesc, 1u);
+        mma_tf32(tRe, arl, brh, kIdesc, 1u);
+        mma_tf32(tRe, aih, bih, kIdescNegA, 1u);
+        mma_tf32(tRe, aih, bil, kIdescNegA, 1u);
+        mma_tf32(tRe, ail, bih, kIdescNegA, 1u);
+        mma_tf32(tIm, arh, bih, kIdesc, acc);
+        mma_tf32(tIm, arh, bil, kIdesc, 1u);
+        mma_tf32(tIm, arl, bih, kIdesc, 1u);
+        mma_tf32(tIm, aih, brh, kIdesc, 1u);
+        mma_tf32(tIm, aih, brl, kIdesc, 1u);
+        mma_tf32(tIm, ail, brh, kIdesc, 1u);
+      }
+      mma_commit(mb);
+    }
+    pending = 1;
+  }
+  // the last slab's MMAs (after a failure too: nothing may still write the
+  // tensor memory when it is freed)
+  if (pending && !mbar_wait(mb, phase)) *s_fail = 1;
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const bool good = *s_fail == 0;
+  if (!good && tid == 0) atomicExch(err, 1);
+  if (good) {
+    const int m = m0 + 32 * warp + lane;
+    const uint32_t row_addr = (uint32_t)(32 * warp) << 16;
+    for (int cb = 0; cb < kTcN; cb += 16) {
+      uint32_t re[16], im[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(re[0]), "=r"(re[1]), "=r"(re[2]), "=r"(re[3]), "=r"(re[4]), "=r"(re[5]), "=r"(re[6]), "=r"(re[7]),
+            "=r"(re[8]), "=r"(re[9]), "=r"(re[10]), "=r"(re[11]), "=r"(re[12]), "=r"(re[13]), "=r"(re[14]),
+            "=r"(re[15])
+          : "r"(tRe + row_addr + cb));
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+          : "=r"(im[0]), "=r"(im[1]), "=r"(im[2]), "=r"(im[3]), "=r"(im[4]), "=r"(im[5]), "=r"(im[6]), "=r"(im[7]),
+            "=r"(im[8]), "=r"(im[9]), "=r"(im[10]), "=r"(im[11]), "=r"(im[12]), "=r"(im[13]), "=r"(im[14]),
+            "=r"(im[15])
+          : "r"(tIm + row_addr + cb));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (m < g.M) {
+        cplx* Drow = (g.D ? g.D[b] : g.D0 + b * g.sD) + g.offD + (size_t)m * g.ldd;
+        const cplx* Crow = (g.beta.x != 0.0 || g.beta.y != 0.0) ? g.C[b] + g.offC + (size_t)m * g.ldc : nullptr;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = n0 + cb + j;
+          if (n < g.N) {
+            cplx v = cmul(g.alpha, mkc((double)__uint_as_float(re[j]), (double)__uint_as_float(im[j])));
+            if (Crow) v = cfma(g.beta, Crow[n], v);
+            if (m == n) v = cadd(v, g.gammaI);
+            Drow[n] = v;
+          }
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+}  // namespace
+
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* err, cudaStream_t st) {
+  if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
+  if (g.K <= 0 || g.transA || g.transB || g.s || !err) return cudaErrorInvalidValue;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(zgemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kTcSmem);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  dim3 grid((g.N + kTcN - 1) / kTcN, (g.M + kTcM - 1) / kTcM, g.batch);
+  zgemm_tf32x3_kernel<<<grid, kTcThreads, kTcSmem, st>>>(g, err);
+  ++launch_counter();
+  return cudaGetLastError();
+}

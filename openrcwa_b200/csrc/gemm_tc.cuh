@@ -1,0 +1,11 @@
+// Complex GEMM on the fifth-generation tensor cores (tcgen05, kind::tf32) in
+// 3xTF32: every FP64 operand is split into a TF32 high part and a TF32 low
+// part, and each real product is formed as hi*hi + hi*lo + lo*hi with FP32
+// accumulation in tensor memory (about 21 significant bits).
+#pragma once
+#include "linalg.cuh"
+
+// D = alpha*A*B + beta*C + gammaI*I for every batch item (A, B not transposed,
+// no diagonal scaling).  err (device int) is set to 1 if a tensor-core
+// completion wait runs out; the affected tile is then not written.
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* err, cudaStream_t st);

@@ -9,6 +9,7 @@
 #include "eig.cuh"
 #include "engine_internal.cuh"
 #include "fourier.cuh"
+#include "gemm_tc.cuh"
 #include "linalg.cuh"
 #include "rcwa_kernels.cuh"
 
@@ -246,4 +247,49 @@ extern "C" int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_c
     if (!first && hinfo[b]) first = hinfo[b];
   }
   return first;
+}
+
+extern "C" int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch, const rcwa_cplx* A,
+                                  const rcwa_cplx* B, const rcwa_cplx* C, rcwa_cplx alpha, rcwa_cplx beta,
+                                  int precision, rcwa_cplx* D) {
+  if (!e || M < 1 || N < 1 || K < 1 || batch < 1 || !A || !B || !D) return RCWA_ERR_INVALID;
+  if ((beta.re != 0.0 || beta.im != 0.0) && !C) return RCWA_ERR_INVALID;
+  if (precision != RCWA_PREC_FP64 && precision != RCWA_PREC_MIXED) return RCWA_ERR_INVALID;
+  if (cudaSetDevice(e->device) != cudaSuccess) return RCWA_ERR_CUDA;
+  const size_t mk = (size_t)M * K, kn = (size_t)K * N, mn = (size_t)M * N;
+  Dev dA(sizeof(cplx) * mk * batch), dB(sizeof(cplx) * kn * batch), dC(sizeof(cplx) * mn * batch),
+      dD(sizeof(cplx) * mn * batch), dp(sizeof(void*) * 2 * batch), derr(sizeof(int));
+  if (!dA.p || !dB.p || !dC.p || !dD.p || !dp.p || !derr.p) return set_err(e, RCWA_ERR_NOMEM, "allocation failed");
+  const bool useC = beta.re != 0.0 || beta.im != 0.0;
+  if (!up(dA.p, (const cplx*)A, mk * batch) || !up(dB.p, (const cplx*)B, kn * batch) ||
+      (useC && !up(dC.p, (const cplx*)C, mn * batch)))
+    return set_err(e, RCWA_ERR_CUDA, "upload failed");
+  std::vector<void*> hp(2 * batch);
+  for (int b = 0; b < batch; ++b) {
+    hp[b] = dC.as<cplx>() + mn * b;
+    hp[batch + b] = dD.as<cplx>() + mn * b;
+  }
+  const int zero = 0;
+  if (!up(dp.p, hp.data(), 2 * batch) || !up(derr.p, &zero, 1)) return set_err(e, RCWA_ERR_CUDA, "upload failed");
+  GemmArgs g{};
+  g.A0 = dA.as<cplx>(); g.sA = mk;
+  g.B0 = dB.as<cplx>(); g.sB = kn;
+  g.C = useC ? (const cplx* const*)dp.p : nullptr;
+  g.D = (cplx* const*)dp.p + batch;
+  g.M = M; g.N = N; g.K = K;
+  g.lda = K; g.ldb = N; g.ldc = N; g.ldd = N;
+  g.alpha = mkc(alpha.re, alpha.im);
+  g.beta = mkc(beta.re, beta.im);
+  g.gammaI = mkc(0.0, 0.0);
+  g.batch = batch;
+  cudaError_t err = precision == RCWA_PREC_MIXED ? zgemm_tf32x3_batched(g, derr.as<int>(), e->stream)
+                                                 : zgemm_batched(g, e->stream);
+  if (err != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess)
+    return set_err(e, RCWA_ERR_CUDA, "GEMM kernel failed");
+  int herr = 0;
+  if (cudaMemcpy(&herr, derr.p, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(D, dD.p, sizeof(cplx) * mn * batch, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return set_err(e, RCWA_ERR_CUDA, "download failed");
+  if (herr) return set_err(e, RCWA_ERR_CUDA, "tensor-core completion wait ran out");
+  return RCWA_OK;
 }
