@@ -27,6 +27,7 @@
 #include "engine_internal.cuh"
 #include "fourier.cuh"
 #include "linalg.cuh"
+#include "gemm_tc.cuh"
 #include "rcwa_kernels.cuh"
 
 
@@ -88,6 +89,8 @@ struct rcwa_plan {
   double* dRef = nullptr;
   double* dTrn = nullptr;
   int* dStatus = nullptr;
+  int* dTcErr = nullptr;   // set when a tensor-core completion wait ran out
+  int precision = RCWA_PREC_FP64;
   std::vector<std::function<cudaError_t(cudaStream_t, long long&, StageProf&)>> steps;
   long long launches = 0;
   std::unique_ptr<StageProf> prof{new StageProf()};
@@ -318,7 +321,8 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   *out = nullptr;
   if (n_stacks <= 0 || !stacks || n_pts <= 0 || !pts || n_exc <= 0 || !pxy)
     return fail(e, RCWA_ERR_INVALID, "empty batch or null pointer");
-  if (precision != RCWA_PREC_FP64) return fail(e, RCWA_ERR_UNSUPPORTED, "precision mode not available");
+  if (precision != RCWA_PREC_FP64 && precision != RCWA_PREC_MIXED)
+    return fail(e, RCWA_ERR_INVALID, "unknown precision mode");
   if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, RCWA_ERR_CUDA, "cudaSetDevice failed");
   std::vector<StackInfo> si;
   for (int s = 0; s < n_stacks; ++s) {
@@ -336,6 +340,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   std::unique_ptr<rcwa_plan> P(new rcwa_plan());
   P->e = e;
   P->n_pts = n_pts;
+  P->precision = precision;
   P->n_exc = n_exc;
   P->point_N.resize(n_pts);
   P->order_offset.resize(n_pts);
@@ -378,6 +383,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     size_t oR = ol.take(sizeof(double) * n_pts * n_exc), oT = ol.take(sizeof(double) * n_pts * n_exc);
     size_t oRef = ol.take(sizeof(double) * std::max<size_t>(acc, 1)), oTrn = ol.take(sizeof(double) * std::max<size_t>(acc, 1));
     size_t oS = ol.take(sizeof(int) * n_pts);
+    size_t oE = ol.take(sizeof(int));
     if (cudaMalloc(&P->outputs.p, ol.off) != cudaSuccess) return fail(e, RCWA_ERR_NOMEM, "output allocation failed");
     P->outputs.bytes = ol.off;
     char* b = (char*)P->outputs.p;
@@ -386,6 +392,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     P->dRef = (double*)(b + oRef);
     P->dTrn = (double*)(b + oTrn);
     P->dStatus = (int*)(b + oS);
+    P->dTcErr = (int*)(b + oE);
   }
 
   // ---- chunking: group by (nx, ny), then fill chunks up to the memory budget
@@ -759,7 +766,13 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         int* pipiv = (int*)(wb + c.pipiv);
         int* pinfo = (int*)(wb + c.pinfo);
         int* status = P->dStatus;
+        int* tcerr = P->dTcErr;
+        const bool mixed = precision == RCWA_PREC_MIXED;
         P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+          // the cascade products: FP64 tensor path, or 3xTF32 on tcgen05
+          auto product = [&](const GemmArgs& ga) {
+            return mixed ? zgemm_tf32x3_batched(ga, tcerr, st) : zgemm_batched(ga, st);
+          };
           char* m = (char*)plan->meta.p;
           auto cpa = [m](size_t o) { return (const cplx* const*)(m + o); };
           auto pa = [m](size_t o) { return (cplx* const*)(m + o); };
@@ -785,10 +798,10 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           // F = IE + IE waveRud ; G = IH - IH waveRud   (:440-443)
           g.A = cpa(ofA); g.B = cpa(ofB); g.C = cpa(ofC); g.D = pa(ofD);
           g.alpha = mkc(1, 0); g.beta = mkc(1, 0);
-          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          if ((err = product(g)) != cudaSuccess) return err;
           g.A = cpa(ogA); g.B = cpa(ogB); g.C = cpa(ogC); g.D = pa(ogD);
           g.alpha = mkc(-1, 0); g.beta = mkc(1, 0);
-          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          if ((err = product(g)) != cudaSuccess) return err;
           pf.mark(st, kStCascadeGemm);
           // tau = (F + G)^-1  (:451-453)
           if ((err = zaxpby_batched(cpa(osF), cpa(osG), pa(osD), mkc(1, 0), mkc(1, 0), n, k, st)) != cudaSuccess)
@@ -804,10 +817,10 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           // Rud = I - 2 G tau ; Tdd = 2 waveTdd tau  (:457-460)
           g.A = cpa(otG); g.B = cpa(otTau); g.C = nullptr; g.D = pa(orD);
           g.alpha = mkc(-2, 0); g.beta = mkc(0, 0); g.gammaI = mkc(1, 0);
-          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          if ((err = product(g)) != cudaSuccess) return err;
           g.A = cpa(otT); g.B = cpa(otTau); g.C = nullptr; g.D = pa(otD);
           g.alpha = mkc(2, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
-          err = zgemm_batched(g, st);
+          err = product(g);
           pf.mark(st, kStCascadeGemm);
           return err;
         });
@@ -871,6 +884,7 @@ namespace {
 cudaError_t issue_plan(rcwa_plan* p, cudaStream_t st) {
   long long nl = 0;
   cudaError_t err = cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st);
+  if (err == cudaSuccess) err = cudaMemsetAsync(p->dTcErr, 0, sizeof(int), st);
   p->prof->begin(st);
   for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, nl, *p->prof);
   return err;
@@ -995,6 +1009,9 @@ extern "C" int rcwa_plan_results(rcwa_plan* p, double* R, double* T, double* ref
   if (cudaMemcpy(hs.data(), p->dStatus, sizeof(int) * p->n_pts, cudaMemcpyDeviceToHost) != cudaSuccess)
     return RCWA_ERR_CUDA;
   if (status) std::memcpy(status, hs.data(), sizeof(int) * p->n_pts);
+  int tcerr = 0;
+  if (cudaMemcpy(&tcerr, p->dTcErr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
+  if (tcerr) return fail(p->e, RCWA_ERR_CUDA, "a tensor-core completion wait ran out; results are incomplete");
   for (int v : hs)
     if (v) return v;
   return RCWA_OK;
