@@ -8,11 +8,15 @@ One step = one batched pass of the full RCWA solve (convolution matrices,
 per-layer eigenproblems, interface solves, S-matrix cascade, per-order
 efficiencies of TE and TM) over a batch of --batch points of that sweep.
 
-value: device time of K plan executions with the inputs resident (CUDA events
-on the launching stream, max over ranks).  e2e: the same metric through the
-public C ABI (rcwa_engine_solve_batch) with host buffers, host<->device copies
-inside the timed region.  --impl reference times the CPU oracle (the NumPy
-restatement of the reference's LAPACK path) on the host cores.
+value: the mixed-precision engine (cascade products in 3xTF32 on the tcgen05
+tensor cores, everything else FP64): device time of K plan executions with the
+inputs resident (CUDA events on the launching stream, max over ranks).
+plain_fp64: the same batch through the FP64 engine; mixed_error: the largest
+efficiency difference between the two (the accuracy bound is 1e-4).  e2e: the
+mixed engine through the public C ABI (rcwa_engine_solve_batch) with host
+buffers, host<->device copies inside the timed region.  --impl reference times
+the CPU oracle (the NumPy restatement of the reference's LAPACK path) on the
+host cores.
 
 Multi-GPU: every rank solves its own batch of the sweep (weak scaling, no
 data-path collective); only the barrier and the max of the timings cross ranks.
@@ -239,40 +243,54 @@ def main():
     B = args.batch
     eng = o.Engine(local)
     bpts, bpxy = workloads.batch_slice(pts, pxy, workloads.shard_start(rank, world, B, 0), B)
-    plan = eng.plan(stacks, bpts, bpxy)
     stream = torch.cuda.Stream()
-    # stage-timing events on from the start: the second execution captures the
-    # launch sequence (with its event records) into the CUDA graph that every
-    # later execution launches
-    plan.set_profiling(True)
-    for _ in range(args.warmup):
-        plan.execute(stream.cuda_stream)
-    stream.synchronize()
-    R, T, _, _, status = plan.results()
-    if np.any(status):
-        raise SystemExit(f"solve status {status}")
     fp64_peak = fp64_gemm_peak_tflops(torch)
-    barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
-    stage_ms = {}
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        plan.execute(stream.cuda_stream)
-        for k, v in plan.stage_times().items():
-            stage_ms[k] = stage_ms.get(k, 0.0) + v
-    e1.record(stream)
-    stream.synchronize()
-    clk = clocks.stop()
-    plan.set_profiling(False)
-    t_ms = allmax(e0.elapsed_time(e1))
-    launches = plan.launch_count() * args.steps
+
+    def timed_plan(precision, warmup, sample_clocks):
+        """Warm up, then time `steps` executions of one plan of this rank's
+        batch on `stream` (CUDA events, max over ranks).  Stage-timing events
+        are on from the start: the second execution captures the launch
+        sequence (with its event records) into the CUDA graph that every later
+        execution launches."""
+        plan = eng.plan(stacks, bpts, bpxy, precision=precision)
+        plan.set_profiling(True)
+        for _ in range(warmup):
+            plan.execute(stream.cuda_stream)
+        stream.synchronize()
+        barrier()
+        clocks = ClockSampler(local) if sample_clocks else None
+        if clocks:
+            clocks.start()
+        stage_ms = {}
+        e0.record(stream)
+        for _ in range(args.steps):
+            plan.execute(stream.cuda_stream)
+            for k, v in plan.stage_times().items():
+                stage_ms[k] = stage_ms.get(k, 0.0) + v
+        e1.record(stream)
+        stream.synchronize()
+        clk = clocks.stop() if clocks else None
+        t_ms = allmax(e0.elapsed_time(e1))
+        launches = plan.launch_count() * args.steps
+        R, T, REF, TRN, status = plan.results(orders=True)
+        if np.any(status):
+            raise SystemExit(f"solve status {status}")
+        # release the plan (and with it the engine's cached workspace) so that
+        # the next plan and the end-to-end calls find the workspace free
+        plan.close()
+        return t_ms, stage_ms, launches, clk, (R, T, REF, TRN)
+
+    # the headline: the mixed-precision engine; then the plain FP64 engine on
+    # the same batch, whose results (parity-tested against the oracle at 1e-9)
+    # measure the mixed path's error
+    t_ms, stage_ms, launches, clk, res_mixed = timed_plan(o.RCWA_PREC_MIXED, args.warmup, True)
+    t64_ms, stage64_ms, _, _, res_fp64 = timed_plan(o.RCWA_PREC_FP64, max(2, min(args.warmup, 3)), False)
     value = world * B * args.steps / (t_ms * 1e-3)
-    # release the plan (and with it the engine's cached workspace) so that the
-    # end-to-end calls below find the workspace free, as a caller's would
-    plan.close()
+    value64 = world * B * args.steps / (t64_ms * 1e-3)
+    dRT = max(float(np.max(np.abs(res_mixed[0] - res_fp64[0]))), float(np.max(np.abs(res_mixed[1] - res_fp64[1]))))
+    dorders = max(float(np.max(np.abs(res_mixed[2] - res_fp64[2]))), float(np.max(np.abs(res_mixed[3] - res_fp64[3]))))
 
     # e2e: the public C ABI with host buffers, a different batch each step
     barrier()
@@ -280,7 +298,7 @@ def main():
     t0 = time.perf_counter()
     for k in range(args.steps):
         p2, x2 = workloads.batch_slice(pts, pxy, workloads.shard_start(rank, world, B, k + 1), B)
-        R2, T2, _, _, st2 = eng.solve_batch(stacks, p2, x2, orders=False)
+        R2, T2, _, _, st2 = eng.solve_batch(stacks, p2, x2, orders=False, precision=o.RCWA_PREC_MIXED)
         st = stacks[0]
         h2d += st.eps.nbytes + st.cx.nbytes + st.cy.nbytes + st.thickness.nbytes + p2.nbytes + x2.nbytes
         d2h += R2.nbytes + T2.nbytes + st2.nbytes
@@ -332,18 +350,35 @@ def main():
                 "frac": achieved / fp64_peak, "traffic": traffic,
                 "peak_source": "FP64 DGEMM measured in this run (cuBLAS via torch)",
                 "flops_per_launch": fl[dom] * jobs, "ms_per_launch": per_launch[dom]}
-    conv = None
-    if per_launch.get("conv_gather"):
-        pass
+    # the tensor-core products of the cascade: 4 complex GEMMs of n^3 per
+    # interface step, each 3 TF32 products (hi*hi, hi*lo, lo*hi) of 8 n^3 flops
+    n_iface = stacks[0].eps.shape[0] - 1
+    tc_ms = per_launch.get("cascade_gemm", 0.0)
+    tc_flops = 3 * 4 * 8.0 * n ** 3 * n_iface * B
+    tf32_peak = peaks.get("bf16_tflops", 0.0) / 2 if peaks.get("bf16_tflops") else None
+    tensor_gemm = None
+    if tc_ms > 0:
+        ach = tc_flops / (tc_ms * 1e-3) / 1e12
+        tensor_gemm = {"kernel": "zgemm_tf32x3 (tcgen05 kind::tf32)", "bound": "tensor", "achieved": ach,
+                       "peak": tf32_peak, "unit": "TFLOP/s", "frac": ach / tf32_peak if tf32_peak else None,
+                       "peak_source": "half the measured dense BF16 rate (TF32 runs at half the BF16 rate)",
+                       "flops_per_step": tc_flops, "ms_per_step": tc_ms}
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "vs_baseline": None, "dtype": "c128 with tf32x3 cascade products", "data": "synthetic",
             "config": {"workload": WORKLOAD, "batch_points_per_gpu": B, "orders": N, "matrix": n,
-                       "precision": "plain FP64 (mixed path not built)", "parallelism": f"replicas x{world}",
+                       "precision": "mixed: cascade GEMMs 3xTF32 on tcgen05 (FP32 accumulation); eigensolve, "
+                                    "interface/tau solves, half-spaces and efficiency sums FP64",
+                       "parallelism": f"replicas x{world}",
                        "l2": "per-step working set several GB > 126 MB L2"},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
-            "gpu_launches": launches, "clocks": clk, "roofline": roof, "grating_1d": grating,
+            "gpu_launches": launches, "clocks": clk, "roofline": roof, "tensor_gemm": tensor_gemm,
+            "plain_fp64": {"value": value64, "unit": "solves/s", "ms_per_step": t64_ms / args.steps,
+                           "stage_ms_per_step": {k: v / args.steps for k, v in stage64_ms.items()}},
+            "mixed_error": {"max_abs_dRT_vs_fp64": dRT, "max_abs_dorder_vs_fp64": dorders, "bound": 1e-4,
+                            "reference": "the FP64 engine on the same batch (1e-9 of the oracle in the tests)"},
+            "grating_1d": grating,
             "stage_ms_per_step": per_launch, "peaks": {"fp64_dgemm_tflops": fp64_peak,
                                                        "hbm_gbs": peaks.get("hbm_gbs"), "source": peak_kind}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -352,7 +387,6 @@ def main():
                                 "sample": "1 solve (point 0) of the sweep through the NumPy oracle, all BLAS threads"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    plan.close()
     eng.close()
     if world > 1:
         dist.destroy_process_group()
