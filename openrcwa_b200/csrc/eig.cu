@@ -117,6 +117,10 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
   cplx* a = s.v;    // work column, then v_j
   __shared__ cplx z[2 * kHb];
   cplx* u = s.uv;   // n
+  // the panel's reflectors V and Y = A0 V T column-major (column q at q*n),
+  // so that every sweep over the rows is coalesced
+  cplx* Vc = s.Vb;
+  cplx* Yc = s.Yb;
   for (int k = 0; k + 2 < n; k += nb) {
     const int jb = min(nb, n - 2 - k);
     cplx* T = s.Tall + (size_t)(k / nb) * nb * nb;
@@ -126,7 +130,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       // a = A0(:, j) - Y(:, :jj) conj(V(j, :jj))
       for (int i = tid; i < n; i += blockDim.x) {
         cplx acc = A[(size_t)i * lda + j];
-        for (int q = 0; q < jj; ++q) acc = cfma(cneg(s.Yb[(size_t)i * nb + q]), cconj(s.Vb[(size_t)j * nb + q]), acc);
+        for (int q = 0; q < jj; ++q) acc = cfma(cneg(Yc[(size_t)q * n + i]), cconj(Vc[(size_t)q * n + j]), acc);
         a[i] = acc;
       }
       __syncthreads();
@@ -134,7 +138,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         // a(k+1:) <- (I - V T^H V^H) a(k+1:):  z = V^H a, z = T^H z, a -= V z
         for (int q = wid; q < jj; q += nw) {
           cplx acc = mkc(0.0, 0.0);
-          for (int i = k + 1 + q + lane; i < n; i += 32) acc = cfmaconj(s.Vb[(size_t)i * nb + q], a[i], acc);
+          for (int i = k + 1 + q + lane; i < n; i += 32) acc = cfmaconj(Vc[(size_t)q * n + i], a[i], acc);
           for (int off = 16; off > 0; off >>= 1) {
             acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
             acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
@@ -150,7 +154,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         __syncthreads();
         for (int i = k + 1 + tid; i < n; i += blockDim.x) {
           cplx acc = a[i];
-          for (int q = 0; q < jj; ++q) acc = cfma(cneg(s.Vb[(size_t)i * nb + q]), z[nb + q], acc);
+          for (int q = 0; q < jj; ++q) acc = cfma(cneg(Vc[(size_t)q * n + i]), z[nb + q], acc);
           a[i] = acc;
         }
         __syncthreads();
@@ -177,7 +181,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         else if (i == j + 1) { A[(size_t)i * lda + j] = beta; vi = v0; }
         else { A[(size_t)i * lda + j] = a[i]; vi = a[i]; }
         if (tau == 0.0) vi = mkc(0.0, 0.0);
-        s.Vb[(size_t)i * nb + jj] = vi;
+        Vc[(size_t)jj * n + i] = vi;
         s.VH[(size_t)jj * n + i] = cconj(vi);
         a[i] = vi;
       }
@@ -211,7 +215,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       }
       for (int q = wid; q < jj; q += nw) {
         cplx acc = mkc(0.0, 0.0);
-        for (int i = j + 1 + lane; i < n; i += 32) acc = cfmaconj(s.Vb[(size_t)i * nb + q], s.Vb[(size_t)i * nb + jj], acc);
+        for (int i = j + 1 + lane; i < n; i += 32) acc = cfmaconj(Vc[(size_t)q * n + i], Vc[(size_t)jj * n + i], acc);
         for (int off = 16; off > 0; off >>= 1) {
           acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
           acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
@@ -222,8 +226,8 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       // Y(:, jj) = tau (u - Y(:, :jj) z); T(:jj, jj) = -tau T(:jj, :jj) z; T(jj, jj) = tau
       for (int i = tid; i < n; i += blockDim.x) {
         cplx acc = u[i];
-        for (int q = 0; q < jj; ++q) acc = cfma(cneg(s.Yb[(size_t)i * nb + q]), z[q], acc);
-        s.Yb[(size_t)i * nb + jj] = cscale(acc, tau);
+        for (int q = 0; q < jj; ++q) acc = cfma(cneg(Yc[(size_t)q * n + i]), z[q], acc);
+        Yc[(size_t)jj * n + i] = cscale(acc, tau);
       }
       if (tid < jj) {
         cplx acc = mkc(0.0, 0.0);
@@ -238,8 +242,8 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
     const int m2 = n - c0;
     if (m2 > 0) {
       // A(:, c0:) -= Y V(c0:, :)^H
-      cta_gemm<false, false>(tsm, n, m2, jb, s.Yb, nb, s.VH + c0, n, A + c0, lda, A + c0, lda, mkc(-1.0, 0.0),
-                             mkc(1.0, 0.0));
+      cta_gemm<true, false>(tsm, n, m2, jb, Yc, n, s.VH + c0, n, A + c0, lda, A + c0, lda, mkc(-1.0, 0.0),
+                            mkc(1.0, 0.0));
       // W = V(k+1:, :)^H A(k+1:, c0:)  (jb x m2), W2 = T^H W, A(k+1:, c0:) -= V(k+1:, :) W2
       cta_gemm<false, false>(tsm, jb, m2, n - k - 1, s.VH + k + 1, n, A + (size_t)(k + 1) * lda + c0, lda, s.Wb + c0, n,
                              nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
@@ -250,9 +254,9 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       __syncthreads();
       cta_gemm<false, false>(tsm, jb, m2, jb, s.Vt, nb, s.Wb + c0, n, s.Yb + c0, n, nullptr, 0, mkc(1.0, 0.0),
                              mkc(0.0, 0.0));
-      cta_gemm<false, false>(tsm, n - k - 1, m2, jb, s.Vb + (size_t)(k + 1) * nb, nb, s.Yb + c0, n,
-                             A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
-                             mkc(-1.0, 0.0), mkc(1.0, 0.0));
+      cta_gemm<true, false>(tsm, n - k - 1, m2, jb, Vc + k + 1, n, s.Yb + c0, n,
+                            A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
+                            mkc(-1.0, 0.0), mkc(1.0, 0.0));
     }
   }
   // Z (column-major, i.e. Zt = Z^T row-major) = Q, accumulated backwards:
