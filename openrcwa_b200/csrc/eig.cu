@@ -40,6 +40,15 @@ struct Scratch {
   double* tau; // n
 };
 
+#ifdef RCWA_EIG_STATS
+// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles,
+// 8 early-deflation cycles, 9 single-shift cycles, 10 Schur cycles, 11 early deflations, 12 deflated by them
+__device__ unsigned long long g_eig_stats[16];
+#define STAT_ADD(i, v) do { if (threadIdx.x == 0) atomicAdd(&g_eig_stats[i], (unsigned long long)(v)); } while (0)
+#else
+#define STAT_ADD(i, v) do { } while (0)
+#endif
+
 __device__ Scratch scratch_for(void* work, int n, int b) {
   const size_t nn = (size_t)n * n;
   const size_t nk = (size_t)n * kHb;
@@ -122,6 +131,9 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
   cplx* Vc = s.Vb;
   cplx* Yc = s.Yb;
   for (int k = 0; k + 2 < n; k += nb) {
+#ifdef RCWA_EIG_STATS
+    const long long c_p0 = clock64();
+#endif
     const int jb = min(nb, n - 2 - k);
     cplx* T = s.Tall + (size_t)(k / nb) * nb * nb;
     for (int idx = tid; idx < nb * nb; idx += blockDim.x) T[idx] = mkc(0.0, 0.0);
@@ -237,6 +249,10 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       if (tid == 0) T[jj * nb + jj] = mkc(tau, 0.0);
       __syncthreads();
     }
+#ifdef RCWA_EIG_STATS
+    const long long c_p1 = clock64();
+    STAT_ADD(13, c_p1 - c_p0);
+#endif
     // trailing columns c0..n-1
     const int c0 = k + jb;
     const int m2 = n - c0;
@@ -258,7 +274,13 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
                             A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
                             mkc(-1.0, 0.0), mkc(1.0, 0.0));
     }
+#ifdef RCWA_EIG_STATS
+    STAT_ADD(14, clock64() - c_p1);
+#endif
   }
+#ifdef RCWA_EIG_STATS
+  const long long c_q0 = clock64();
+#endif
   // Z (column-major, i.e. Zt = Z^T row-major) = Q, accumulated backwards:
   // Zt(k+1:, k+1:) -= (Zt conj(V)) T^T V^T
   for (size_t idx = tid; idx < (size_t)n * n; idx += blockDim.x)
@@ -299,6 +321,9 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
     if (i > j + 1) A[(size_t)i * lda + j] = mkc(0.0, 0.0);
   }
   __syncthreads();
+#ifdef RCWA_EIG_STATS
+  STAT_ADD(15, clock64() - c_q0);
+#endif
 }
 
 // ---------------------------------------------------------------- QR
@@ -506,14 +531,6 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
   return 0;
 }
 
-#ifdef RCWA_EIG_STATS
-// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles,
-// 8 early-deflation cycles, 9 single-shift cycles, 10 Schur cycles, 11 early deflations, 12 deflated by them
-__device__ unsigned long long g_eig_stats[16];
-#define STAT_ADD(i, v) do { if (threadIdx.x == 0) atomicAdd(&g_eig_stats[i], (unsigned long long)(v)); } while (0)
-#else
-#define STAT_ADD(i, v) do { } while (0)
-#endif
 
 // ---------------------------------------------------------------- multishift QR
 // Small-bulge multishift QR (the scheme of Braman, Byers and Mathias, SIAM J.
