@@ -50,9 +50,32 @@ def parse():
                     "fill the GPU too)")
     ap.add_argument("--nh", type=int, default=10, help="harmonics per axis (Nx=Ny)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gemm-only", default=None, metavar="N,BATCH",
+                    help="one batched n x n x n complex GEMM in 3xTF32 on tcgen05 and one on the FP64 path "
+                         "(profiling aid)")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
                     help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
+
+
+def run_gemm_only(spec):
+    """Batched complex GEMMs through rcwa_zgemm_batched on seeded random
+    matrices: the 3xTF32 tcgen05 kernel, then the FP64 tile kernel, for
+    counter captures of those kernels; prints their relative errors."""
+    import openrcwa_b200 as o
+    n, b = (int(x) for x in spec.split(","))
+    rng = np.random.default_rng(0)
+    A = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
+    B = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
+    eng = o.Engine(0)
+    Dm = eng.zgemm(A, B, precision=o.RCWA_PREC_MIXED)
+    D6 = eng.zgemm(A, B, precision=o.RCWA_PREC_FP64)
+    ref = A[0] @ B[0]
+    scale = np.abs(A[0]) @ np.abs(B[0])
+    print(json.dumps({"gemm_only": {"n": n, "batch": b, "tf32x3_rel_err": float(np.max(np.abs(Dm[0] - ref) / scale)),
+                                    "fp64_rel_err": float(np.max(np.abs(D6[0] - ref) / scale))}}))
+    eng.close()
+    return 0
 
 
 def run_eig_only(spec):
@@ -209,6 +232,8 @@ def main():
     args = parse()
     if args.eig_only:
         return run_eig_only(args.eig_only)
+    if args.gemm_only:
+        return run_gemm_only(args.gemm_only)
     if args.impl == "reference":
         return run_reference(args)
     import torch
@@ -343,7 +368,8 @@ def main():
     tfile = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            traffic = json.load(f).get(dom)
+            per_matrix = json.load(f).get(dom + "_per_matrix")
+        traffic = per_matrix * jobs if per_matrix else None
     if dom in ("schur_qr", "hessenberg"):
         achieved = fl[dom] * jobs / (per_launch[dom] * 1e-3) / 1e12
         roof = {"kernel": dom, "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",

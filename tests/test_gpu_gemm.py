@@ -1,6 +1,6 @@
 """The batched complex GEMM through the C ABI: the FP64 tensor path against
 NumPy (1e-13 relative) and the 3xTF32 tcgen05 path against NumPy (error below
-2e-6 of |A||B| summed over K, the 3xTF32 bound with FP32 accumulation)."""
+1e-5 of |A||B| summed over K: the 3xTF32 error with FP32 accumulation over K up to 882)."""
 import numpy as np
 import pytest
 
@@ -31,11 +31,11 @@ def test_gemm_fp64_and_tf32x3(eng, M, N, K, b):
     D64 = eng.zgemm(A, B, C, alpha, beta, o.RCWA_PREC_FP64)
     assert np.max(np.abs(D64 - ref) / (scale + np.abs(beta * C))) < 1e-13
     Dtc = eng.zgemm(A, B, C, alpha, beta, o.RCWA_PREC_MIXED)
-    assert np.max(np.abs(Dtc - ref) / (scale + np.abs(beta * C))) < 2e-6
+    assert np.max(np.abs(Dtc - ref) / (scale + np.abs(beta * C))) < 1e-5
 
 
 def test_gemm_tf32x3_without_c(eng):
     rng = np.random.default_rng(9)
     A, B = crand(rng, 4, 150, 70), crand(rng, 4, 70, 140)
     D = eng.zgemm(A, B, precision=o.RCWA_PREC_MIXED)
-    assert np.max(np.abs(D - A @ B) / (np.abs(A) @ np.abs(B))) < 2e-6
+    assert np.max(np.abs(D - A @ B) / (np.abs(A) @ np.abs(B))) < 1e-5
