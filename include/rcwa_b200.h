@@ -180,6 +180,29 @@ int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
 int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch, const rcwa_cplx* A, const rcwa_cplx* B,
                        const rcwa_cplx* C, rcwa_cplx alpha, rcwa_cplx beta, int precision, rcwa_cplx* D);
 
+/* ---- learned surrogate ------------------------------------------------------
+ * No counterpart in the reference.  A fully connected network with n_layers
+ * hidden layers of n_hidden units (GELU) mapping n_in grating parameters to
+ * n_out efficiencies, trained on efficiencies this engine computed; the
+ * engine's FP64 solve is its fallback (openrcwa_b200/surrogate.py).
+ * Parameters, in order for every layer: W (out x in, row-major) then b (out).
+ * Training: FP32 weights, minibatch Adam on the mean squared error.
+ * rcwa_mlp_predict: BF16 weights and activations with FP32 accumulation on the
+ * tensor cores (n_hidden, n_out <= 256); rcwa_mlp_predict_fp32: the FP32
+ * training forward.  Rows are host float arrays [n][n_in] / [n][n_out]. */
+typedef struct rcwa_mlp rcwa_mlp;
+int rcwa_mlp_create(rcwa_engine* e, int n_in, int n_hidden, int n_layers, int n_out, unsigned long long seed,
+                    rcwa_mlp** out);
+void rcwa_mlp_destroy(rcwa_mlp* m);
+long long rcwa_mlp_param_count(const rcwa_mlp* m);
+int rcwa_mlp_get_params(rcwa_mlp* m, float* params);
+int rcwa_mlp_set_params(rcwa_mlp* m, const float* params);
+int rcwa_mlp_set_data(rcwa_mlp* m, const float* X, const float* Y, int n);
+int rcwa_mlp_train(rcwa_mlp* m, int epochs, int batch, float lr, unsigned long long seed, float* loss_per_epoch);
+int rcwa_mlp_loss_grad(rcwa_mlp* m, const float* X, const float* Y, int n, double* loss, float* grad);
+int rcwa_mlp_predict_fp32(rcwa_mlp* m, const float* X, int n, float* Y);
+int rcwa_mlp_predict(rcwa_mlp* m, const float* X, int n, float* Y);
+
 /* ---- slab S-matrices and the Redheffer star product -------------------------
  * Batched, FP64, host buffers; every matrix row-major [batch][n*n].
  *

@@ -37,6 +37,8 @@ EXPORTS = [
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
     "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_zgemm_batched",
+    "rcwa_mlp_create", "rcwa_mlp_destroy", "rcwa_mlp_param_count", "rcwa_mlp_get_params", "rcwa_mlp_set_params",
+    "rcwa_mlp_set_data", "rcwa_mlp_train", "rcwa_mlp_loss_grad", "rcwa_mlp_predict_fp32", "rcwa_mlp_predict",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -120,6 +122,20 @@ def load() -> C.CDLL:
     lib.rcwa_star_product_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 8 + [_IP]
     lib.rcwa_zgemm_batched.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, rcwa_cplx, rcwa_cplx, C.c_int, C.c_void_p]
+    _FP = C.POINTER(C.c_float)
+    lib.rcwa_mlp_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_ulonglong,
+                                    C.POINTER(C.c_void_p)]
+    lib.rcwa_mlp_destroy.argtypes = [C.c_void_p]
+    lib.rcwa_mlp_destroy.restype = None
+    lib.rcwa_mlp_param_count.argtypes = [C.c_void_p]
+    lib.rcwa_mlp_param_count.restype = C.c_longlong
+    lib.rcwa_mlp_get_params.argtypes = [C.c_void_p, _FP]
+    lib.rcwa_mlp_set_params.argtypes = [C.c_void_p, _FP]
+    lib.rcwa_mlp_set_data.argtypes = [C.c_void_p, _FP, _FP, C.c_int]
+    lib.rcwa_mlp_train.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_ulonglong, _FP]
+    lib.rcwa_mlp_loss_grad.argtypes = [C.c_void_p, _FP, _FP, C.c_int, _DP, _FP]
+    lib.rcwa_mlp_predict_fp32.argtypes = [C.c_void_p, _FP, C.c_int, _FP]
+    lib.rcwa_mlp_predict.argtypes = [C.c_void_p, _FP, C.c_int, _FP]
     _lib = lib
     return lib
 
@@ -404,6 +420,71 @@ class Plan:
     def close(self):
         if self.h:
             self.eng.lib.rcwa_plan_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _f(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Mlp:
+    """The surrogate network of rcwa_mlp_* (training and inference on the GPU)."""
+
+    def __init__(self, eng: Engine, n_in, n_hidden, n_layers, n_out, seed=0):
+        self.eng = eng
+        self.n_in, self.n_out = n_in, n_out
+        self.dims = [n_in] + [n_hidden] * n_layers + [n_out]
+        h = C.c_void_p()
+        eng._check(eng.lib.rcwa_mlp_create(eng.h, n_in, n_hidden, n_layers, n_out, seed, C.byref(h)), "mlp_create")
+        self.h = h
+
+    def param_count(self):
+        return int(self.eng.lib.rcwa_mlp_param_count(self.h))
+
+    def get_params(self):
+        p = np.zeros(self.param_count(), dtype=np.float32)
+        self.eng._check(self.eng.lib.rcwa_mlp_get_params(self.h, _f(p)), "mlp_get_params")
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        self.eng._check(self.eng.lib.rcwa_mlp_set_params(self.h, _f(p)), "mlp_set_params")
+
+    def set_data(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        self.eng._check(self.eng.lib.rcwa_mlp_set_data(self.h, _f(X), _f(Y), X.shape[0]), "mlp_set_data")
+
+    def train(self, epochs, batch, lr, seed=0):
+        loss = np.zeros(epochs, dtype=np.float32)
+        self.eng._check(self.eng.lib.rcwa_mlp_train(self.h, epochs, batch, lr, seed, _f(loss)), "mlp_train")
+        return loss
+
+    def loss_grad(self, X, Y):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.ascontiguousarray(Y, dtype=np.float32)
+        loss = C.c_double()
+        g = np.zeros(self.param_count(), dtype=np.float32)
+        self.eng._check(self.eng.lib.rcwa_mlp_loss_grad(self.h, _f(X), _f(Y), X.shape[0], C.byref(loss), _f(g)),
+                        "mlp_loss_grad")
+        return loss.value, g
+
+    def predict(self, X, tensor_cores=True):
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        Y = np.zeros((X.shape[0], self.n_out), dtype=np.float32)
+        fn = self.eng.lib.rcwa_mlp_predict if tensor_cores else self.eng.lib.rcwa_mlp_predict_fp32
+        self.eng._check(fn(self.h, _f(X), X.shape[0], _f(Y)), "mlp_predict")
+        return Y
+
+    def close(self):
+        if self.h:
+            self.eng.lib.rcwa_mlp_destroy(self.h)
             self.h = None
 
     def __del__(self):
