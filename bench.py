@@ -50,12 +50,64 @@ def parse():
                     "fill the GPU too)")
     ap.add_argument("--nh", type=int, default=10, help="harmonics per axis (Nx=Ny)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--surrogate", action="store_true",
+                    help="the learned-surrogate pipeline on a reduced cfg4 (Nx=Ny=5 solves): data generation, "
+                         "GPU training, tensor-core inference, surrogate plus fallback with a 2%% audit")
     ap.add_argument("--gemm-only", default=None, metavar="N,BATCH",
                     help="one batched n x n x n complex GEMM in 3xTF32 on tcgen05 and one on the FP64 path "
                          "(profiling aid)")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
                     help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
+
+
+def run_surrogate(args):
+    """cfg4's pipeline on a reduced grid (nH = 2, the 25 orders m, n in [-2, 2]
+    are then all the orders): 200k training solves by the FP64 engine, the
+    network (4 x 256 GELU) trained on the GPU, 65,536-query batches answered by
+    the network on the tensor cores and by the surrogate with fallback (2%
+    audit), against the FP64 solve of the same queries."""
+    import openrcwa_b200 as o
+    from openrcwa_b200 import surrogate as sg
+    eng = o.Engine(0)
+    rng = np.random.default_rng(0)
+    nh = 2
+    t0 = time.perf_counter()
+    P = sg.sample(200000, rng)
+    Y = sg.solve(eng, P, nh, chunk=4096)
+    t_gen = time.perf_counter() - t0
+    sur = sg.Surrogate(eng, nh, hidden=256, layers=4, seed=1)
+    t0 = time.perf_counter()
+    loss = sur.fit(P, Y, epochs=40, batch=512, lr=1e-3, seed=3)
+    t_train = time.perf_counter() - t0
+    Q = sg.sample(65536, rng)
+    sur.predict(Q[:1024])
+    t0 = time.perf_counter()
+    for _ in range(5):
+        Yn = sur.predict(Q)
+    t_net = (time.perf_counter() - t0) / 5
+    t0 = time.perf_counter()
+    r = sur.query(Q, audit=0.02, seed=5)
+    t_q = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    Ys = sg.solve(eng, Q, nh, chunk=4096)
+    t_solve = time.perf_counter() - t0
+    err = np.abs(r["Y"] - Ys)
+    line = {"surrogate": {
+        "config": "reduced cfg4: one-rectangle 2D grating, Nx=Ny=5 solves, 11 parameters -> 52 efficiencies",
+        "train_solves": len(P), "generation_solves_per_s": len(P) / t_gen, "train_s": t_train,
+        "final_train_mse": float(loss[-1]),
+        "query_batch": len(Q), "network_queries_per_s": len(Q) / t_net,
+        "surrogate_with_fallback_queries_per_s": len(Q) / t_q, "fp64_solve_queries_per_s": len(Q) / t_solve,
+        "speedup_network": t_solve / t_net, "speedup_with_fallback": t_solve / t_q,
+        "fallback_fraction": float(np.mean(r["source"] != sg.SOURCE_NET)),
+        "audit_max_abs_err": float(np.max(r["audit_err"])) if len(r["audit_err"]) else None,
+        "rms_err_vs_solve": float(np.sqrt(np.mean(err ** 2))), "max_abs_err_vs_solve": float(np.max(err)),
+        "network_rms_err": float(np.sqrt(np.mean((Yn - Ys) ** 2)))}}
+    print(json.dumps(line), flush=True)
+    sur.close()
+    eng.close()
+    return 0
 
 
 def run_gemm_only(spec):
@@ -234,6 +286,8 @@ def main():
         return run_eig_only(args.eig_only)
     if args.gemm_only:
         return run_gemm_only(args.gemm_only)
+    if args.surrogate:
+        return run_surrogate(args)
     if args.impl == "reference":
         return run_reference(args)
     import torch
