@@ -42,7 +42,10 @@ extern "C" {
 #define RCWA_PREC_MIXED 1     /* cascade GEMMs (F, G, Rud, Tdd) in 3xTF32 on the
                                  tensor cores with FP32 accumulation; the
                                  eigensolve, the interface and tau solves, the
-                                 half-spaces and the efficiency sums stay FP64  */
+                                 half-spaces and the efficiency sums stay FP64.
+                                 Stacks with a metallic layer (Re eps < 0 in
+                                 some cell) keep FP64 products: their cascade
+                                 is too ill-conditioned for 3xTF32             */
 
 typedef struct { double re, im; } rcwa_cplx;
 

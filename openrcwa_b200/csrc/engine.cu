@@ -18,6 +18,7 @@
 #include <cstring>
 #include <functional>
 #include <map>
+#include <tuple>
 #include <memory>
 #include <set>
 #include <string>
@@ -90,6 +91,7 @@ struct rcwa_plan {
   double* dTrn = nullptr;
   int* dStatus = nullptr;
   int* dTcErr = nullptr;   // set when a tensor-core completion wait ran out
+  int* dTcScale = nullptr; // operand scale exponents of the tensor-core products (2 x 1024)
   int precision = RCWA_PREC_FP64;
   std::vector<std::function<cudaError_t(cudaStream_t, long long&, StageProf&)>> steps;
   long long launches = 0;
@@ -251,6 +253,9 @@ struct ChunkWork {
   size_t hW0 = 0, hV0 = 0, hWL = 0, hVL = 0, hg0 = 0, hgL = 0;
   size_t Rud = 0, Tdd = 0, F = 0, G = 0, tau = 0, IE = 0, IH = 0, WLU = 0, VLU = 0, pipiv = 0, pinfo = 0;
   size_t total = 0;
+  // mixed plans: this chunk's products stay FP64 (its stacks have a layer
+  // with Re(eps) < 0, whose cascade the 3xTF32 products cannot resolve)
+  bool fp64 = false;
 };
 
 }  // namespace
@@ -384,6 +389,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     size_t oRef = ol.take(sizeof(double) * std::max<size_t>(acc, 1)), oTrn = ol.take(sizeof(double) * std::max<size_t>(acc, 1));
     size_t oS = ol.take(sizeof(int) * n_pts);
     size_t oE = ol.take(sizeof(int));
+    size_t oSc = ol.take(sizeof(int) * 2 * 1024);
     if (cudaMalloc(&P->outputs.p, ol.off) != cudaSuccess) return fail(e, RCWA_ERR_NOMEM, "output allocation failed");
     P->outputs.bytes = ol.off;
     char* b = (char*)P->outputs.p;
@@ -393,6 +399,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     P->dTrn = (double*)(b + oTrn);
     P->dStatus = (int*)(b + oS);
     P->dTcErr = (int*)(b + oE);
+    P->dTcScale = (int*)(b + oSc);
   }
 
   // ---- chunking: group by (nx, ny), then fill chunks up to the memory budget
@@ -400,16 +407,28 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   cudaMemGetInfo(&free_b, &total_b);
   if (!e->work_cache_busy) free_b += e->work_cache_bytes;
   const size_t budget = std::min<size_t>((size_t)(0.6 * free_b), (size_t)96 << 30);
-  std::map<std::pair<int, int>, std::vector<int>> groups;
-  for (int p = 0; p < n_pts; ++p) groups[{si[pts[p].stack].nx, si[pts[p].stack].ny}].push_back(p);
+  // In mixed plans, stacks with a metallic layer (Re(eps) < 0 in some cell)
+  // keep FP64 products: the evanescent modes of such layers make the cascade
+  // ill-conditioned beyond what 3xTF32 (about 21 bits) can carry.
+  std::vector<char> metallic(n_stacks, 0);
+  for (int s = 0; s < n_stacks; ++s)
+    for (const cplx& z : si[s].eps)
+      if (z.x < 0.0) { metallic[s] = 1; break; }
+  std::map<std::tuple<int, int, int>, std::vector<int>> groups;
+  for (int p = 0; p < n_pts; ++p) {
+    const int s = pts[p].stack;
+    const int f64 = precision == RCWA_PREC_MIXED ? metallic[s] : 0;
+    groups[{si[s].nx, si[s].ny, f64}].push_back(p);
+  }
   std::vector<ChunkWork> chunks;
   std::vector<int> chunk_N;
   for (auto& g : groups) {
-    const int N = g.first.first * g.first.second;
+    const int N = std::get<0>(g.first) * std::get<1>(g.first);
+    const bool f64 = std::get<2>(g.first) != 0;
     size_t used = 0;
     ChunkWork cur;
     auto flush = [&]() {
-      if (!cur.points.empty()) { chunks.push_back(cur); chunk_N.push_back(N); }
+      if (!cur.points.empty()) { cur.fp64 = f64; chunks.push_back(cur); chunk_N.push_back(N); }
       cur = ChunkWork();
       used = 0;
     };
@@ -767,11 +786,12 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         int* pinfo = (int*)(wb + c.pinfo);
         int* status = P->dStatus;
         int* tcerr = P->dTcErr;
-        const bool mixed = precision == RCWA_PREC_MIXED;
+        int* tcscale = P->dTcScale;
+        const bool mixed = precision == RCWA_PREC_MIXED && !c.fp64;
         P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
           // the cascade products: FP64 tensor path, or 3xTF32 on tcgen05
           auto product = [&](const GemmArgs& ga) {
-            return mixed ? zgemm_tf32x3_batched(ga, tcerr, st) : zgemm_batched(ga, st);
+            return mixed ? zgemm_tf32x3_batched(ga, tcscale, tcerr, st) : zgemm_batched(ga, st);
           };
           char* m = (char*)plan->meta.p;
           auto cpa = [m](size_t o) { return (const cplx* const*)(m + o); };

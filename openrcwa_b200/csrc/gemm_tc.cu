@@ -92,7 +92,34 @@ __device__ __forceinline__ void st_plane4(float* plane, int off, float a, float 
   *reinterpret_cast<float4*>(reinterpret_cast<char*>(plane) + off) = make_float4(a, b, c, d);
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g, int* err) {
+// Largest |re|, |im| of each batch item's A (z = 0) or B (z = 1) as a binary
+// exponent e with max < 2^e, combined over blocks by atomicMax into exps
+// (initialised very negative; an all-zero matrix keeps that value).
+__global__ void tc_scale_kernel(GemmArgs g, int* exps) {
+  __shared__ double red[8];
+  const int b = blockIdx.y, isB = blockIdx.z;
+  const cplx* X = isB ? (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB : (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
+  const int rows = isB ? g.K : g.M, cols = isB ? g.N : g.K, ld = isB ? g.ldb : g.lda;
+  double mx = 0.0;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < (size_t)rows * cols;
+       idx += (size_t)gridDim.x * blockDim.x) {
+    const cplx v = X[(idx / cols) * ld + idx % cols];
+    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) mx = fmax(mx, red[w]);
+    if (mx > 0.0 && mx < INFINITY) {
+      int e;
+      frexp(mx, &e);  // mx = f 2^e, 0.5 <= f < 1
+      atomicMax(&exps[isB * gridDim.y + b], e);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g, const int* exps, int* err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
   float* planes = reinterpret_cast<float*>(tsm);
   float* Arh = planes;
@@ -113,6 +140,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
   const cplx* A = (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
   const cplx* B = (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB;
   const uint32_t mb = smem_u32(mbar);
+  // exact power-of-two operand scales (an all-zero operand keeps scale 1)
+  const int eA = max(exps[b], -1000), eB = max(exps[g.batch + b], -1000);
+  const double sA = ldexp(1.0, eA > -1000 ? -eA : 0), sB = ldexp(1.0, eB > -1000 ? -eB : 0);
+  const int eAB = (eA > -1000 ? eA : 0) + (eB > -1000 ? eB : 0);
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -156,8 +187,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
           const int gk = k0 + 4 * q + j;
           cplx v = mkc(0.0, 0.0);
           if (gm < g.M && gk < g.K) v = A[(size_t)gm * g.lda + gk];
-          split_tf32(v.x, rh[j], rl[j]);
-          split_tf32(v.y, ih[j], il[j]);
+          split_tf32(v.x * sA, rh[j], rl[j]);
+          split_tf32(v.y * sA, ih[j], il[j]);
         }
         const int off = plane_off(tid, 4 * q);
         st_plane4(Arh, off, rh[0], rh[1], rh[2], rh[3]);
@@ -177,8 +208,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
           const int gk = k0 + 4 * q + j;
           cplx v = mkc(0.0, 0.0);
           if (gn < g.N && gk < g.K) v = B[(size_t)gk * g.ldb + gn];
-          split_tf32(v.x, rh[j], rl[j]);
-          split_tf32(v.y, ih[j], il[j]);
+          split_tf32(v.x * sB, rh[j], rl[j]);
+          split_tf32(v.y * sB, ih[j], il[j]);
         }
         const int off = plane_off(tid, 4 * q);
         st_plane4(Brh, off, rh[0], rh[1], rh[2], rh[3]);
@@ -250,7 +281,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
         for (int j = 0; j < 16; ++j) {
           const int n = n0 + cb + j;
           if (n < g.N) {
-            cplx v = cmul(g.alpha, mkc((double)__uint_as_float(re[j]), (double)__uint_as_float(im[j])));
+            cplx v = cmul(g.alpha, mkc(ldexp((double)__uint_as_float(re[j]), eAB),
+                                       ldexp((double)__uint_as_float(im[j]), eAB)));
             if (Crow) v = cfma(g.beta, Crow[n], v);
             if (m == n) v = cadd(v, g.gammaI);
             Drow[n] = v;
@@ -267,9 +299,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
 
 }  // namespace
 
-cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* err, cudaStream_t st) {
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st) {
   if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
-  if (g.K <= 0 || g.transA || g.transB || g.s || !err) return cudaErrorInvalidValue;
+  if (g.K <= 0 || g.transA || g.transB || g.s || !err || !scale_ws) return cudaErrorInvalidValue;
   static bool attr_set[64] = {};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -279,8 +311,13 @@ cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* err, cudaStream_t st) {
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
+  // 0x80 bytes: every exponent starts at a very negative value
+  cudaError_t e = cudaMemsetAsync(scale_ws, 0x80, sizeof(int) * 2 * g.batch, st);
+  if (e != cudaSuccess) return e;
+  tc_scale_kernel<<<dim3(16, g.batch, 2), 256, 0, st>>>(g, scale_ws);
+  ++launch_counter();
   dim3 grid((g.N + kTcN - 1) / kTcN, (g.M + kTcM - 1) / kTcM, g.batch);
-  zgemm_tf32x3_kernel<<<grid, kTcThreads, kTcSmem, st>>>(g, err);
+  zgemm_tf32x3_kernel<<<grid, kTcThreads, kTcSmem, st>>>(g, scale_ws, err);
   ++launch_counter();
   return cudaGetLastError();
 }

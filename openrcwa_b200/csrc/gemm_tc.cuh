@@ -6,6 +6,9 @@
 #include "linalg.cuh"
 
 // D = alpha*A*B + beta*C + gammaI*I for every batch item (A, B not transposed,
-// no diagonal scaling).  err (device int) is set to 1 if a tensor-core
-// completion wait runs out; the affected tile is then not written.
-cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* err, cudaStream_t st);
+// no diagonal scaling).  Every A and B is scaled by a power of two that brings
+// its largest entry below 1 before the split (FP32 range), and the product is
+// scaled back exactly; scale_ws is device scratch of 2*batch ints.  err
+// (device int) is set to 1 if a tensor-core completion wait runs out; the
+// affected tile is then not written.
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st);

@@ -258,8 +258,10 @@ extern "C" int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch
   if (cudaSetDevice(e->device) != cudaSuccess) return RCWA_ERR_CUDA;
   const size_t mk = (size_t)M * K, kn = (size_t)K * N, mn = (size_t)M * N;
   Dev dA(sizeof(cplx) * mk * batch), dB(sizeof(cplx) * kn * batch), dC(sizeof(cplx) * mn * batch),
-      dD(sizeof(cplx) * mn * batch), dp(sizeof(void*) * 2 * batch), derr(sizeof(int));
-  if (!dA.p || !dB.p || !dC.p || !dD.p || !dp.p || !derr.p) return set_err(e, RCWA_ERR_NOMEM, "allocation failed");
+      dD(sizeof(cplx) * mn * batch), dp(sizeof(void*) * 2 * batch), derr(sizeof(int)),
+      dscale(sizeof(int) * 2 * batch);
+  if (!dA.p || !dB.p || !dC.p || !dD.p || !dp.p || !derr.p || !dscale.p)
+    return set_err(e, RCWA_ERR_NOMEM, "allocation failed");
   const bool useC = beta.re != 0.0 || beta.im != 0.0;
   if (!up(dA.p, (const cplx*)A, mk * batch) || !up(dB.p, (const cplx*)B, kn * batch) ||
       (useC && !up(dC.p, (const cplx*)C, mn * batch)))
@@ -282,7 +284,7 @@ extern "C" int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch
   g.beta = mkc(beta.re, beta.im);
   g.gammaI = mkc(0.0, 0.0);
   g.batch = batch;
-  cudaError_t err = precision == RCWA_PREC_MIXED ? zgemm_tf32x3_batched(g, derr.as<int>(), e->stream)
+  cudaError_t err = precision == RCWA_PREC_MIXED ? zgemm_tf32x3_batched(g, dscale.as<int>(), derr.as<int>(), e->stream)
                                                  : zgemm_batched(g, e->stream);
   if (err != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess)
     return set_err(e, RCWA_ERR_CUDA, "GEMM kernel failed");

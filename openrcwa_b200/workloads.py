@@ -87,6 +87,45 @@ def pillars_2d(seed=0, nH=10, n_lambda=256, n_angle=8, n_layers=5):
     return [st], np.array(pts), np.array(pxy, dtype=complex)
 
 
+def lorentz_eps(einf, ae, be, ce, omega):
+    """Single-pole Lorentz permittivity einf + ae^2 / (ce^2 - w^2 - i be w)
+    (the pole model of sol/rcwa_bridge.cpp:116-121, angular frequencies)."""
+    return einf + ae * ae / (ce * ce - omega * omega - 1j * be * omega)
+
+
+def uneven_batch(seed=0, n_instances=4096, nh_range=(3, 15), max_layers=10, period=4e-7):
+    """Independent 2D-grating instances of uneven size: nH = Nx = Ny ~ U{3..15}
+    (49-961 orders), 1..max_layers patterned layers, each one rectangle with
+    fills ~U(0.1, 0.9) and thickness ~U(20, 500) nm, eps1 from a one-pole
+    Lorentz model (einf ~U(1, 4), ae ~U(1e15, 5e15), be ~U(1e13, 1e14),
+    ce ~U(2e15, 6e15) rad/s) or a lossy metal -U(5, 30) + iU(0.5, 3), eps2 = 1;
+    one point per instance at lambda ~U(400, 1000) nm, theta ~U(0, 70) deg,
+    phi = 0.  Returns (stacks, points, pxy) with TE and TM per point."""
+    rng = np.random.default_rng(seed)
+    stacks, pts, pxy = [], [], []
+    for i in range(n_instances):
+        nh = int(rng.integers(nh_range[0], nh_range[1] + 1))
+        nl = int(rng.integers(1, max_layers + 1))
+        lam = rng.uniform(400e-9, 1000e-9)
+        omega = 2 * PI * 2.99792458e8 / lam
+        layers = []
+        for _ in range(nl):
+            fx, fy = rng.uniform(0.1, 0.9, 2)
+            d = rng.uniform(20e-9, 500e-9)
+            if rng.random() < 0.5:
+                e1 = lorentz_eps(rng.uniform(1, 4), rng.uniform(1e15, 5e15), rng.uniform(1e13, 1e14),
+                                 rng.uniform(2e15, 6e15), omega)
+            else:
+                e1 = complex(-rng.uniform(5, 30), rng.uniform(0.5, 3))
+            layers.append((e1, 1.0, fx, fy, d))
+        stacks.append(rect_stack(nh, nh, period, period, layers))
+        th = rng.uniform(0, 70)
+        k0 = 2 * PI / lam
+        pts.append((i, lam, k0 * math.sin(math.radians(th)), 0.0))
+        pxy.append(pol_vectors(th, 0.0))
+    return stacks, np.array(pts), np.array(pxy, dtype=complex)
+
+
 def batch_slice(points, pxy, start, count):
     idx = (np.arange(count) + start) % len(points)
     return points[idx], pxy[idx]

@@ -39,3 +39,12 @@ def test_gemm_tf32x3_without_c(eng):
     A, B = crand(rng, 4, 150, 70), crand(rng, 4, 70, 140)
     D = eng.zgemm(A, B, precision=o.RCWA_PREC_MIXED)
     assert np.max(np.abs(D - A @ B) / (np.abs(A) @ np.abs(B))) < 1e-5
+
+
+def test_gemm_tf32x3_outside_fp32_range(eng):
+    # operands far outside the FP32 range are scaled by powers of two first
+    rng = np.random.default_rng(11)
+    A, B = crand(rng, 2, 96, 80) * 1e50, crand(rng, 2, 80, 70) * 1e-60
+    D = eng.zgemm(A, B, precision=o.RCWA_PREC_MIXED)
+    assert np.all(np.isfinite(D))
+    assert np.max(np.abs(D - A @ B) / (np.abs(A) @ np.abs(B))) < 1e-5

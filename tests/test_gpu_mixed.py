@@ -71,3 +71,19 @@ def test_mixed_lossless_energy(eng):
     R, T, _, _, status = eng.solve_batch([st], pts, pxy, orders=False, precision=o.RCWA_PREC_MIXED)
     assert not np.any(status)
     assert np.max(np.abs(R + T - 1.0)) < TOL_MIXED
+
+
+def test_mixed_keeps_fp64_products_for_metal(eng):
+    # a stack with a metal layer: the mixed plan routes it to FP64 products,
+    # so its results equal the FP64 plan's bit for bit
+    from openrcwa_b200 import workloads
+    st = workloads.rect_stack(4, 4, 4e-7, 4e-7, [(complex(-20.0, 1.5), 1.0, 0.5, 0.4, 2e-7),
+                                                 (complex(4.0, 0.1), 1.0, 0.3, 0.7, 1e-7)])
+    lam = 6e-7
+    k0 = 2 * np.pi / lam
+    pts = np.array([(0, lam, k0 * 0.3, 0.1 * k0)])
+    pxy = np.array([[(0.0, 1.0), (1.0, 0.0)]], dtype=complex)
+    Rm, Tm, _, _, sm = eng.solve_batch([st], pts, pxy, orders=False, precision=o.RCWA_PREC_MIXED)
+    R6, T6, _, _, s6 = eng.solve_batch([st], pts, pxy, orders=False, precision=o.RCWA_PREC_FP64)
+    assert not np.any(sm) and not np.any(s6)
+    assert np.array_equal(Rm, R6) and np.array_equal(Tm, T6)

@@ -256,3 +256,47 @@ def test_plan_graph_replay_and_rescatter(eng):
     assert not np.any(st) and not np.any(st2)
     assert np.max(np.abs(R - R2)) < 1e-12 and np.max(np.abs(T - T2)) < 1e-12
     plan.close()
+
+
+def test_uneven_batch_sizes_and_materials(eng):
+    # cfg3's instance mix (Lorentz and metal layers, 1-3 layers, nH 3..5)
+    # in one call, every point against the oracle
+    import openrcwa_b200 as o
+    from openrcwa_b200 import workloads
+    stacks, pts, pxy = workloads.uneven_batch(seed=2, n_instances=6, nh_range=(3, 5), max_layers=3)
+    R, T, REF, TRN, st = eng.solve_batch(stacks, pts, pxy)
+    assert np.all(st == 0)
+    for i, s in enumerate(stacks):
+        sol = orc.RCWASolver(s.nHx, s.nHy)
+        for l in range(s.eps.shape[0]):
+            sol.addLayer(orc.OracleLayer(s.cx, s.cy, s.eps[l]))
+        sol.setBlochWavevector(pts[i, 2], pts[i, 3])
+        sol.solve(pts[i, 1], list(range(s.eps.shape[0])), list(s.thickness))
+        k0 = 2 * math.pi / pts[i, 1]
+        for x in range(2):
+            c = sol.generateHorizontalPlaneWave(pxy[i, x, 0], pxy[i, x, 1], 0)
+            ref, trn = sol.scatterPlaneWave(c, 0, s.eps.shape[0] - 1, k0)
+            assert abs(R[i, x] - ref.sum()) < TOL_RT and abs(T[i, x] - trn.sum()) < TOL_RT
+
+
+def test_largest_order_count(eng):
+    # nH = 15 (961 orders, 1922 x 1922 layer matrices), one patterned layer
+    import openrcwa_b200 as o
+    from openrcwa_b200 import workloads
+    st = workloads.rect_stack(15, 15, 4e-7, 4e-7, [(complex(6.0, 0.2), 1.0, 0.4, 0.6, 1.5e-7)])
+    lam = 7e-7
+    k0 = 2 * math.pi / lam
+    pts = np.array([(0, lam, k0 * math.sin(0.3), 0.0)])
+    te, tm = workloads.pol_vectors(math.degrees(0.3), 0.0)
+    pxy = np.array([[te, tm]], dtype=complex)
+    R, T, _, _, status = eng.solve_batch([st], pts, pxy, orders=False)
+    assert not np.any(status)
+    sol = orc.RCWASolver(15, 15)
+    for l in range(st.eps.shape[0]):
+        sol.addLayer(orc.OracleLayer(st.cx, st.cy, st.eps[l]))
+    sol.setBlochWavevector(pts[0, 2], pts[0, 3])
+    sol.solve(lam, list(range(st.eps.shape[0])), list(st.thickness))
+    for x in range(2):
+        c = sol.generateHorizontalPlaneWave(pxy[0, x, 0], pxy[0, x, 1], 0)
+        ref, trn = sol.scatterPlaneWave(c, 0, st.eps.shape[0] - 1, k0)
+        assert abs(R[0, x] - ref.sum()) < TOL_RT and abs(T[0, x] - trn.sum()) < TOL_RT
