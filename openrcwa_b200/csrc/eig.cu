@@ -546,7 +546,7 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
 constexpr int kMsW = 64;           // window order
 constexpr int kMsShifts = 10;      // bulges per sweep
 constexpr int kMsMin = 64;         // smaller active blocks use single-shift sweeps
-constexpr int kMsThreads = 128;    // four warps
+constexpr int kMsThreads = 192;    // six warps
 constexpr int kMsTileElems = 2112 + 66; // 66 rows x 33 (row tasks) or 32 rows x 67 (column tasks)
 constexpr int kMsLog = kMsW + 1;         // rotation log per bulge; slot kMsW holds the identity
 constexpr int kMsMaxSteps = kMsW + 3 * kMsShifts;  // chain steps of one window pass
@@ -569,7 +569,12 @@ struct MsSmem {
   int* aed;      // [4] early-deflation results: converged flag, undeflated count, shift count
 };
 
-constexpr size_t kMsSmemBytes = sizeof(cplx) * kMsW * (kMsW + 1) + sizeof(cplx) * (kMsThreads / 32) * kMsTileElems +
+// the window is only used by the in-window chase and the tiles only by the
+// replay that follows it, so the two share one region
+constexpr size_t kMsRegion = sizeof(cplx) * kMsW * (kMsW + 1) > sizeof(cplx) * (kMsThreads / 32) * kMsTileElems
+                                 ? sizeof(cplx) * kMsW * (kMsW + 1)
+                                 : sizeof(cplx) * (kMsThreads / 32) * kMsTileElems;
+constexpr size_t kMsSmemBytes = kMsRegion +
                                 sizeof(double) * kMsShifts * kMsLog + sizeof(cplx) * kMsShifts * kMsLog +
                                 sizeof(int) * kMsMaxSteps * kMsShifts + sizeof(int) * 3 * kMsShifts +
                                 sizeof(cplx) * kMsShifts + sizeof(int) * 12;
@@ -578,8 +583,8 @@ static_assert(kMsSmemBytes <= 232448, "multishift shared memory exceeds the per-
 __device__ MsSmem carve_ms_smem(unsigned char* base) {
   MsSmem sm;
   sm.Wt = (cplx*)base;
-  sm.tiles = sm.Wt + kMsW * (kMsW + 1);
-  sm.ls = sm.tiles + (kMsThreads / 32) * kMsTileElems;
+  sm.tiles = (cplx*)base;
+  sm.ls = (cplx*)(base + kMsRegion);
   sm.shifts = sm.ls + kMsShifts * kMsLog;
   sm.lc = (double*)(sm.shifts + kMsShifts);
   sm.ix = (int*)(sm.lc + kMsShifts * kMsLog);
