@@ -1,7 +1,7 @@
 // 3xTF32 complex GEMM on tcgen05.
 //
 // One CTA (four warps) computes a 128 x 128 complex output tile.  For each
-// 32-deep K slab the CTA converts its FP64 operand tiles into eight TF32
+// 8-deep K slab the CTA converts its FP64 operand tiles into eight TF32
 // planes in shared memory (A: re hi/lo, im hi/lo; B likewise), laid out as
 // K-major, unswizzled UMMA core matrices (8 rows x 16 bytes; 8-row groups
 // 128 B apart, 16-byte K chunks 2048 B apart).  One thread then issues, per
@@ -9,8 +9,10 @@
 //   Re += Ar*Br (3 terms) - Ai*Bi (3 terms, A negated in the descriptor)
 //   Im += Ar*Bi (3 terms) + Ai*Br (3 terms)
 // into two FP32 accumulators in tensor memory (256 columns), and commits to
-// an mbarrier; the next slab's conversion waits for that commit before it
-// overwrites the planes.  The epilogue reads the accumulators with
+// the stage's mbarrier.  Slabs alternate between two stages of planes, so
+// the conversion of one slab overlaps the MMAs of the previous one; a stage
+// is refilled only after its last commit completed.  The two stages take
+// 64 KB, so two CTAs share an SM (512 tensor-memory columns) and overlap too.  The epilogue reads the accumulators with
 // tcgen05.ld (warp w owns rows 32w..32w+31) and writes alpha*acc + beta*C.
 // Every wait is bounded: a wait that runs out sets the error flag, waits
 // (bounded) for the MMAs in flight, frees the tensor memory and skips the
@@ -21,11 +23,11 @@
 
 namespace {
 
-constexpr int kTcM = 128, kTcN = 128, kTcK = 32;
+constexpr int kTcM = 128, kTcN = 128, kTcK = 8;
 constexpr int kTcThreads = 128;
-constexpr int kPlaneFloats = kTcM * kTcK;                // 4096 floats = 16 KB
+constexpr int kPlaneFloats = kTcM * kTcK;                // 1024 floats = 4 KB
 constexpr int kLbo = 2048, kSbo = 128;                   // bytes
-constexpr size_t kTcSmem = 8 * kPlaneFloats * sizeof(float) + 64;
+constexpr size_t kTcSmem = 2 * 8 * kPlaneFloats * sizeof(float) + 64;  // two stages
 constexpr uint32_t kTmemCols = 256;
 constexpr long kWaitLimit = 1L << 22;
 
@@ -119,19 +121,12 @@ __global__ void tc_scale_kernel(GemmArgs g, int* exps) {
   }
 }
 
-__global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g, const int* exps, int* err) {
+__global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g, const int* exps, int* err) {
   extern __shared__ __align__(1024) unsigned char tsm[];
+  // two stages of eight planes (A: re hi, re lo, im hi, im lo; then B)
   float* planes = reinterpret_cast<float*>(tsm);
-  float* Arh = planes;
-  float* Arl = planes + kPlaneFloats;
-  float* Aih = planes + 2 * kPlaneFloats;
-  float* Ail = planes + 3 * kPlaneFloats;
-  float* Brh = planes + 4 * kPlaneFloats;
-  float* Brl = planes + 5 * kPlaneFloats;
-  float* Bih = planes + 6 * kPlaneFloats;
-  float* Bil = planes + 7 * kPlaneFloats;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 8 * kPlaneFloats * sizeof(float));
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 1);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 2 * 8 * kPlaneFloats * sizeof(float));  // one per stage
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
   int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
 
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -139,7 +134,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
   const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
   const cplx* A = (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
   const cplx* B = (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB;
-  const uint32_t mb = smem_u32(mbar);
+  const uint32_t mb0 = smem_u32(mbar), mb1 = smem_u32(mbar + 1);
   // exact power-of-two operand scales (an all-zero operand keeps scale 1)
   const int eA = max(exps[b], -1000), eB = max(exps[g.batch + b], -1000);
   const double sA = ldexp(1.0, eA > -1000 ? -eA : 0), sB = ldexp(1.0, eB > -1000 ? -eB : 0);
@@ -152,7 +147,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb0) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb1) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     *s_fail = 0;
   }
@@ -162,24 +158,33 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
   const uint32_t tmem = *tmem_slot;
   const uint32_t tRe = tmem, tIm = tmem + kTcN;
 
-  uint32_t phase = 0;
-  int pending = 0;  // a commit not yet waited for (uniform across the CTA)
-  for (int k0 = 0; k0 < g.K; k0 += kTcK) {
-    if (pending) {
-      // the planes are free once the previous slab's MMAs completed
-      if (mbar_wait(mb, phase)) {
-        phase ^= 1u;
-        pending = 0;
+  // slab i goes to stage i % 2; before stage s is refilled, the MMAs of slab
+  // i - 2 (its previous contents) must have completed.  The conversion of
+  // slab i thus overlaps the MMAs of slab i - 1.
+  uint32_t phase[2] = {0u, 0u};
+  int pending[2] = {0, 0};  // uniform across the CTA
+  int slab = 0;
+  for (int k0 = 0; k0 < g.K; k0 += kTcK, ++slab) {
+    const int st = slab & 1;
+    const uint32_t mbs = st ? mb1 : mb0;
+    if (pending[st]) {
+      if (mbar_wait(mbs, phase[st])) {
+        phase[st] ^= 1u;
+        pending[st] = 0;
       } else {
         *s_fail = 1;
       }
     }
     __syncthreads();
     if (*s_fail) break;
+    float* P = planes + st * 8 * kPlaneFloats;
+    float *Arh = P, *Arl = P + kPlaneFloats, *Aih = P + 2 * kPlaneFloats, *Ail = P + 3 * kPlaneFloats;
+    float *Brh = P + 4 * kPlaneFloats, *Brl = P + 5 * kPlaneFloats, *Bih = P + 6 * kPlaneFloats,
+          *Bil = P + 7 * kPlaneFloats;
     // A: row tid, K chunks q (4 consecutive k each)
     {
       const int gm = m0 + tid;
-#pragma unroll 2
+#pragma unroll
       for (int q = 0; q < kTcK / 4; ++q) {
         float rh[4], rl[4], ih[4], il[4];
 #pragma unroll
@@ -200,7 +205,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
     // B: column tid (row of the K-major plane), K chunks q
     {
       const int gn = n0 + tid;
-#pragma unroll 2
+#pragma unroll
       for (int q = 0; q < kTcK / 4; ++q) {
         float rh[4], rl[4], ih[4], il[4];
 #pragma unroll
@@ -244,13 +249,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) zgemm_tf32x3_kernel(GemmArgs g,
         mma_tf32(tIm, aih, brl, kIdesc, 1u);
         mma_tf32(tIm, ail, brh, kIdesc, 1u);
       }
-      mma_commit(mb);
+      mma_commit(mbs);
     }
-    pending = 1;
+    pending[st] = 1;
   }
-  // the last slab's MMAs (after a failure too: nothing may still write the
-  // tensor memory when it is freed)
-  if (pending && !mbar_wait(mb, phase)) *s_fail = 1;
+  // the outstanding slabs' MMAs (after a failure too: nothing may still write
+  // the tensor memory or the planes when they are freed); the commit of the
+  // last slab also covers every earlier MMA
+  for (int s2 = 0; s2 < 2; ++s2)
+    if (pending[s2] && !mbar_wait(s2 ? mb1 : mb0, phase[s2])) *s_fail = 1;
+
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
