@@ -45,8 +45,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=145, help="solve points per step per GPU (145 x 5 layers = 725 "
-                    "eigensolves, about five waves on 148 SMs; the interface and tau factorisations then "
+    ap.add_argument("--batch", type=int, default=148, help="solve points per step per GPU (148 x 5 layers = 740 "
+                    "eigensolves, five full waves on 148 SMs; the interface and tau factorisations then "
                     "fill the GPU too)")
     ap.add_argument("--nh", type=int, default=10, help="harmonics per axis (Nx=Ny)")
     ap.add_argument("--no-cpu-baseline", action="store_true")

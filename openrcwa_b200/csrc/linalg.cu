@@ -199,30 +199,39 @@ __global__ void __launch_bounds__(kTileThreads) zgetrf_kernel(cplx* const* Aarr,
   if (tid == 0) info_all[b] = info;
 }
 
+// Panel width of the multi-launch LU, and the panel kernel's block size: a
+// whole SM per panel keeps enough loads in flight for the rank-1 updates,
+// whose rows come from L2.
+constexpr int kLuPanel = 32;
+constexpr int kLuPanelThreads = 512;
+
 // Panel step of the multi-launch LU: one CTA per matrix factorises columns
 // kb .. kb+jb-1 (the first panel also clears info).
-__global__ void __launch_bounds__(kTileThreads) getrf_panel_kernel(cplx* const* Aarr, int n, int lda, int kb, int jb,
-                                                                  int* ipiv_all, int* info_all) {
-  __shared__ double red_v[kTileThreads / 32];
-  __shared__ int red_i[kTileThreads / 32];
+__global__ void __launch_bounds__(kLuPanelThreads) getrf_panel_kernel(cplx* const* Aarr, int n, int lda, int kb,
+                                                                     int jb, int* ipiv_all, int* info_all) {
+  __shared__ double red_v[kLuPanelThreads / 32];
+  __shared__ int red_i[kLuPanelThreads / 32];
   __shared__ int s_piv;
-  __shared__ cplx prow[32];
+  __shared__ cplx prow[kLuPanel];
   const int b = blockIdx.x;
   int info = kb == 0 ? 0 : info_all[b];
   lu_panel(Aarr[b], n, lda, kb, jb, ipiv_all + (size_t)b * n, info, red_v, red_i, &s_piv, prow);
   if (threadIdx.x == 0) info_all[b] = info;
 }
 
-// U12 of the multi-launch LU: one CTA per (matrix, 64 columns right of the panel).
+// U12 of the multi-launch LU: one CTA per (matrix, 64 columns right of the
+// panel), a thread per column; the unit lower L11 (jb <= kLuPanel) is read
+// through the read-only path (every thread reads the same entry).
 __global__ void __launch_bounds__(64) getrf_trsm_kernel(cplx* const* Aarr, int n, int lda, int kb, int jb) {
-  __shared__ cplx Lsm[32][33];
   cplx* A = Aarr[blockIdx.y];
-  for (int idx = threadIdx.x; idx < jb * jb; idx += 64) {
-    const int r = idx / jb, q = idx % jb;
-    Lsm[r][q] = A[(size_t)(kb + r) * lda + kb + q];
+  const int c = kb + jb + blockIdx.x * 64 + threadIdx.x;
+  if (c >= n) return;
+  for (int r = 1; r < jb; ++r) {
+    cplx x = A[(size_t)(kb + r) * lda + c];
+    const cplx* Lr = A + (size_t)(kb + r) * lda + kb;
+    for (int q = 0; q < r; ++q) x = cfma(cneg(__ldg(&Lr[q])), A[(size_t)(kb + q) * lda + c], x);
+    A[(size_t)(kb + r) * lda + c] = x;
   }
-  __syncthreads();
-  lu_trsm_cols(A, n, lda, kb, jb, kb + jb + blockIdx.x * 64 + threadIdx.x, Lsm);
 }
 
 // Blocked LU solve, left-looking: one CTA per (matrix, 64-column slab of B).
@@ -402,9 +411,9 @@ cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info,
     ++launch_counter();
     return cudaGetLastError();
   }
-  for (int kb = 0; kb < n; kb += 32) {
-    const int jb = min(32, n - kb);
-    getrf_panel_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, kb, jb, ipiv, info);
+  for (int kb = 0; kb < n; kb += kLuPanel) {
+    const int jb = min(kLuPanel, n - kb);
+    getrf_panel_kernel<<<batch, kLuPanelThreads, 0, st>>>(A, n, lda, kb, jb, ipiv, info);
     ++launch_counter();
     const int m2 = n - kb - jb;
     if (m2 <= 0) break;
