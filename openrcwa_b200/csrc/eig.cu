@@ -107,6 +107,15 @@ __device__ void cta_gemm(TileSmem& sm, int M, int N, int K, const cplx* A, int l
     if (K > 0) tile_mma<TA, TB>(sm, acc, A, lda, B, ldb, nullptr, M, N, K, m0, n0);
     tile_store(acc, D, ldd, C, ldc, alpha, beta, mkc(0.0, 0.0), M, N, m0, n0);
   }
+  tile_barrier();
+}
+
+// cta_gemm by the first kTileThreads threads of a larger CTA, then a full
+// barrier (the Hessenberg kernel runs more warps than the tile routines use).
+template <bool TA, bool TB>
+__device__ void cta_gemm_part(TileSmem& sm, int M, int N, int K, const cplx* A, int lda, const cplx* B, int ldb,
+                              cplx* D, int ldd, const cplx* C, int ldc, cplx alpha, cplx beta) {
+  if (threadIdx.x < kTileThreads) cta_gemm<TA, TB>(sm, M, N, K, A, lda, B, ldb, D, ldd, C, ldc, alpha, beta);
   __syncthreads();
 }
 
@@ -258,19 +267,19 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
     const int m2 = n - c0;
     if (m2 > 0) {
       // A(:, c0:) -= Y V(c0:, :)^H
-      cta_gemm<true, false>(tsm, n, m2, jb, Yc, n, s.VH + c0, n, A + c0, lda, A + c0, lda, mkc(-1.0, 0.0),
+      cta_gemm_part<true, false>(tsm, n, m2, jb, Yc, n, s.VH + c0, n, A + c0, lda, A + c0, lda, mkc(-1.0, 0.0),
                             mkc(1.0, 0.0));
       // W = V(k+1:, :)^H A(k+1:, c0:)  (jb x m2), W2 = T^H W, A(k+1:, c0:) -= V(k+1:, :) W2
-      cta_gemm<false, false>(tsm, jb, m2, n - k - 1, s.VH + k + 1, n, A + (size_t)(k + 1) * lda + c0, lda, s.Wb + c0, n,
+      cta_gemm_part<false, false>(tsm, jb, m2, n - k - 1, s.VH + k + 1, n, A + (size_t)(k + 1) * lda + c0, lda, s.Wb + c0, n,
                              nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
       for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
         const int r = idx / nb, c = idx % nb;
         s.Vt[idx] = (r < jb && c < jb) ? cconj(T[c * nb + r]) : mkc(0.0, 0.0);  // T^H in Vt
       }
       __syncthreads();
-      cta_gemm<false, false>(tsm, jb, m2, jb, s.Vt, nb, s.Wb + c0, n, s.Yb + c0, n, nullptr, 0, mkc(1.0, 0.0),
+      cta_gemm_part<false, false>(tsm, jb, m2, jb, s.Vt, nb, s.Wb + c0, n, s.Yb + c0, n, nullptr, 0, mkc(1.0, 0.0),
                              mkc(0.0, 0.0));
-      cta_gemm<true, false>(tsm, n - k - 1, m2, jb, Vc + k + 1, n, s.Yb + c0, n,
+      cta_gemm_part<true, false>(tsm, n - k - 1, m2, jb, Vc + k + 1, n, s.Yb + c0, n,
                             A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
                             mkc(-1.0, 0.0), mkc(1.0, 0.0));
     }
@@ -311,10 +320,10 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
     __syncthreads();
     const int m = n - k - 1;
     cplx* Zs = s.Z + (size_t)(k + 1) * n + (k + 1);
-    cta_gemm<false, false>(tsm, m, jb, m, Zs, n, s.Wb + (size_t)(k + 1) * nb, nb, s.Yb, nb, nullptr, 0,
+    cta_gemm_part<false, false>(tsm, m, jb, m, Zs, n, s.Wb + (size_t)(k + 1) * nb, nb, s.Yb, nb, nullptr, 0,
                            mkc(1.0, 0.0), mkc(0.0, 0.0));
-    cta_gemm<false, false>(tsm, m, jb, jb, s.Yb, nb, s.Vt, nb, s.Vb, nb, nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
-    cta_gemm<false, false>(tsm, m, m, jb, s.Vb, nb, s.VH + k + 1, n, Zs, n, Zs, n, mkc(-1.0, 0.0), mkc(1.0, 0.0));
+    cta_gemm_part<false, false>(tsm, m, jb, jb, s.Yb, nb, s.Vt, nb, s.Vb, nb, nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
+    cta_gemm_part<false, false>(tsm, m, m, jb, s.Vb, nb, s.VH + k + 1, n, Zs, n, Zs, n, mkc(-1.0, 0.0), mkc(1.0, 0.0));
   }
   for (size_t idx = tid; idx < (size_t)n * n; idx += blockDim.x) {
     const int i = (int)(idx / n), j = (int)(idx % n);
@@ -1364,8 +1373,13 @@ __device__ void trevc_blocked(const cplx* T, int ldt, cplx* X, int n, TileSmem& 
   }
 }
 
-__global__ void __launch_bounds__(kEigThreads) hessenberg_kernel(cplx* const* Aarr, int n, int lda, void* work) {
-  __shared__ double red[kEigThreads / 32];
+// The Hessenberg reduction runs 512 threads: its per-column sweeps and
+// matrix-vector products stream from L2/DRAM and need the loads in flight;
+// the first 256 threads also run the tile products.
+constexpr int kHessThreads = 512;
+
+__global__ void __launch_bounds__(kHessThreads) hessenberg_kernel(cplx* const* Aarr, int n, int lda, void* work) {
+  __shared__ double red[kHessThreads / 32];
   __shared__ TileSmem tsm;
   const Scratch s = scratch_for(work, n, blockIdx.x);
   hessenberg_blocked(Aarr[blockIdx.x], n, lda, s, red, tsm);
@@ -1414,7 +1428,7 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   if (batch <= 0 || n <= 0) return cudaSuccess;
   StageProf none;
   StageProf& P = prof ? *prof : none;
-  hessenberg_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, work);
+  hessenberg_kernel<<<batch, kHessThreads, 0, st>>>(A, n, lda, work);
   ++launch_counter();
   P.mark(st, kStHessenberg);
   if (n < kMsMin) {

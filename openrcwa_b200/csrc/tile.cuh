@@ -30,6 +30,11 @@ __device__ __forceinline__ void tile_zero(cplx acc[4][4]) {
     for (int j = 0; j < 4; ++j) acc[i][j] = mkc(0.0, 0.0);
 }
 
+// Barrier over the kTileThreads threads that run the tile routines (named
+// barrier 1), so that a larger CTA can leave its other warps out of a tile
+// product; with a CTA of exactly kTileThreads it is a full barrier.
+__device__ __forceinline__ void tile_barrier() { asm volatile("bar.sync 1, %0;" ::"n"(kTileThreads) : "memory"); }
+
 // d(8x8 fragment, two doubles per lane) += a(8x4) * b(4x8)
 __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
   asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -94,8 +99,9 @@ __device__ __forceinline__ void tile_stage(TileSmem& sm, const cplx pa[4], const
 
 // acc += op(A)[m0:m0+64, :K] * diag(s) * op(B)[:K, n0:n0+64], where op(A) is
 // M x K and op(B) is K x N; TA/TB select the transposed reading of a
-// row-major operand.  Out-of-range elements read as zero.  Every thread of
-// the CTA must call this (it contains __syncthreads).
+// row-major operand.  Out-of-range elements read as zero.  The first
+// kTileThreads threads of the CTA must all call this (it contains
+// tile_barrier).
 template <bool TA, bool TB>
 __device__ __forceinline__ void tile_mma(TileSmem& sm, cplx acc[4][4], const cplx* __restrict__ A, int lda,
                                          const cplx* __restrict__ B, int ldb, const cplx* __restrict__ s,
@@ -107,7 +113,7 @@ __device__ __forceinline__ void tile_mma(TileSmem& sm, cplx acc[4][4], const cpl
   cplx pa[4], pb[4];
   tile_fetch<TA, TB>(A, lda, B, ldb, s, M, N, K, m0, n0, 0, pa, pb);
   tile_stage<TA, TB>(sm, pa, pb);
-  __syncthreads();
+  tile_barrier();
   for (int k0 = 0; k0 < K; k0 += kTBK) {
     const bool more = k0 + kTBK < K;
     if (more) tile_fetch<TA, TB>(A, lda, B, ldb, s, M, N, K, m0, n0, k0 + kTBK, pa, pb);
@@ -137,10 +143,10 @@ __device__ __forceinline__ void tile_mma(TileSmem& sm, cplx acc[4][4], const cpl
           dmma_8x8x4(c0.y, c1.y, ai[rt], br[ct]);
         }
     }
-    __syncthreads();
+    tile_barrier();
     if (more) {
       tile_stage<TA, TB>(sm, pa, pb);
-      __syncthreads();
+      tile_barrier();
     }
   }
 }
