@@ -1463,6 +1463,7 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   g.M = n; g.N = n; g.K = n;
   g.lda = n; g.ldb = n; g.ldd = ldv; g.ldc = ldv;
   g.transA = 1; g.transB = 0;
+  g.triB = 1;  // X is upper triangular
   g.alpha = mkc(1.0, 0.0); g.beta = mkc(0.0, 0.0); g.gammaI = mkc(0.0, 0.0);
   g.batch = batch;
   cudaError_t err = zgemm_batched(g, st);

@@ -17,14 +17,15 @@ __global__ void __launch_bounds__(kTileThreads) zgemm_kernel(GemmArgs g) {
   const cplx* B = (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB;
   const cplx* s = g.s ? g.s[b] : nullptr;
   const int m0 = blockIdx.y * kTBM, n0 = blockIdx.x * kTBN;
+  const int K = g.triB ? min(g.K, n0 + kTBN) : g.K;
   cplx acc[4][4];
   tile_zero(acc);
   if (g.transA) {
-    if (g.transB) tile_mma<true, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
-    else tile_mma<true, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
+    if (g.transB) tile_mma<true, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, K, m0, n0);
+    else tile_mma<true, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, K, m0, n0);
   } else {
-    if (g.transB) tile_mma<false, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
-    else tile_mma<false, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, g.K, m0, n0);
+    if (g.transB) tile_mma<false, true>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, K, m0, n0);
+    else tile_mma<false, false>(sm, acc, A, g.lda, B, g.ldb, s, g.M, g.N, K, m0, n0);
   }
   const cplx* C = (g.beta.x != 0.0 || g.beta.y != 0.0) ? g.C[b] + g.offC : nullptr;
   tile_store(acc, (g.D ? g.D[b] : g.D0 + b * g.sD) + g.offD, g.ldd, C, g.ldc, g.alpha, g.beta, g.gammaI, g.M, g.N,

@@ -22,6 +22,9 @@ struct GemmArgs {
   size_t sA = 0, sB = 0, sD = 0;
   // element offsets added to every item's A, B, C and D (sub-blocks)
   size_t offA = 0, offB = 0, offC = 0, offD = 0;
+  // op(B) is upper triangular: output column tile [n0, n0+64) only needs
+  // k < n0 + 64
+  int triB = 0;
 };
 
 // D = alpha*op(A)*diag(s)*op(B) + beta*C + gammaI*I for every batch item.
