@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--gemm-only", default=None, metavar="N,BATCH",
                     help="one batched n x n x n complex GEMM in 3xTF32 on tcgen05 and one on the FP64 path "
                          "(profiling aid)")
+    ap.add_argument("--tuning", default="auto", choices=["auto", "off"],
+                    help="auto: the engine's autotuner times the candidate schedules of each new (decision, "
+                         "matrix order, batch class) while a plan is created, before warm-up; off: built-in rules")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
                     help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
@@ -76,8 +79,16 @@ def run_uneven(args):
     eng = o.Engine(0)
     stream = torch.cuda.Stream()
     res = {}
-    for name, prec in (("mixed", o.RCWA_PREC_MIXED), ("fp64", o.RCWA_PREC_FP64)):
+    tuner = o.Tuner() if args.tuning == "auto" else None
+    runs = [("mixed", o.RCWA_PREC_MIXED, tuner), ("fp64", o.RCWA_PREC_FP64, tuner)]
+    if tuner is not None:
+        runs.append(("mixed_untuned", o.RCWA_PREC_MIXED, None))
+    tune_s = 0.0
+    for name, prec, tn in runs:
+        eng.set_tuner(tn, o.RCWA_TUNING_AUTO if tn is not None else o.RCWA_TUNING_OFF)
+        t0 = time.perf_counter()
         plan = eng.plan(stacks, pts, pxy, precision=prec)
+        tune_s += time.perf_counter() - t0 if tn is not None else 0.0
         plan.execute(stream.cuda_stream)
         stream.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
@@ -110,6 +121,12 @@ def run_uneven(args):
                            np.max(np.abs(res["mixed"][2] - T64)[valid]))) if np.any(valid) else None,
                        "failed_points": {k: int(np.sum(v[4] != 0)) for k, v in res.items()},
                        "gpu_launches": res["mixed"][3]}}
+    if tuner is not None:
+        line["uneven"]["tuning"] = {
+            "mode": "auto", "plan_create_s": tune_s, "entries": len(tuner.entries()),
+            "mixed_untuned_solves_per_s": len(stacks) / (res["mixed_untuned"][0] * 1e-3),
+            "changed_from_builtin": [e for e in tuner.entries()
+                                     if e["choice"] != tuner.default(e["op"], e["n"], 148 * e["batch_class"])]}
     print(json.dumps(line), flush=True)
     eng.close()
     return 0
@@ -377,6 +394,11 @@ def main():
     n = 2 * N
     B = args.batch
     eng = o.Engine(local)
+    tuner = None
+    if args.tuning == "auto":
+        tuner = o.Tuner()
+        eng.set_tuner(tuner, o.RCWA_TUNING_AUTO)
+    plan_info = {}
     bpts, bpxy = workloads.batch_slice(pts, pxy, workloads.shard_start(rank, world, B, 0), B)
     stream = torch.cuda.Stream()
     fp64_peak = fp64_gemm_peak_tflops(torch)
@@ -389,7 +411,9 @@ def main():
         are on from the start: the second execution captures the launch
         sequence (with its event records) into the CUDA graph that every later
         execution launches."""
+        tc0 = time.perf_counter()
         plan = eng.plan(stacks, bpts, bpxy, precision=precision)
+        plan_info[precision] = {"plan_create_s": time.perf_counter() - tc0, "schedule": plan.schedule()}
         plan.set_profiling(True)
         for _ in range(warmup):
             plan.execute(stream.cuda_stream)
@@ -457,6 +481,8 @@ def main():
     g_ms = allmax(e0.elapsed_time(e1))
     g_launch = gplan.launch_count()
     gplan.close()
+    for _ in range(10):   # untimed warm-up calls of the end-to-end path
+        eng.solve_batch(g_st, g_pts, g_pxy, orders=True)
     barrier()
     t0 = time.perf_counter()
     for _ in range(reps):
@@ -515,6 +541,10 @@ def main():
             "mixed_error": {"max_abs_dRT_vs_fp64": dRT, "max_abs_dorder_vs_fp64": dorders, "bound": 1e-4,
                             "reference": "the FP64 engine on the same batch (1e-9 of the oracle in the tests)"},
             "grating_1d": grating,
+            "schedule": plan_info[o.RCWA_PREC_MIXED]["schedule"],
+            "tuning": {"mode": args.tuning,
+                       "plan_create_s": plan_info[o.RCWA_PREC_MIXED]["plan_create_s"],
+                       "entries": tuner.entries() if tuner is not None else []},
             "stage_ms_per_step": per_launch, "peaks": {"fp64_dgemm_tflops": fp64_peak,
                                                        "hbm_gbs": peaks.get("hbm_gbs"), "source": peak_kind}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

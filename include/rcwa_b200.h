@@ -133,6 +133,12 @@ int rcwa_plan_rescatter(rcwa_plan* p, const rcwa_cplx* pxy);
 
 /* Number of engine kernel launches the last plan_execute enqueued. */
 long long rcwa_plan_launch_count(const rcwa_plan* p);
+/* Schedules the plan uses, per chunk: sched[6] = {matrix order n, points,
+ * interface LU schedule, tau LU schedule, Schur crossover, product path}
+ * (values as in rcwa_tuner_*; product path 1 for FP64 plans and for chunks
+ * whose points all keep FP64 products).  Returns the number of chunks (chunk < 0 or
+ * sched NULL: only the count), -1 for a bad plan or chunk. */
+int rcwa_plan_schedule(const rcwa_plan* p, int chunk, int* sched);
 /* Per-stage device time: with profiling on, plan_execute records CUDA events
  * between the stages on its stream; plan_stage_times waits and writes the
  * milliseconds of every stage of the last execution into ms[max_stages] and
@@ -182,6 +188,53 @@ int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
  * counterpart in the reference (its Eigen products). */
 int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch, const rcwa_cplx* A, const rcwa_cplx* B,
                        const rcwa_cplx* C, rcwa_cplx alpha, rcwa_cplx beta, int precision, rcwa_cplx* D);
+
+/* ---- Schedule autotuner ----------------------------------------------
+ * No counterpart in the reference (its CPU path calls LAPACK with fixed
+ * blocking).  A tuner is a table of schedule choices keyed by decision, matrix
+ * order n and batch class (waves of one-CTA-per-matrix work: 1, 2, 3, 4 for
+ * 4-7, 8 for 8 and more).  Decisions and their choices:
+ *   RCWA_TUNE_LU       0: one CTA factors each matrix, 1: panel by panel
+ *   RCWA_TUNE_SCHUR    active-block size below which the Schur iteration uses
+ *                      single-shift sweeps (64, 96, 128, 192; only 64 for
+ *                      n < 64 and n >= 512; default 128 for 64 <= n < 128,
+ *                      else 64)
+ *   RCWA_TUNE_PRODUCT  mixed plans' cascade products, 0: 3xTF32 on tcgen05,
+ *                      1: FP64 tensor path
+ * Every choice computes the same quantities (LU: same pivoting rule; Schur:
+ * same convergence tests; products: within the mixed tolerance), so a tuner
+ * changes speed, not results beyond rounding.
+ * rcwa_engine_set_tuner: mode RCWA_TUNING_OFF (built-in rules),
+ * RCWA_TUNING_TABLE (the table, else the rules) or RCWA_TUNING_AUTO (the
+ * table, else time every candidate on the device while the plan is created,
+ * on seeded random matrices, and record the fastest).  The engine does not
+ * own the tuner; keep it alive while the engine uses it.  The table calls are
+ * host-only and thread-safe.  rcwa_tuner_get writes -1 for a missing entry;
+ * rcwa_tuner_entry lists entries (cand/ms: 4 slots, unused -1 / 0); the file
+ * format is text, one entry per line. */
+#define RCWA_TUNE_LU      0
+#define RCWA_TUNE_SCHUR   1
+#define RCWA_TUNE_PRODUCT 2
+#define RCWA_TUNING_OFF   0
+#define RCWA_TUNING_TABLE 1
+#define RCWA_TUNING_AUTO  2
+typedef struct rcwa_tuner rcwa_tuner;
+int rcwa_tuner_create(rcwa_tuner** out);
+void rcwa_tuner_destroy(rcwa_tuner* t);
+int rcwa_tuner_set_sms(rcwa_tuner* t, int sms);
+int rcwa_tuner_candidates(int op, int n, int* choices);
+int rcwa_tuner_default(const rcwa_tuner* t, int op, int n, int batch);
+int rcwa_tuner_set(rcwa_tuner* t, int op, int n, int batch, int choice);
+int rcwa_tuner_get(const rcwa_tuner* t, int op, int n, int batch, int* choice);
+int rcwa_tuner_count(const rcwa_tuner* t);
+int rcwa_tuner_entry(const rcwa_tuner* t, int index, int* op, int* n, int* batch_class, int* choice,
+                     int* ncand, int* cand, double* ms);
+int rcwa_tuner_save(const rcwa_tuner* t, const char* path);
+int rcwa_tuner_load(rcwa_tuner* t, const char* path);
+int rcwa_engine_set_tuner(rcwa_engine* e, rcwa_tuner* t, int mode);
+/* Time every candidate of (op, n, batch) now, record the entry, and return
+ * the fastest choice and the candidates' milliseconds (ms[4]). */
+int rcwa_tuner_measure(rcwa_engine* e, rcwa_tuner* t, int op, int n, int batch, int* choice, double* ms);
 
 /* ---- learned surrogate ------------------------------------------------------
  * No counterpart in the reference.  A fully connected network with n_layers

@@ -28,6 +28,9 @@ RCWA_ERR_UNSUPPORTED = 9
 RCWA_CONTINUOUS_XY, RCWA_DISCONTINUOUS_X, RCWA_DISCONTINUOUS_Y = 0, 1, 2
 RCWA_PREC_FP64 = 0
 RCWA_PREC_MIXED = 1
+RCWA_TUNE_LU, RCWA_TUNE_SCHUR, RCWA_TUNE_PRODUCT = 0, 1, 2
+RCWA_TUNING_OFF, RCWA_TUNING_TABLE, RCWA_TUNING_AUTO = 0, 1, 2
+TUNE_OPS = {"lu": RCWA_TUNE_LU, "schur": RCWA_TUNE_SCHUR, "product": RCWA_TUNE_PRODUCT}
 
 # every symbol declared in include/rcwa_b200.h
 EXPORTS = [
@@ -39,6 +42,9 @@ EXPORTS = [
     "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_zgemm_batched",
     "rcwa_mlp_create", "rcwa_mlp_destroy", "rcwa_mlp_param_count", "rcwa_mlp_get_params", "rcwa_mlp_set_params",
     "rcwa_mlp_set_data", "rcwa_mlp_train", "rcwa_mlp_loss_grad", "rcwa_mlp_predict_fp32", "rcwa_mlp_predict",
+    "rcwa_plan_schedule", "rcwa_tuner_create", "rcwa_tuner_destroy", "rcwa_tuner_set_sms", "rcwa_tuner_candidates",
+    "rcwa_tuner_default", "rcwa_tuner_set", "rcwa_tuner_get", "rcwa_tuner_count", "rcwa_tuner_entry",
+    "rcwa_tuner_save", "rcwa_tuner_load", "rcwa_engine_set_tuner", "rcwa_tuner_measure",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -136,6 +142,21 @@ def load() -> C.CDLL:
     lib.rcwa_mlp_loss_grad.argtypes = [C.c_void_p, _FP, _FP, C.c_int, _DP, _FP]
     lib.rcwa_mlp_predict_fp32.argtypes = [C.c_void_p, _FP, C.c_int, _FP]
     lib.rcwa_mlp_predict.argtypes = [C.c_void_p, _FP, C.c_int, _FP]
+    lib.rcwa_plan_schedule.argtypes = [C.c_void_p, C.c_int, _IP]
+    lib.rcwa_tuner_create.argtypes = [C.POINTER(C.c_void_p)]
+    lib.rcwa_tuner_destroy.argtypes = [C.c_void_p]
+    lib.rcwa_tuner_destroy.restype = None
+    lib.rcwa_tuner_set_sms.argtypes = [C.c_void_p, C.c_int]
+    lib.rcwa_tuner_candidates.argtypes = [C.c_int, C.c_int, _IP]
+    lib.rcwa_tuner_default.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int]
+    lib.rcwa_tuner_set.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.rcwa_tuner_get.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _IP]
+    lib.rcwa_tuner_count.argtypes = [C.c_void_p]
+    lib.rcwa_tuner_entry.argtypes = [C.c_void_p, C.c_int, _IP, _IP, _IP, _IP, _IP, _IP, _DP]
+    lib.rcwa_tuner_save.argtypes = [C.c_void_p, C.c_char_p]
+    lib.rcwa_tuner_load.argtypes = [C.c_void_p, C.c_char_p]
+    lib.rcwa_engine_set_tuner.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    lib.rcwa_tuner_measure.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, _IP, _DP]
     _lib = lib
     return lib
 
@@ -205,6 +226,13 @@ class Engine:
     def _check(self, rc, what):
         if rc:
             raise RcwaError(rc, f"{what}: {self.last_error()}")
+
+    def set_tuner(self, tuner, mode=RCWA_TUNING_AUTO):
+        """Consult `tuner` (a Tuner) when plans are built; mode RCWA_TUNING_OFF,
+        _TABLE or _AUTO (measure on a miss).  The engine keeps a reference."""
+        self._tuner = tuner
+        self._check(self.lib.rcwa_engine_set_tuner(self.h, tuner.h if tuner is not None else None, mode),
+                    "engine_set_tuner")
 
     # -- batched solve ------------------------------------------------------
     @staticmethod
@@ -390,6 +418,17 @@ class Plan:
     def launch_count(self):
         return int(self.eng.lib.rcwa_plan_launch_count(self.h))
 
+    def schedule(self):
+        """Per chunk: dict of n, points, lu_interface, lu_tau, schur_crossover,
+        product (0: 3xTF32 tensor cores, 1: FP64 tensor path)."""
+        count = self.eng.lib.rcwa_plan_schedule(self.h, -1, None)
+        out, v = [], (C.c_int * 6)()
+        keys = ("n", "points", "lu_interface", "lu_tau", "schur_crossover", "product")
+        for c in range(max(count, 0)):
+            self.eng.lib.rcwa_plan_schedule(self.h, c, C.cast(v, _IP))
+            out.append(dict(zip(keys, list(v))))
+        return out
+
     def rescatter(self, pxy):
         """New incident polarisations (n_pts, n_exc, 2) on the kept S-matrices."""
         pxy = np.ascontiguousarray(pxy, dtype=np.complex128).reshape(self.n_pts, self.n_exc, 2)
@@ -485,6 +524,93 @@ class Mlp:
     def close(self):
         if self.h:
             self.eng.lib.rcwa_mlp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Tuner:
+    """Schedule table of the engine's autotuner (host data; see rcwa_tuner_*).
+    Decisions are named "lu", "schur" and "product"."""
+
+    def __init__(self, lib=None):
+        self.lib = lib or load()
+        h = C.c_void_p()
+        rc = self.lib.rcwa_tuner_create(C.byref(h))
+        if rc:
+            raise RcwaError(rc, "tuner_create")
+        self.h = h
+
+    @staticmethod
+    def _op(op):
+        return TUNE_OPS[op] if isinstance(op, str) else int(op)
+
+    def set_sms(self, sms):
+        if self.lib.rcwa_tuner_set_sms(self.h, sms):
+            raise RcwaError(RCWA_ERR_INVALID, "tuner_set_sms")
+
+    def candidates(self, op, n):
+        c = (C.c_int * 4)()
+        k = self.lib.rcwa_tuner_candidates(self._op(op), n, C.cast(c, _IP))
+        if k < 0:
+            raise RcwaError(RCWA_ERR_INVALID, "tuner_candidates")
+        return list(c)[:k]
+
+    def default(self, op, n, batch):
+        return int(self.lib.rcwa_tuner_default(self.h, self._op(op), n, batch))
+
+    def set(self, op, n, batch, choice):
+        rc = self.lib.rcwa_tuner_set(self.h, self._op(op), n, batch, choice)
+        if rc:
+            raise RcwaError(rc, "tuner_set")
+
+    def get(self, op, n, batch):
+        """The recorded choice, or None."""
+        c = C.c_int(-1)
+        rc = self.lib.rcwa_tuner_get(self.h, self._op(op), n, batch, C.byref(c))
+        if rc:
+            raise RcwaError(rc, "tuner_get")
+        return None if c.value < 0 else c.value
+
+    def entries(self):
+        names = {v: k for k, v in TUNE_OPS.items()}
+        out = []
+        for i in range(self.lib.rcwa_tuner_count(self.h)):
+            op, n, cls, ch, nc = (C.c_int() for _ in range(5))
+            cand = (C.c_int * 4)()
+            ms = (C.c_double * 4)()
+            self.lib.rcwa_tuner_entry(self.h, i, C.byref(op), C.byref(n), C.byref(cls), C.byref(ch), C.byref(nc),
+                                      C.cast(cand, _IP), C.cast(ms, _DP))
+            out.append({"op": names[op.value], "n": n.value, "batch_class": cls.value, "choice": ch.value,
+                        "ms": {int(cand[k]): float(ms[k]) for k in range(nc.value)}})
+        return out
+
+    def save(self, path):
+        rc = self.lib.rcwa_tuner_save(self.h, os.fsencode(path))
+        if rc:
+            raise RcwaError(rc, "tuner_save")
+
+    def load(self, path):
+        rc = self.lib.rcwa_tuner_load(self.h, os.fsencode(path))
+        if rc:
+            raise RcwaError(rc, "tuner_load")
+
+    def measure(self, eng: Engine, op, n, batch):
+        """Time every candidate now; returns (choice, {candidate: ms})."""
+        ch = C.c_int(-1)
+        ms = (C.c_double * 4)()
+        eng._check(self.lib.rcwa_tuner_measure(eng.h, self.h, self._op(op), n, batch, C.byref(ch), C.cast(ms, _DP)),
+                   "tuner_measure")
+        cand = self.candidates(op, n)
+        return ch.value, {c: float(ms[k]) for k, c in enumerate(cand)}
+
+    def close(self):
+        if self.h:
+            self.lib.rcwa_tuner_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -554,7 +554,7 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
 // element of T or Z crosses DRAM once per pass instead of once per rotation.
 constexpr int kMsW = 64;           // window order
 constexpr int kMsShifts = 10;      // bulges per sweep
-constexpr int kMsMin = 64;         // smaller active blocks use single-shift sweeps
+constexpr int kMsMin = kSchurCrossover;  // smallest crossover: the chase window needs 64 rows
 constexpr int kMsThreads = 192;    // six warps
 constexpr int kMsTileElems = 2112 + 66; // 66 rows x 33 (row tasks) or 32 rows x 67 (column tasks)
 constexpr int kMsLog = kMsW + 1;         // rotation log per bulge; slot kMsW holds the identity
@@ -1169,9 +1169,10 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
   }
 }
 
-// Schur form by multishift sweeps on large active blocks and single-shift
-// sweeps on small ones.  Returns 0 or RCWA_ERR_NOCONV.
-__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
+// Schur form by multishift sweeps on active blocks of at least ms_min rows
+// (ms_min >= kMsMin) and single-shift sweeps on smaller ones.  Returns 0 or
+// RCWA_ERR_NOCONV.
+__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSmem& sm) {
   const double ulp = 2.0 * RCWA_DBL_EPS;
   const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
   const int tid = threadIdx.x;
@@ -1195,7 +1196,7 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
     last_i = i;
     last_l = l;
     const int m = i - l + 1;
-    if (m < kMsMin) {
+    if (m < ms_min) {
       // small blocks: single-shift sweeps whose off-window updates stream
       // only the rotated pairs (cheaper than full tiles for few rotations)
       cplx shift;
@@ -1234,7 +1235,7 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
 #endif
       if (nd > 0) {
         stall = 0;
-        if (100 * nd > kAedNibble * kAedW || i - nd - l + 1 < kMsMin) {
+        if (100 * nd > kAedNibble * kAedW || i - nd - l + 1 < ms_min) {
           if (++sweeps > budget) return RCWA_ERR_NOCONV;
           continue;
         }
@@ -1271,7 +1272,7 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, const MsSmem& sm) {
 }
 
 __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr, int n, int lda, cplx* w_all,
-                                                             void* work, int* info_all) {
+                                                             void* work, int* info_all, int ms_min) {
   extern __shared__ __align__(16) unsigned char dsm[];
   const MsSmem sm = carve_ms_smem(dsm);
   // identity slot of every bulge's rotation log (inactive chain steps)
@@ -1285,7 +1286,7 @@ __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr,
 #ifdef RCWA_EIG_STATS
   const long long c_schur = clock64();
 #endif
-  const int status = schur_ms(A, lda, s.Z, n, sm);
+  const int status = schur_ms(A, lda, s.Z, n, ms_min, sm);
 #ifdef RCWA_EIG_STATS
   STAT_ADD(10, clock64() - c_schur);
 #endif
@@ -1424,14 +1425,15 @@ __global__ void normalize_kernel(cplx* const* VRarr, int n, int ldv, const cplx*
 
 
 cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* VR, int ldv, void* work,
-                          int* info, int batch, cudaStream_t st, StageProf* prof) {
+                          int* info, int batch, cudaStream_t st, StageProf* prof, int ms_min) {
   if (batch <= 0 || n <= 0) return cudaSuccess;
+  ms_min = max(ms_min, kMsMin);
   StageProf none;
   StageProf& P = prof ? *prof : none;
   hessenberg_kernel<<<batch, kHessThreads, 0, st>>>(A, n, lda, work);
   ++launch_counter();
   P.mark(st, kStHessenberg);
-  if (n < kMsMin) {
+  if (n < ms_min) {
     schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info);
     ++launch_counter();
   } else {
@@ -1444,7 +1446,7 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
       if (e != cudaSuccess) return e;
       if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
-    schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info);
+    schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info, ms_min);
     ++launch_counter();
   }
   P.mark(st, kStSchur);

@@ -14,6 +14,7 @@
 // Every batched call receives device pointer arrays that the plan built once,
 // so executing a plan is a fixed sequence of kernel launches on one stream.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <functional>
@@ -30,6 +31,7 @@
 #include "linalg.cuh"
 #include "gemm_tc.cuh"
 #include "rcwa_kernels.cuh"
+#include "tuner.cuh"
 
 
 namespace {
@@ -39,9 +41,26 @@ constexpr double kPi = 3.1415926535897932;
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
-  bool borrowed = false;  // the engine's cached workspace, not freed here
-  ~DevBuf() { if (p && !borrowed) cudaFree(p); }
+  bool borrowed = false;          // the engine's cached workspace, not freed here
+  rcwa_engine* pool = nullptr;    // block from the engine's pool: returned there
+  size_t cap = 0;                 // pooled block size
+  bool take(rcwa_engine* e, size_t n) {
+    p = engine_take_block(e, n, &cap);
+    if (!p) return false;
+    pool = e;
+    bytes = n;
+    return true;
+  }
+  ~DevBuf() {
+    if (!p || borrowed) return;
+    if (pool) engine_release_block(pool, p, cap);
+    else cudaFree(p);
+  }
 };
+
+// pooled blocks: up to 64 MB each, 512 MB in total per engine
+constexpr size_t kPoolBlockMax = (size_t)64 << 20;
+constexpr size_t kPoolTotalMax = (size_t)512 << 20;
 
 // Bump allocator over byte offsets; turned into addresses once the base exists.
 struct Layout {
@@ -92,6 +111,9 @@ struct rcwa_plan {
   int* dStatus = nullptr;
   int* dTcErr = nullptr;   // set when a tensor-core completion wait ran out
   int* dTcScale = nullptr; // operand scale exponents of the tensor-core products (2 x 1024)
+  // per chunk: n, points, interface LU schedule, tau LU schedule, Schur
+  // crossover, product path (0: 3xTF32, 1: FP64 tensor path)
+  std::vector<std::array<int, 6>> sched;
   int precision = RCWA_PREC_FP64;
   std::vector<std::function<cudaError_t(cudaStream_t, long long&, StageProf&)>> steps;
   long long launches = 0;
@@ -107,8 +129,9 @@ struct rcwa_plan {
   long long graph_launches = 0;
   long long executions = 0;
   ~rcwa_plan() {
-    // kernels of this plan may still run on a caller's stream
-    if (graph_exec || work.borrowed) cudaDeviceSynchronize();
+    // kernels of this plan may still run on a caller's stream; its pooled
+    // blocks and the borrowed workspace go back to the engine only after them
+    cudaDeviceSynchronize();
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (work.borrowed && e) e->work_cache_busy = false;
   }
@@ -188,6 +211,45 @@ void alpha_beta(const StackInfo& si, double kx0, double ky0, cplx* ab) {
 
 }  // namespace
 
+void* engine_take_block(rcwa_engine* e, size_t bytes, size_t* got) {
+  bytes = (bytes + 4095) & ~(size_t)4095;
+  {
+    std::lock_guard<std::mutex> lk(e->pool_mu);
+    int best = -1;
+    for (int i = 0; i < (int)e->block_pool.size(); ++i) {
+      const size_t sz = e->block_pool[i].second;
+      if (sz >= bytes && sz <= 4 * bytes + ((size_t)1 << 20) && (best < 0 || sz < e->block_pool[best].second))
+        best = i;
+    }
+    if (best >= 0) {
+      void* p = e->block_pool[best].first;
+      *got = e->block_pool[best].second;
+      e->block_pool_bytes -= *got;
+      e->block_pool.erase(e->block_pool.begin() + best);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMalloc(&p, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  *got = bytes;
+  return p;
+}
+
+void engine_release_block(rcwa_engine* e, void* p, size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(e->pool_mu);
+    if (bytes <= kPoolBlockMax && e->block_pool_bytes + bytes <= kPoolTotalMax) {
+      e->block_pool.push_back({p, bytes});
+      e->block_pool_bytes += bytes;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+
 // ------------------------------------------------------------------ C ABI
 extern "C" {
 
@@ -226,6 +288,9 @@ int rcwa_engine_create(int device, rcwa_engine** out) {
 void rcwa_engine_destroy(rcwa_engine* e) {
   if (!e) return;
   cudaSetDevice(e->device);
+  cudaDeviceSynchronize();
+  for (auto& b : e->block_pool) cudaFree(b.first);
+  e->block_pool.clear();
   if (e->work_cache) cudaFree(e->work_cache);
   if (e->stream) cudaStreamDestroy(e->stream);
   delete e;
@@ -253,9 +318,13 @@ struct ChunkWork {
   size_t hW0 = 0, hV0 = 0, hWL = 0, hVL = 0, hg0 = 0, hgL = 0;
   size_t Rud = 0, Tdd = 0, F = 0, G = 0, tau = 0, IE = 0, IH = 0, WLU = 0, VLU = 0, pipiv = 0, pinfo = 0;
   size_t total = 0;
-  // mixed plans: this chunk's products stay FP64 (its stacks have a layer
-  // with Re(eps) < 0, whose cascade the 3xTF32 products cannot resolve)
-  bool fp64 = false;
+  // mixed plans: per chunk point, whether its products stay FP64 (its stack
+  // has a layer with Re(eps) < 0, whose cascade the 3xTF32 products cannot
+  // resolve)
+  std::vector<char> fp64_pt;
+  // schedules (tuner or built-in rules): LU of the interface and tau
+  // factorisations, Schur crossover, product path of mixed plans
+  int lu_if = -1, lu_tau = -1, ms_min = kSchurCrossover, prod = 0;
 };
 
 }  // namespace
@@ -367,8 +436,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   }
   std::vector<size_t> ab_off(n_pts);
   for (int p = 0; p < n_pts; ++p) ab_off[p] = il.take(sizeof(cplx) * 2 * P->point_N[p]);
-  if (cudaMalloc(&P->inputs.p, il.off) != cudaSuccess) return fail(e, RCWA_ERR_NOMEM, "input allocation failed");
-  P->inputs.bytes = il.off;
+  if (!P->inputs.take(e, il.off)) return fail(e, RCWA_ERR_NOMEM, "input allocation failed");
   {
     std::vector<unsigned char> h(il.off);
     for (int s = 0; s < n_stacks; ++s) {
@@ -390,8 +458,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     size_t oS = ol.take(sizeof(int) * n_pts);
     size_t oE = ol.take(sizeof(int));
     size_t oSc = ol.take(sizeof(int) * 2 * 1024);
-    if (cudaMalloc(&P->outputs.p, ol.off) != cudaSuccess) return fail(e, RCWA_ERR_NOMEM, "output allocation failed");
-    P->outputs.bytes = ol.off;
+    if (!P->outputs.take(e, ol.off)) return fail(e, RCWA_ERR_NOMEM, "output allocation failed");
     char* b = (char*)P->outputs.p;
     P->dR = (double*)(b + oR);
     P->dT = (double*)(b + oT);
@@ -409,7 +476,9 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   const size_t budget = std::min<size_t>((size_t)(0.6 * free_b), (size_t)96 << 30);
   // In mixed plans, stacks with a metallic layer (Re(eps) < 0 in some cell)
   // keep FP64 products: the evanescent modes of such layers make the cascade
-  // ill-conditioned beyond what 3xTF32 (about 21 bits) can carry.
+  // ill-conditioned beyond what 3xTF32 (about 21 bits) can carry.  They share
+  // chunks with the other points; each cascade product is then two batched
+  // calls, one per precision.
   std::vector<char> metallic(n_stacks, 0);
   for (int s = 0; s < n_stacks; ++s)
     for (const cplx& z : si[s].eps)
@@ -417,18 +486,20 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   std::map<std::tuple<int, int, int>, std::vector<int>> groups;
   for (int p = 0; p < n_pts; ++p) {
     const int s = pts[p].stack;
-    const int f64 = precision == RCWA_PREC_MIXED ? metallic[s] : 0;
-    groups[{si[s].nx, si[s].ny, f64}].push_back(p);
+    groups[{si[s].nx, si[s].ny, 0}].push_back(p);
   }
   std::vector<ChunkWork> chunks;
   std::vector<int> chunk_N;
   for (auto& g : groups) {
     const int N = std::get<0>(g.first) * std::get<1>(g.first);
-    const bool f64 = std::get<2>(g.first) != 0;
     size_t used = 0;
     ChunkWork cur;
     auto flush = [&]() {
-      if (!cur.points.empty()) { cur.fp64 = f64; chunks.push_back(cur); chunk_N.push_back(N); }
+      if (!cur.points.empty()) {
+        for (int p : cur.points) cur.fp64_pt.push_back(precision == RCWA_PREC_MIXED ? metallic[pts[p].stack] : 1);
+        chunks.push_back(cur);
+        chunk_N.push_back(N);
+      }
       cur = ChunkWork();
       used = 0;
     };
@@ -458,6 +529,19 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         c.job_layer.push_back(l);
       }
     }
+  }
+  // schedules of each chunk's large operations (may time candidates on the
+  // device when the engine's tuner measures on a miss)
+  for (size_t ci = 0; ci < chunks.size(); ++ci) {
+    ChunkWork& c = chunks[ci];
+    const int n = 2 * chunk_N[ci], np = (int)c.points.size(), nj = (int)c.job_point.size();
+    c.lu_if = tune_resolve(e, kTuneLU, n, 2 * np);
+    c.lu_tau = tune_resolve(e, kTuneLU, n, np);
+    if (nj > 0) c.ms_min = tune_resolve(e, kTuneSchur, n, nj);
+    int n_tc = 0;
+    for (char f : c.fp64_pt) n_tc += f ? 0 : 1;
+    c.prod = n_tc > 0 ? tune_resolve(e, kTuneProduct, n, n_tc) : 1;
+    P->sched.push_back({n, np, c.lu_if, c.lu_tau, c.ms_min, c.prod});
   }
   size_t wbytes = 0;
   for (size_t ci = 0; ci < chunks.size(); ++ci) wbytes = std::max(wbytes, chunk_layout(chunks[ci], si, chunk_N[ci]));
@@ -621,6 +705,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       void* eigw = wb + c.eigw;
       int* einfo = (int*)(wb + c.einfo);
       int* status = P->dStatus;
+      const int ms_min = c.ms_min;
       P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
         char* m = (char*)plan->meta.p;
         GemmArgs g{};
@@ -640,7 +725,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         if ((err = assemble_m(it, nj, N, st)) != cudaSuccess) return err;
         pf.mark(st, kStAssemble);
         if ((err = zgeev_batched((cplx* const*)(m + oM), n, n, mu, (cplx* const*)(m + oW), n, eigw, einfo, nj, st,
-                                 &pf)) != cudaSuccess)
+                                 &pf, ms_min)) != cudaSuccess)
           return err;
         if ((err = fold_info(einfo, (const int*)(m + oJP), nj, 0, status, st)) != cudaSuccess) return err;
         GemmArgs v{};
@@ -732,6 +817,11 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           if (si[pts[c.points[lp]].stack].L - 1 > step) part.push_back(lp);
         const int k = (int)part.size();
         if (k == 0) continue;
+        // points whose products run in 3xTF32 first, the FP64 ones after them
+        const bool tc_plan = precision == RCWA_PREC_MIXED && c.prod == 0;
+        std::stable_partition(part.begin(), part.end(), [&](int lp) { return tc_plan && !c.fp64_pt[lp]; });
+        int kt = 0;
+        for (int lp : part) kt += (tc_plan && !c.fp64_pt[lp]) ? 1 : 0;
         std::vector<const cplx*> csrc(4 * k);
         std::vector<cplx*> cdst(4 * k), lu(2 * k), rhs(2 * k);
         std::vector<PhaseItem> ph;
@@ -787,11 +877,27 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         int* status = P->dStatus;
         int* tcerr = P->dTcErr;
         int* tcscale = P->dTcScale;
-        const bool mixed = precision == RCWA_PREC_MIXED && !c.fp64;
+        const int lu_if = c.lu_if, lu_tau = c.lu_tau;
         P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
-          // the cascade products: FP64 tensor path, or 3xTF32 on tcgen05
+          // the cascade products: items [0, kt) in 3xTF32 on tcgen05, the
+          // rest on the FP64 tensor path
           auto product = [&](const GemmArgs& ga) {
-            return mixed ? zgemm_tf32x3_batched(ga, tcscale, tcerr, st) : zgemm_batched(ga, st);
+            cudaError_t x = cudaSuccess;
+            if (kt > 0) {
+              GemmArgs t = ga;
+              t.batch = kt;
+              x = zgemm_tf32x3_batched(t, tcscale, tcerr, st);
+            }
+            if (x == cudaSuccess && kt < ga.batch) {
+              GemmArgs f = ga;
+              f.A = ga.A + kt;
+              f.B = ga.B + kt;
+              f.C = ga.C ? ga.C + kt : nullptr;
+              f.D = ga.D + kt;
+              f.batch = ga.batch - kt;
+              x = zgemm_batched(f, st);
+            }
+            return x;
           };
           char* m = (char*)plan->meta.p;
           auto cpa = [m](size_t o) { return (const cplx* const*)(m + o); };
@@ -800,7 +906,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           // interface matrices IE = Wa^-1 Wb, IH = Va^-1 Vb (rcwa/RCWASolver.cpp:537-543)
           if ((err = zcopy_batched(cpa(ocs), n, pa(ocd), n, n, n, 4 * k, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
-          if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * k, st)) != cudaSuccess) return err;
+          if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * k, st, lu_if)) != cudaSuccess) return err;
           if ((err = fold_info(pinfo, (const int*)(m + oip), 2 * k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStInterfaceLU);
@@ -827,7 +933,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           if ((err = zaxpby_batched(cpa(osF), cpa(osG), pa(osD), mkc(1, 0), mkc(1, 0), n, k, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStTau);
-          if ((err = zgetrf_batched(pa(oSp), n, n, pipiv, pinfo, k, st)) != cudaSuccess) return err;
+          if ((err = zgetrf_batched(pa(oSp), n, n, pipiv, pinfo, k, st, lu_tau)) != cudaSuccess) return err;
           if ((err = fold_info(pinfo, (const int*)(m + osp), k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStTauLU);
@@ -886,8 +992,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     }
   }
   P->chunks = (int)chunks.size();
-  if (cudaMalloc(&P->meta.p, std::max<size_t>(meta.bytes.size(), 16)) != cudaSuccess)
-    return fail(e, RCWA_ERR_NOMEM, "metadata allocation failed");
+  if (!P->meta.take(e, std::max<size_t>(meta.bytes.size(), 16))) return fail(e, RCWA_ERR_NOMEM, "metadata allocation failed");
   P->meta.bytes = meta.bytes.size();
   if (!meta.bytes.empty() &&
       cudaMemcpy(P->meta.p, meta.bytes.data(), meta.bytes.size(), cudaMemcpyHostToDevice) != cudaSuccess)
@@ -985,6 +1090,14 @@ extern "C" int rcwa_plan_rescatter(rcwa_plan* p, const rcwa_cplx* pxy) {
   return cudaStreamSynchronize(st) == cudaSuccess ? RCWA_OK : RCWA_ERR_CUDA;
 }
 
+extern "C" int rcwa_plan_schedule(const rcwa_plan* p, int chunk, int* sched) {
+  if (!p) return -1;
+  if (chunk < 0 || !sched) return (int)p->sched.size();
+  if (chunk >= (int)p->sched.size()) return -1;
+  for (int k = 0; k < 6; ++k) sched[k] = p->sched[chunk][k];
+  return (int)p->sched.size();
+}
+
 extern "C" long long rcwa_plan_launch_count(const rcwa_plan* p) { return p ? p->launches : 0; }
 
 extern "C" int rcwa_plan_set_profiling(rcwa_plan* p, int on) {
@@ -1017,20 +1130,21 @@ extern "C" int rcwa_plan_results(rcwa_plan* p, double* R, double* T, double* ref
   if (cudaDeviceSynchronize() != cudaSuccess)
     return fail(p->e, RCWA_ERR_CUDA, std::string("execution failed: ") + cudaGetErrorString(cudaGetLastError()));
   const size_t ne = (size_t)p->n_pts * p->n_exc;
-  if (R && cudaMemcpy(R, p->dR, sizeof(double) * ne, cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
-  if (T && cudaMemcpy(T, p->dT, sizeof(double) * ne, cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
-  if (ref_orders &&
-      cudaMemcpy(ref_orders, p->dRef, sizeof(double) * p->total_orders, cudaMemcpyDeviceToHost) != cudaSuccess)
-    return RCWA_ERR_CUDA;
-  if (trn_orders &&
-      cudaMemcpy(trn_orders, p->dTrn, sizeof(double) * p->total_orders, cudaMemcpyDeviceToHost) != cudaSuccess)
-    return RCWA_ERR_CUDA;
+  // one download of the output block (R, T, orders, status, tensor-core flag)
+  const char* base = (const char*)p->outputs.p;
+  const size_t span = (size_t)((const char*)(p->dTcErr + 1) - base);
+  std::vector<unsigned char> h(span);
+  if (cudaMemcpy(h.data(), base, span, cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
+  auto at = [&](const void* d) { return h.data() + ((const char*)d - base); };
+  if (R) std::memcpy(R, at(p->dR), sizeof(double) * ne);
+  if (T) std::memcpy(T, at(p->dT), sizeof(double) * ne);
+  if (ref_orders) std::memcpy(ref_orders, at(p->dRef), sizeof(double) * p->total_orders);
+  if (trn_orders) std::memcpy(trn_orders, at(p->dTrn), sizeof(double) * p->total_orders);
   std::vector<int> hs(p->n_pts);
-  if (cudaMemcpy(hs.data(), p->dStatus, sizeof(int) * p->n_pts, cudaMemcpyDeviceToHost) != cudaSuccess)
-    return RCWA_ERR_CUDA;
+  std::memcpy(hs.data(), at(p->dStatus), sizeof(int) * p->n_pts);
   if (status) std::memcpy(status, hs.data(), sizeof(int) * p->n_pts);
   int tcerr = 0;
-  if (cudaMemcpy(&tcerr, p->dTcErr, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return RCWA_ERR_CUDA;
+  std::memcpy(&tcerr, at(p->dTcErr), sizeof(int));
   if (tcerr) return fail(p->e, RCWA_ERR_CUDA, "a tensor-core completion wait ran out; results are incomplete");
   for (int v : hs)
     if (v) return v;

@@ -404,10 +404,16 @@ int sm_count() {
 }
 }  // namespace
 
+int zgetrf_default_schedule(int n, int batch, int sms) {
+  if (sms <= 0) sms = sm_count();
+  return (n <= 128 || batch >= 4 * sms) ? 0 : 1;
+}
+
 cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
-                           cudaStream_t st) {
+                           cudaStream_t st, int schedule) {
   if (batch <= 0 || n <= 0) return cudaSuccess;
-  if (n <= 128 || batch >= 4 * sm_count()) {
+  if (schedule < 0) schedule = zgetrf_default_schedule(n, batch);
+  if (schedule == 0) {
     zgetrf_kernel<<<batch, kTileThreads, 0, st>>>(A, n, lda, ipiv, info);
     ++launch_counter();
     return cudaGetLastError();

@@ -32,12 +32,15 @@ cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st);
 
 // In-place LU with partial pivoting (row interchanges, LAPACK getrf
 // convention, 0-based pivots) of square n x n matrices.  info[b] = 0, or k+1
-// when U(k,k) is exactly zero.  Batches that fill the GPU run one CTA per
-// matrix; smaller batches of large matrices run panel by panel, the panel
-// factorisation one CTA per matrix and the triangular solve and trailing
-// update spread over all SMs.
+// when U(k,k) is exactly zero.  schedule 0: one CTA factors each matrix;
+// schedule 1: panel by panel, the panel factorisation one CTA per matrix and
+// the triangular solve and trailing update spread over all SMs; -1: the
+// default rule (zgetrf_default_schedule: schedule 0 for n <= 128 or batches of
+// at least four waves of CTAs, else 1).  Both pivot by the same rule; their
+// rounding differs in the trailing updates.
+int zgetrf_default_schedule(int n, int batch, int sms = 0);  // sms <= 0: this device's SM count
 cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
-                           cudaStream_t st);
+                           cudaStream_t st, int schedule = -1);
 
 // Solve A X = B in place of B (n x nrhs) from the factors of zgetrf_batched.
 cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipiv,
