@@ -43,7 +43,7 @@ struct Scratch {
 #ifdef RCWA_EIG_STATS
 // counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles,
 // 8 early-deflation cycles, 9 single-shift cycles, 10 Schur cycles, 11 early deflations, 12 deflated by them
-__device__ unsigned long long g_eig_stats[16];
+__device__ unsigned long long g_eig_stats[32];
 #define STAT_ADD(i, v) do { if (threadIdx.x == 0) atomicAdd(&g_eig_stats[i], (unsigned long long)(v)); } while (0)
 #else
 #define STAT_ADD(i, v) do { } while (0)
@@ -139,6 +139,9 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
   // so that every sweep over the rows is coalesced
   cplx* Vc = s.Vb;
   cplx* Yc = s.Yb;
+  // v_j in shared memory during the panel (aliases the tile buffer)
+  cplx* vs = reinterpret_cast<cplx*>(&tsm);
+  const bool vs_ok = (size_t)n * sizeof(cplx) <= sizeof(TileSmem);
   for (int k = 0; k + 2 < n; k += nb) {
 #ifdef RCWA_EIG_STATS
     const long long c_p0 = clock64();
@@ -148,6 +151,12 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
     for (int idx = tid; idx < nb * nb; idx += blockDim.x) T[idx] = mkc(0.0, 0.0);
     for (int jj = 0; jj < jb; ++jj) {
       const int j = k + jj;
+#ifdef RCWA_EIG_STATS
+      long long h_t = clock64();
+#define HMARK(i) do { if (tid == 0) { const long long t_ = clock64(); atomicAdd(&g_eig_stats[i], (unsigned long long)(t_ - h_t)); h_t = t_; } } while (0)
+#else
+#define HMARK(i) do {} while (0)
+#endif
       // a = A0(:, j) - Y(:, :jj) conj(V(j, :jj))
       for (int i = tid; i < n; i += blockDim.x) {
         cplx acc = A[(size_t)i * lda + j];
@@ -155,6 +164,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         a[i] = acc;
       }
       __syncthreads();
+      HMARK(16);
       if (jj > 0) {
         // a(k+1:) <- (I - V T^H V^H) a(k+1:):  z = V^H a, z = T^H z, a -= V z
         for (int q = wid; q < jj; q += nw) {
@@ -180,6 +190,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         }
         __syncthreads();
       }
+      HMARK(17);
       // reflector from a(j+1:)
       double sig = 0.0;
       for (int i = j + 2 + tid; i < n; i += blockDim.x) sig += cnorm2(a[i]);
@@ -195,7 +206,9 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         v0 = cscale(ph, aa + xnorm);
         tau = 2.0 / (cnorm2(v0) + sig);
       }
-      // column j of the result; explicit v_j in V(:, jj) and V^H(jj, :)
+      // column j of the result; explicit v_j in V(:, jj) and V^H(jj, :),
+      // and in shared memory for the matrix-vector product (the tile
+      // buffer is free during the panel)
       for (int i = tid; i < n; i += blockDim.x) {
         cplx vi = mkc(0.0, 0.0);
         if (i <= j) A[(size_t)i * lda + j] = a[i];
@@ -205,35 +218,50 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         Vc[(size_t)jj * n + i] = vi;
         s.VH[(size_t)jj * n + i] = cconj(vi);
         a[i] = vi;
+        if (vs_ok) vs[i] = vi;
       }
       if (tid == 0) { s.tau[j] = tau; s.v0[j] = v0; }
       __syncthreads();
+      HMARK(18);
       // u = A0(:, j+1:) v_j (one pass over the trailing columns), z = V(:, :jj)^H v_j.
-      // The pass streams the trailing matrix from DRAM; eight independent
-      // loads per lane keep enough bytes in flight to cover the latency.
-      for (int i = wid; i < n; i += nw) {
-        const cplx* row = A + (size_t)i * lda;
-        cplx acc[8];
+      // The pass is bound by the loads in flight (the trailing matrix mostly
+      // comes from L2): a warp takes two rows at a time and issues all eight
+      // loads of a 128-column step at once, predicated at the row end rather
+      // than finished by a serial tail loop; v_j comes from shared memory.
+      const cplx* vj = vs_ok ? vs : a;
+      for (int i0 = 2 * wid; i0 < n; i0 += 2 * nw) {
+        const bool two = i0 + 1 < n;
+        const cplx* row0 = A + (size_t)i0 * lda;
+        const cplx* row1 = two ? row0 + lda : row0;
+        cplx acc0 = mkc(0.0, 0.0), acc1 = mkc(0.0, 0.0);
+        for (int c = j + 1 + lane; c < n; c += 128) {
+          cplx r0[4], r1[4], w[4];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) acc[q] = mkc(0.0, 0.0);
-        int c = j + 1 + lane;
-        for (; c + 224 < n; c += 256) {
-          cplx r[8];
+          for (int q = 0; q < 4; ++q) {
+            const int cc = c + 32 * q;
+            const bool in = cc < n;
+            r0[q] = in ? row0[cc] : mkc(0.0, 0.0);
+            r1[q] = in ? row1[cc] : mkc(0.0, 0.0);
+            w[q] = in ? vj[cc] : mkc(0.0, 0.0);
+          }
 #pragma unroll
-          for (int q = 0; q < 8; ++q) r[q] = row[c + 32 * q];
-#pragma unroll
-          for (int q = 0; q < 8; ++q) acc[q] = cfma(r[q], a[c + 32 * q], acc[q]);
+          for (int q = 0; q < 4; ++q) {
+            acc0 = cfma(r0[q], w[q], acc0);
+            acc1 = cfma(r1[q], w[q], acc1);
+          }
         }
-        for (; c < n; c += 32) acc[0] = cfma(row[c], a[c], acc[0]);
-        cplx acc0 = acc[0];
-#pragma unroll
-        for (int q = 1; q < 8; ++q) acc0 = cadd(acc0, acc[q]);
         for (int off = 16; off > 0; off >>= 1) {
           acc0.x += __shfl_xor_sync(0xffffffffu, acc0.x, off);
           acc0.y += __shfl_xor_sync(0xffffffffu, acc0.y, off);
+          acc1.x += __shfl_xor_sync(0xffffffffu, acc1.x, off);
+          acc1.y += __shfl_xor_sync(0xffffffffu, acc1.y, off);
         }
-        if (lane == 0) u[i] = acc0;
+        if (lane == 0) {
+          u[i0] = acc0;
+          if (two) u[i0 + 1] = acc1;
+        }
       }
+      HMARK(19);
       for (int q = wid; q < jj; q += nw) {
         cplx acc = mkc(0.0, 0.0);
         for (int i = j + 1 + lane; i < n; i += 32) acc = cfmaconj(Vc[(size_t)q * n + i], Vc[(size_t)jj * n + i], acc);
@@ -244,6 +272,7 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         if (lane == 0) z[q] = acc;
       }
       __syncthreads();
+      HMARK(20);
       // Y(:, jj) = tau (u - Y(:, :jj) z); T(:jj, jj) = -tau T(:jj, :jj) z; T(jj, jj) = tau
       for (int i = tid; i < n; i += blockDim.x) {
         cplx acc = u[i];
@@ -257,6 +286,8 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       }
       if (tid == 0) T[jj * nb + jj] = mkc(tau, 0.0);
       __syncthreads();
+      HMARK(21);
+#undef HMARK
     }
 #ifdef RCWA_EIG_STATS
     const long long c_p1 = clock64();
@@ -1480,11 +1511,11 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
 
 #ifdef RCWA_EIG_STATS
 extern "C" int rcwa_debug_eig_stats(unsigned long long* out, int reset) {
-  unsigned long long h[16];
+  unsigned long long h[32];
   if (cudaMemcpyFromSymbol(h, g_eig_stats, sizeof(h)) != cudaSuccess) return 2;
-  for (int i = 0; i < 16; ++i) out[i] = h[i];
+  for (int i = 0; i < 32; ++i) out[i] = h[i];
   if (reset) {
-    unsigned long long z[16] = {};
+    unsigned long long z[32] = {};
     cudaMemcpyToSymbol(g_eig_stats, z, sizeof(z));
   }
   return 0;
