@@ -822,12 +822,16 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         std::stable_partition(part.begin(), part.end(), [&](int lp) { return tc_plan && !c.fp64_pt[lp]; });
         int kt = 0;
         for (int lp : part) kt += (tc_plan && !c.fp64_pt[lp]) ? 1 : 0;
-        std::vector<const cplx*> csrc(4 * k);
-        std::vector<cplx*> cdst(4 * k), lu(2 * k), rhs(2 * k);
+        // interfaces whose upper layer a is a patterned layer take the dense
+        // LU route; those below the uniform superstrate (a = 0: Wa = I, Va
+        // 2x2-block diagonal) take IE = Wb and the per-order 2x2 solve
+        std::vector<const cplx*> csrc, csrcV;
+        std::vector<cplx*> cdst, cdstV, lu, luV, rhs, rhsV;
+        std::vector<HalfSolveItem> hs;
         std::vector<PhaseItem> ph;
         std::vector<const cplx*> fA(k), fB(k), fC(k), gA(k), gB(k), gC(k), sF(k), sG(k), tG(k), tT(k), tTau(k);
         std::vector<cplx*> fD(k), gD(k), sD(k), tauD(k), rD(k), tD(k), Sp(k);
-        std::vector<int> ipoint(2 * k), spoint(k);
+        std::vector<int> ipoint, spoint(k);
         for (int q = 0; q < k; ++q) {
           const int lp = part[q], p = c.points[lp];
           const int L = si[pts[p].stack].L;
@@ -836,13 +840,21 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           cplx* IH = W_(c.IH) + nn * lp;
           cplx* WLU = W_(c.WLU) + nn * lp;
           cplx* VLU = W_(c.VLU) + nn * lp;
-          csrc[q] = layerW(lp, a); cdst[q] = WLU;
-          csrc[k + q] = layerV(lp, a); cdst[k + q] = VLU;
-          csrc[2 * k + q] = layerW(lp, b); cdst[2 * k + q] = IE;
-          csrc[3 * k + q] = layerV(lp, b); cdst[3 * k + q] = IH;
-          lu[q] = WLU; lu[k + q] = VLU;
-          rhs[q] = IE; rhs[k + q] = IH;
-          ipoint[q] = p; ipoint[k + q] = p;
+          csrc.push_back(layerW(lp, b)); cdst.push_back(IE);
+          csrc.push_back(layerV(lp, b)); cdst.push_back(IH);
+          if (a == 0) {
+            HalfSolveItem h;
+            h.X = IH;
+            h.V0 = layerV(lp, 0);
+            h.point = p;
+            hs.push_back(h);
+          } else {
+            csrcV.push_back(layerW(lp, a)); cdstV.push_back(WLU);
+            csrcV.push_back(layerV(lp, a)); cdstV.push_back(VLU);
+            lu.push_back(WLU); luV.push_back(VLU);
+            rhs.push_back(IE); rhsV.push_back(IH);
+            ipoint.push_back(p);
+          }
           spoint[q] = p;
           if (step > 0) {
             PhaseItem it;
@@ -863,8 +875,17 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           tT[q] = tdd[lp]; tD[q] = gbuf[lp];
           std::swap(tdd[lp], gbuf[lp]);
         }
+        // LU batch: the W's of the dense-route points, then their V's
+        const int kd = (int)lu.size(), kh = (int)hs.size();
+        csrc.insert(csrc.end(), csrcV.begin(), csrcV.end());
+        cdst.insert(cdst.end(), cdstV.begin(), cdstV.end());
+        lu.insert(lu.end(), luV.begin(), luV.end());
+        rhs.insert(rhs.end(), rhsV.begin(), rhsV.end());
+        const std::vector<int> ipointW = ipoint;
+        ipoint.insert(ipoint.end(), ipointW.begin(), ipointW.end());
+        const int ncopy = (int)csrc.size();
         const size_t ocs = meta.add_vec(csrc), ocd = meta.add_vec(cdst), olu = meta.add_vec(lu), orhs = meta.add_vec(rhs);
-        const size_t oip = meta.add_vec(ipoint), osp = meta.add_vec(spoint);
+        const size_t oip = meta.add_vec(ipoint), osp = meta.add_vec(spoint), ohs = meta.add_vec(hs);
         const size_t oph = meta.add_vec(ph);
         const int nph = (int)ph.size();
         const size_t ofA = meta.add_vec(fA), ofB = meta.add_vec(fB), ofC = meta.add_vec(fC), ofD = meta.add_vec(fD);
@@ -904,13 +925,14 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
           auto pa = [m](size_t o) { return (cplx* const*)(m + o); };
           cudaError_t err;
           // interface matrices IE = Wa^-1 Wb, IH = Va^-1 Vb (rcwa/RCWASolver.cpp:537-543)
-          if ((err = zcopy_batched(cpa(ocs), n, pa(ocd), n, n, n, 4 * k, st)) != cudaSuccess) return err;
+          if ((err = zcopy_batched(cpa(ocs), n, pa(ocd), n, n, n, ncopy, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
-          if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * k, st, lu_if)) != cudaSuccess) return err;
-          if ((err = fold_info(pinfo, (const int*)(m + oip), 2 * k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
+          if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * kd, st, lu_if)) != cudaSuccess) return err;
+          if ((err = fold_info(pinfo, (const int*)(m + oip), 2 * kd, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStInterfaceLU);
-          if ((err = zgetrs_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * k, st)) != cudaSuccess) return err;
+          if ((err = zgetrs_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * kd, st)) != cudaSuccess) return err;
+          if ((err = halfspace_solve((const HalfSolveItem*)(m + ohs), kh, N, status, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
           if (nph > 0) {
             if ((err = apply_phase((const PhaseItem*)(m + oph), nph, n, st)) != cudaSuccess) return err;

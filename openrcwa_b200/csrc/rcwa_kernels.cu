@@ -109,6 +109,34 @@ __global__ void halfspace_kernel(const HalfItem* items, int N, int* status) {
   }
 }
 
+// The interface matrices IH = Va^-1 Vb of rcwa/RCWASolver.cpp:537-543 when
+// layer a is the uniform superstrate: Va couples only rows h and N+h, so its
+// LU is N independent 2x2 eliminations (IE = Wa^-1 Wb = Wb since Wa = I).
+__global__ void halfspace_solve_kernel(const HalfSolveItem* items, int N, int* status) {
+  const HalfSolveItem it = items[blockIdx.y];
+  const int n = 2 * N;
+  const size_t total = (size_t)N * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int h = (int)(e / n), c = (int)(e % n);
+    cplx p = it.V0[(size_t)h * n + h], q = it.V0[(size_t)h * n + N + h];
+    cplx r = it.V0[(size_t)(N + h) * n + h], s = it.V0[(size_t)(N + h) * n + N + h];
+    cplx x0 = it.X[(size_t)h * n + c], x1 = it.X[(size_t)(N + h) * n + c];
+    if (cabs1(r) > cabs1(p)) {
+      cplx t = p; p = r; r = t;
+      t = q; q = s; s = t;
+      t = x0; x0 = x1; x1 = t;
+    }
+    if (p.x == 0.0 && p.y == 0.0) { set_status(status, it.point, RCWA_ERR_SINGULAR); continue; }
+    const cplx l = cdiv(r, p);
+    const cplx u = csub(s, cmul(l, q));
+    if (u.x == 0.0 && u.y == 0.0) { set_status(status, it.point, RCWA_ERR_SINGULAR); continue; }
+    const cplx y1 = cdiv(csub(x1, cmul(l, x0)), u);
+    const cplx y0 = cdiv(csub(x0, cmul(q, y1)), p);
+    it.X[(size_t)h * n + c] = y0;
+    it.X[(size_t)(N + h) * n + c] = y1;
+  }
+}
+
 // waveRud = Phi Rud Phi, waveTdd = Tdd Phi, Phi = diag(exp(i gamma d))
 // (rcwa/RCWASolver.cpp:421-434).
 __global__ void phase_kernel(const PhaseItem* items, int n) {
@@ -238,6 +266,13 @@ cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, 
 cudaError_t halfspace_modes(const HalfItem* items, int count, int N, int* status, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   halfspace_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, status);
+  ++launch_counter();
+  return cudaGetLastError();
+}
+
+cudaError_t halfspace_solve(const HalfSolveItem* items, int count, int N, int* status, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  halfspace_solve_kernel<<<ew_grid((size_t)2 * N * N, count), 256, 0, st>>>(items, N, status);
   ++launch_counter();
   return cudaGetLastError();
 }

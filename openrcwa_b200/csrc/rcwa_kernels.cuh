@@ -29,6 +29,13 @@ struct HalfItem {
   int point;
 };
 
+// Interface whose upper layer is a uniform half-space: X <- V0^-1 X.
+struct HalfSolveItem {
+  cplx* X;            // n x n right-hand sides, overwritten
+  const cplx* V0;     // n x n half-space V (2x2 blocks of diagonal N x N blocks)
+  int point;
+};
+
 struct PhaseItem {
   cplx* Rud;
   cplx* Tdd;
@@ -54,6 +61,11 @@ cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st
 cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st);
 cudaError_t halfspace_modes(const HalfItem* items, int count, int N, int* status, cudaStream_t st);
 cudaError_t apply_phase(const PhaseItem* items, int count, int n, cudaStream_t st);
+// X <- V0^-1 X per item: for each order h, rows h and N+h of X against the 2x2
+// block [V0(h,h) V0(h,N+h); V0(N+h,h) V0(N+h,N+h)] by Gaussian elimination
+// with partial pivoting (the steps the dense LU takes on this structure);
+// an exactly singular block sets RCWA_ERR_SINGULAR for the item's point.
+cudaError_t halfspace_solve(const HalfSolveItem* items, int count, int N, int* status, cudaStream_t st);
 cudaError_t scatter_efficiencies(const ScatterItem* items, int count, int N, int nx, int ny, int* status,
                                  cudaStream_t st);
 // D = a*X + b*Y (n x n) for every item
