@@ -81,6 +81,8 @@ typedef struct {
 /* ---- engine ----------------------------------------------------------------- */
 const char* rcwa_status_string(int status);
 int rcwa_engine_create(int device, rcwa_engine** out);
+/* Destroy every plan and surrogate network of the engine first: plans return
+ * their device buffers to the engine's pool and workspace cache. */
 void rcwa_engine_destroy(rcwa_engine* e);
 /* Message of the last failure on this engine ("" if none). */
 const char* rcwa_engine_last_error(const rcwa_engine* e);

@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
+import weakref
 from typing import Optional, Sequence
 
 import numpy as np
@@ -208,9 +209,14 @@ class Engine:
         if rc:
             raise RcwaError(rc, "engine_create")
         self.h = h
+        # plans and networks of this engine: destroyed before the engine, whose
+        # buffer pool and workspace cache they return their memory to
+        self._children = weakref.WeakSet()
 
     def close(self):
         if self.h:
+            for child in list(self._children):
+                child.close()
             self.lib.rcwa_engine_destroy(self.h)
             self.h = None
 
@@ -410,6 +416,7 @@ class Plan:
         rc = eng.lib.rcwa_plan_create(eng.h, st, len(stacks), cp, len(cp), n_exc, _v(pxy), precision, C.byref(h))
         eng._check(rc, "plan_create")
         self.h = h
+        eng._children.add(self)
 
     def execute(self, stream: Optional[int] = None):
         self.eng._check(self.eng.lib.rcwa_plan_execute(self.h, C.c_void_p(stream) if stream else None),
@@ -482,6 +489,7 @@ class Mlp:
         h = C.c_void_p()
         eng._check(eng.lib.rcwa_mlp_create(eng.h, n_in, n_hidden, n_layers, n_out, seed, C.byref(h)), "mlp_create")
         self.h = h
+        eng._children.add(self)
 
     def param_count(self):
         return int(self.eng.lib.rcwa_mlp_param_count(self.h))
