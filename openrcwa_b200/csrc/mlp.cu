@@ -10,7 +10,7 @@
 //               GELU fused into the epilogue
 //
 // No counterpart in the reference; the engine's plain FP64 solve is the
-// surrogate's fallback and the judge of its error (host side,
+// surrogate's fallback and the reference for its error (host side,
 // openrcwa_b200/surrogate.py).
 #include <cmath>
 #include <cstdint>

@@ -1,5 +1,5 @@
 """Learned surrogate of the RCWA efficiencies, with the FP64 solve as its
-fallback and the judge of its error.
+fallback and the reference for its error.
 
 The network (rcwa_mlp_*: GPU training and tensor-core inference) maps eleven
 grating parameters -- fill_x, fill_y, thickness, Re/Im eps1, eps2, lambda,
