@@ -107,3 +107,18 @@ def test_load_rejects_bad_files_whole(tuner, tmp_path):
         assert t.entries() == []
     with pytest.raises(o.RcwaError):
         t.load(os.path.join(tmp_path, "missing.txt"))
+
+
+def test_schedule_table_from_plain_c(tmp_path):
+    # the same table calls from a C program linked against the library
+    import subprocess
+    from tests.test_abi_cpu import ROOT
+    o, _ = _lib()
+    exe = os.path.join(tmp_path, "tuner_table")
+    lib_dir = os.path.dirname(o.abi.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "tuner_table.c"), "-L", lib_dir, "-lrcwa_b200",
+                    "-Wl,-rpath," + lib_dir, "-o", exe], check=True)
+    out = subprocess.run([exe, os.path.join(tmp_path, "table.txt")], capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "ok"
