@@ -8,11 +8,16 @@
 //           M = PQ/k0^2, eig(M) -> (mu, W), gamma, V = QW/keff; analytic
 //           half-space modes per point
 //   cascade per interface, bottom to top (rcwa/RCWASolver.cpp:378-492):
-//           IE = Wa^-1 Wb, IH = Va^-1 Vb, phase, F, G, tau = (F+G)^-1,
-//           Rud = I - 2 G tau, Tdd = 2 waveTdd tau
+//           IE = Wa^-1 Wb, IH = Va^-1 Vb (below the uniform superstrate:
+//           IE = Wb and a 2x2 solve per order), phase, F, G,
+//           tau = (F+G)^-1, Rud = I - 2 G tau, Tdd = 2 waveTdd tau; in mixed
+//           plans the products of points without a metallic layer run in
+//           3xTF32 on the tensor cores, the others on the FP64 path
 //   scatter per (point, excitation): per-order efficiencies and their sums.
 // Every batched call receives device pointer arrays that the plan built once,
 // so executing a plan is a fixed sequence of kernel launches on one stream.
+// The LU schedules, the Schur crossover and the product path of each chunk
+// come from the engine's schedule tuner or its built-in rules (tuner.cu).
 #include <algorithm>
 #include <array>
 #include <cmath>
