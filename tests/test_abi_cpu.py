@@ -101,3 +101,34 @@ def test_workload_shapes():
     assert st[0].N == 11 and pts.shape == (16, 4)
     starts = {workloads.shard_start(r, 4, 32, k) for r in range(4) for k in range(3)}
     assert len(starts) == 12
+
+
+def test_uneven_workload_distribution():
+    # the uneven batch: orders, layer counts and materials span their ranges
+    from openrcwa_b200 import workloads
+    st, pts, pxy = workloads.uneven_batch(seed=0, n_instances=400)
+    assert len(st) == 400 and pts.shape == (400, 4) and pxy.shape == (400, 2, 2)
+    nh = np.array([s.nHx for s in st])
+    assert nh.min() == 3 and nh.max() == 15 and np.all(np.array([s.nHy for s in st]) == nh)
+    layers = np.array([s.eps.shape[0] - 2 for s in st])
+    assert layers.min() == 1 and layers.max() == 10
+    lam = pts[:, 1]
+    assert lam.min() >= 400e-9 and lam.max() <= 1000e-9
+    theta = np.degrees(np.arcsin(pts[:, 2] / (2 * np.pi / lam)))
+    assert theta.min() >= 0 and theta.max() <= 70 and np.all(pts[:, 3] == 0)
+    eps_in = np.concatenate([s.eps[1:-1].reshape(s.eps.shape[0] - 2, -1)[:, 0] for s in st])
+    # half the layers are drawn as lossy metal, the rest from the Lorentz pole
+    # (which is also negative above its resonance); all are passive
+    box = (eps_in.real >= -30) & (eps_in.real <= -5) & (eps_in.imag >= 0.5) & (eps_in.imag <= 3)
+    assert 0.3 < box.mean() < 0.7
+    assert np.all(np.isfinite(eps_in)) and np.all(eps_in.imag >= 0)
+    thick = np.concatenate([s.thickness[1:-1] for s in st])
+    assert thick.min() >= 20e-9 and thick.max() <= 500e-9
+
+
+def test_surrogate_sampler_ranges():
+    from openrcwa_b200 import surrogate
+    P = surrogate.sample(5000, np.random.default_rng(0))
+    assert P.shape == (5000, len(surrogate.PARAMS))
+    lo, hi = surrogate.RANGES[:, 0], surrogate.RANGES[:, 1]
+    assert np.all(P >= lo) and np.all(P <= hi)
