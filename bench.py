@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--tuning", default="auto", choices=["auto", "off"],
                     help="auto: the engine's autotuner times the candidate schedules of each new (decision, "
                          "matrix order, batch class) while a plan is created, before warm-up; off: built-in rules")
+    ap.add_argument("--smatrix", default=None, metavar="N,BATCH",
+                    help="the z-integrator entry points: BATCH slab S-matrices and star products of order N, "
+                         "end to end with host buffers")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
                     help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
@@ -199,6 +202,43 @@ def run_gemm_only(spec):
                                     "fp64_rel_err": float(np.max(np.abs(D6[0] - ref) / scale))}}))
     eng.close()
     return 0
+
+
+def run_smatrix(spec):
+    """The z-integrator entry points (row a13) end to end with host buffers:
+    BATCH slab S-matrices of order N (rcwa_slab_smatrix_batched) and BATCH
+    star products into a running S-matrix (rcwa_star_product_batched), on
+    seeded inputs: slab modes W, V near the identity, propagating and
+    evanescent gamma, the uniform reference medium W0 = I.  Wall time of one
+    call after a warm-up call, host copies included."""
+    import openrcwa_b200 as o
+    n, b = (int(x) for x in spec.split(","))
+    rng = np.random.default_rng(0)
+
+    def near_identity():
+        return np.eye(n) + 0.1 * (rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))) / np.sqrt(n)
+
+    W, V, V0 = near_identity(), near_identity(), near_identity()
+    W0 = np.broadcast_to(np.eye(n, dtype=complex), (b, n, n)).copy()
+    gamma = rng.uniform(0.5, 2.0, (b, n)) + 1j * rng.uniform(0.0, 0.5, (b, n))
+    eng = o.Engine(0)
+    out = {"n": n, "batch": b}
+    for rep in range(2):
+        t0 = time.perf_counter()
+        Rud, Tuu, st = eng.slab_smatrix(W, V, gamma, W0, V0, 6e-7, 1e-7)
+        t1 = time.perf_counter()
+        S = {"Rud": np.zeros((b, n, n), complex), "Rdu": np.zeros((b, n, n), complex),
+             "Tdd": np.broadcast_to(np.eye(n, dtype=complex), (b, n, n)).copy(),
+             "Tuu": np.broadcast_to(np.eye(n, dtype=complex), (b, n, n)).copy()}
+        S2, st2 = eng.star_product(S, {"rud": Rud, "rdu": Rud, "tdd": Tuu, "tuu": Tuu})
+        t2 = time.perf_counter()
+        out.update({"slab_ms": 1e3 * (t1 - t0), "slabs_per_s": b / (t1 - t0), "star_ms": 1e3 * (t2 - t1),
+                    "star_products_per_s": b / (t2 - t1), "status_nonzero": int(np.sum(st != 0) + np.sum(st2 != 0)),
+                    "finite": bool(np.all(np.isfinite(S2["Rud"])) and np.all(np.isfinite(S2["Tdd"]))),
+                    "timing": "wall clock of one call after a warm-up call, host buffers and copies included"})
+    print(json.dumps({"smatrix": out}), flush=True)
+    eng.close()
+    return 0 if out["status_nonzero"] == 0 and out["finite"] else 1
 
 
 def run_eig_only(spec):
@@ -357,6 +397,8 @@ def main():
         return run_eig_only(args.eig_only)
     if args.gemm_only:
         return run_gemm_only(args.gemm_only)
+    if args.smatrix:
+        return run_smatrix(args.smatrix)
     if args.surrogate:
         return run_surrogate(args)
     if args.uneven:
