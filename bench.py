@@ -575,6 +575,8 @@ def main():
                                     "interface/tau solves, half-spaces and efficiency sums FP64",
                        "parallelism": f"replicas x{world}",
                        "l2": "per-step working set several GB > 126 MB L2"},
+            "outputs_per_s": {"value": value * bpxy.shape[1], "unit": "(point, polarisation) R/T outputs/s",
+                              "note": "each solve serves both polarisations from one S-matrix"},
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "gpu_launches": launches, "clocks": clk, "roofline": roof, "tensor_gemm": tensor_gemm,
