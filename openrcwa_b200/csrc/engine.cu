@@ -120,7 +120,7 @@ struct rcwa_plan {
   // crossover, product path (0: 3xTF32, 1: FP64 tensor path)
   std::vector<std::array<int, 6>> sched;
   int precision = RCWA_PREC_FP64;
-  std::vector<std::function<cudaError_t(cudaStream_t, long long&, StageProf&)>> steps;
+  std::vector<std::function<cudaError_t(cudaStream_t, StageProf&)>> steps;
   long long launches = 0;
   std::unique_ptr<StageProf> prof{new StageProf()};
   // scatter items of a single-chunk plan, kept for rcwa_plan_rescatter
@@ -630,10 +630,10 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       CL.tyinv_ptrs = tp + 3 * strips * nconv;
       CL.ipiv = (int*)(wb + c.tipiv);
       CL.info = (int*)(wb + c.tinfo);
-      P->steps.push_back([plan, CL, jobs_meta](cudaStream_t st, long long& nl, StageProf& pf) {
+      P->steps.push_back([plan, CL, jobs_meta](cudaStream_t st, StageProf& pf) {
         ConvLaunch cl = CL;
         cl.jobs = (ConvJob*)((char*)plan->meta.p + jobs_meta);
-        cudaError_t err = conv_matrices(cl, st, &nl);
+        cudaError_t err = conv_matrices(cl, st);
         pf.mark(st, kStConvGather);
         return err;
       });
@@ -643,7 +643,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       const size_t o33 = meta.add_vec(f33), oE = meta.add_vec(einv);
       int* cipiv = (int*)(wb + c.cipiv);
       int* cinfo = (int*)(wb + c.cinfo);
-      P->steps.push_back([plan, o33, oE, N, nconv, cipiv, cinfo](cudaStream_t st, long long& nl, StageProf& pf) {
+      P->steps.push_back([plan, o33, oE, N, nconv, cipiv, cinfo](cudaStream_t st, StageProf& pf) {
         cplx* const* a = (cplx* const*)((char*)plan->meta.p + o33);
         cplx* const* b = (cplx* const*)((char*)plan->meta.p + oE);
         cudaError_t err;
@@ -711,7 +711,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       int* einfo = (int*)(wb + c.einfo);
       int* status = P->dStatus;
       const int ms_min = c.ms_min;
-      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+      P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
         char* m = (char*)plan->meta.p;
         GemmArgs g{};
         g.A = (const cplx* const*)(m + oA);
@@ -768,7 +768,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       const size_t oh = meta.add_vec(hs);
       int* status = P->dStatus;
       const int cnt = 2 * np;
-      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+      P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
         cudaError_t err = halfspace_modes((const HalfItem*)((char*)plan->meta.p + oh), cnt, N, status, st);
         pf.mark(st, kStHalfspace);
         return err;
@@ -784,7 +784,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         gbuf[lp] = W_(c.G) + nn * lp;
       }
       const size_t oR0 = meta.add_vec(rud), oT0 = meta.add_vec(tdd);
-      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+      P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
         cudaError_t err = cascade_init((cplx* const*)((char*)plan->meta.p + oR0),
                                        (cplx* const*)((char*)plan->meta.p + oT0), n, np, st);
         pf.mark(st, kStPhase);
@@ -904,7 +904,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         int* tcerr = P->dTcErr;
         int* tcscale = P->dTcScale;
         const int lu_if = c.lu_if, lu_tau = c.lu_tau;
-        P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+        P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
           // the cascade products: items [0, kt) in 3xTF32 on tcgen05, the
           // rest on the FP64 tensor path
           auto product = [&](const GemmArgs& ga) {
@@ -1010,7 +1010,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       P->scatter_nx = nx;
       P->scatter_ny = ny;
       int* status = P->dStatus;
-      P->steps.push_back([=](cudaStream_t st, long long& nl, StageProf& pf) {
+      P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
         cudaError_t err = scatter_efficiencies((const ScatterItem*)((char*)plan->meta.p + osc), nsc, N, nx, ny, status,
                                                st);
         pf.mark(st, kStScatter);
@@ -1034,11 +1034,10 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
 namespace {
 // The plan's launch sequence on stream st (status reset, then every step).
 cudaError_t issue_plan(rcwa_plan* p, cudaStream_t st) {
-  long long nl = 0;
   cudaError_t err = cudaMemsetAsync(p->dStatus, 0, sizeof(int) * p->n_pts, st);
   if (err == cudaSuccess) err = cudaMemsetAsync(p->dTcErr, 0, sizeof(int), st);
   p->prof->begin(st);
-  for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, nl, *p->prof);
+  for (size_t i = 0; err == cudaSuccess && i < p->steps.size(); ++i) err = p->steps[i](st, *p->prof);
   return err;
 }
 }  // namespace

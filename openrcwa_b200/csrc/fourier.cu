@@ -179,7 +179,7 @@ __global__ void fill_table_ptrs(const ConvJob* jobs, int njobs, int nx, int ny, 
 
 size_t conv_table_elems(int nx, int ny, int ncx, int ncy) { return tab_layout(nx, ny, ncx, ncy).total; }
 
-cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st, long long* launches) {
+cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st) {
   if (P.njobs <= 0) return cudaSuccess;
   const int mys = P.max_ncy - 1, mxs = P.max_ncx - 1;
   conv_tables_kernel<<<P.njobs, 256, 0, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy);
@@ -189,7 +189,6 @@ cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st, long long* launc
   ++launch_counter();
   cudaError_t err = cudaGetLastError();
   if (err != cudaSuccess) return err;
-  *launches += 2;
   if ((err = zgetrf_batched(P.tx_ptrs, P.nx, P.nx, P.ipiv, P.info, P.njobs * mys, st)) != cudaSuccess) return err;
   if ((err = zgetrs_batched(P.tx_ptrs, P.nx, P.nx, P.ipiv, P.txinv_ptrs, P.nx, P.nx, P.njobs * mys, st)) !=
       cudaSuccess)
@@ -198,13 +197,11 @@ cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st, long long* launc
   if ((err = zgetrs_batched(P.ty_ptrs, P.ny, P.ny, P.ipiv, P.tyinv_ptrs, P.ny, P.ny, P.njobs * mxs, st)) !=
       cudaSuccess)
     return err;
-  *launches += 4;
   const size_t NN = (size_t)P.nx * P.ny * P.nx * P.ny;
   const size_t nblk = (NN + 255) / 256;
   dim3 grid((unsigned)(nblk < 2048 ? nblk : 2048), P.njobs);
   conv_gather_kernel<<<grid, 256, 0, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy);
   ++launch_counter();
-  *launches += 1;
   return cudaGetLastError();
 }
 

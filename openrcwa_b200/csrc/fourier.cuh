@@ -36,7 +36,7 @@ struct ConvLaunch {
   int* info;           // device [njobs*max(...)]
 };
 
-cudaError_t conv_matrices(const ConvLaunch& L, cudaStream_t st, long long* launches);
+cudaError_t conv_matrices(const ConvLaunch& L, cudaStream_t st);
 
 // FourierSolver1D::solve on the device: Ff[M] from edges x[nxe], f[nxe-1].
 cudaError_t fourier1d_device(const double* x, int nxe, double d, const cplx* f, int M, cplx* Ff,

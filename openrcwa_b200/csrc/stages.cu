@@ -86,8 +86,7 @@ int conv_one(rcwa_engine* e, const double* cx, int ncx, const double* cy, int nc
   L.tyinv_ptrs = tp + 2 * (ncy - 1) + (ncx - 1);
   L.ipiv = dipiv.as<int>();
   L.info = dinfo.as<int>();
-  long long nl = 0;
-  if (conv_matrices(L, e->stream, &nl) != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess)
+  if (conv_matrices(L, e->stream) != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess)
     return set_err(e, RCWA_ERR_CUDA, "convolution kernels failed");
   return RCWA_OK;
 }
