@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--surrogate", action="store_true",
                     help="the learned-surrogate pipeline on a reduced cfg4 (Nx=Ny=5 solves): data generation, "
                          "GPU training, tensor-core inference, surrogate plus fallback with a 2%% audit")
+    ap.add_argument("--surrogate-nh", type=int, default=2,
+                    help="harmonics per axis of the surrogate's training solves (cfg4: 7)")
     ap.add_argument("--gemm-only", default=None, metavar="N,BATCH",
                     help="one batched n x n x n complex GEMM in 3xTF32 on tcgen05 and one on the FP64 path "
                          "(profiling aid)")
@@ -136,16 +138,18 @@ def run_uneven(args):
 
 
 def run_surrogate(args):
-    """cfg4's pipeline on a reduced grid (nH = 2, the 25 orders m, n in [-2, 2]
-    are then all the orders): 200k training solves by the FP64 engine, the
-    network (4 x 256 GELU) trained on the GPU, 65,536-query batches answered by
-    the network on the tensor cores and by the surrogate with fallback (2%
-    audit), against the FP64 solve of the same queries."""
+    """cfg4's pipeline: 200k training solves by the FP64 engine at nH
+    harmonics per axis (default 2, a reduced grid whose 25 orders m, n in
+    [-2, 2] are then all the orders; cfg4 itself is nH = 7, 225 orders), the
+    network (4 x 256 GELU) trained on the GPU on the efficiencies of the 25
+    lowest orders and the totals, 65,536-query batches answered by the network
+    on the tensor cores and by the surrogate with fallback (2% audit), against
+    the FP64 solve of the same queries."""
     import openrcwa_b200 as o
     from openrcwa_b200 import surrogate as sg
     eng = o.Engine(0)
     rng = np.random.default_rng(0)
-    nh = 2
+    nh = args.surrogate_nh
     t0 = time.perf_counter()
     P = sg.sample(200000, rng)
     Y = sg.solve(eng, P, nh, chunk=4096)
@@ -168,7 +172,9 @@ def run_surrogate(args):
     t_solve = time.perf_counter() - t0
     err = np.abs(r["Y"] - Ys)
     line = {"surrogate": {
-        "config": "reduced cfg4: one-rectangle 2D grating, Nx=Ny=5 solves, 11 parameters -> 52 efficiencies",
+        "config": "cfg4%s: one-rectangle 2D grating, nH=%d harmonics per axis (%d orders) per solve, 11 parameters "
+                  "-> 52 efficiencies (25 lowest orders, TE, and the totals)" % ("" if nh == 7 else " reduced", nh,
+                                                                                 (2 * nh + 1) ** 2),
         "train_solves": len(P), "generation_solves_per_s": len(P) / t_gen, "train_s": t_train,
         "final_train_mse": float(loss[-1]),
         "query_batch": len(Q), "network_queries_per_s": len(Q) / t_net,
