@@ -139,6 +139,49 @@ def fourier2d(cx, cy, f: np.ndarray, nx: int, ny: int, opt: int) -> np.ndarray:
     return Ff
 
 
+def circle_fourier2d(Lx: float, Ly: float, radius: float, center, eps1: complex, eps2: complex,
+                     nx: int, ny: int) -> np.ndarray:
+    """2D Fourier coefficients of a circular pillar (eps1 inside a disk of the
+    given radius and center, eps2 elsewhere) in the unit cell [0,Lx]x[0,Ly],
+    in the layout of the F2D table of FourierSolver2D's ContinuousXY branch
+    (rcwa/FourierSolver2D.cpp:250-349): F2D[m+nx-1, n+ny-1] =
+    (1/(Lx Ly)) * integral of eps(x,y) exp(-i 2pi (m x/Lx + n y/Ly)).
+
+    The reference has no analytic circle: its .orcwa driver staircases curved
+    shapes into rectangles, subdividing their bounding boxes into
+    N_CURVED_CELLS = 8 strips per curved axis (rcwa/RCWADriver.cpp:19-37).  This is the closed form of
+    the disk transform, integral over the disk of exp(-i G.r) =
+    exp(-i G.c) 2 pi R^2 J1(|G| R) / (|G| R) (pi R^2 at G = 0), the Laurent
+    rule for all three tensors of the circular-pillar layers."""
+    from scipy.special import j1
+    m = np.arange(-(nx - 1), nx)[:, None]
+    n = np.arange(-(ny - 1), ny)[None, :]
+    gx = 2 * PI * m / Lx
+    gy = 2 * PI * n / Ly
+    g = np.hypot(gx, gy)
+    gr = g * radius
+    with np.errstate(invalid="ignore", divide="ignore"):
+        airy = np.where(gr > 0, 2 * j1(gr) / np.where(gr > 0, gr, 1.0), 1.0)
+    disk = PI * radius * radius * airy * np.exp(-1j * (gx * center[0] + gy * center[1]))
+    F2D = (eps1 - eps2) * disk / (Lx * Ly)
+    F2D[nx - 1, ny - 1] += eps2
+    return F2D.astype(np.complex128)
+
+
+def circle_staircase(Lx: float, Ly: float, radius: float, center, eps1: complex, eps2: complex, cells: int):
+    """A staircase of a circular pillar on a uniform cells x cells grid (a cell
+    takes eps1 when its center lies in the disk), for convergence checks of
+    circle_fourier2d (the reference's .orcwa driver staircases circles on a
+    coarser, shape-aligned grid, rcwa/RCWADriver.cpp:19-37): returns the cell
+    edges cx, cy and the (cells x cells) permittivity grid, row = y."""
+    cx = np.linspace(0.0, Lx, cells + 1)
+    cy = np.linspace(0.0, Ly, cells + 1)
+    xm = 0.5 * (cx[1:] + cx[:-1])
+    ym = 0.5 * (cy[1:] + cy[:-1])
+    inside = (xm[None, :] - center[0]) ** 2 + (ym[:, None] - center[1]) ** 2 < radius * radius
+    return cx, cy, np.where(inside, eps1, eps2).astype(np.complex128)
+
+
 # --------------------------------------------------------------------------
 # Layer eigenproblem (rcwa/Layer.cpp:75-273, rcwa/WaveEquationSolver.cpp:8-37)
 # --------------------------------------------------------------------------

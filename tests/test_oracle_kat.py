@@ -148,3 +148,26 @@ def test_gamma_sqrt_branches():
     assert g[3].real > 0 and g[3].imag < 0          # 4th quadrant: principal root
     assert g[4].real < 0 and g[4].imag > 0          # 3rd quadrant: negated root
     assert g[5].real > 0 and g[5].imag > 0
+
+
+def test_circle_fourier_closed_form():
+    # analytic circular-pillar coefficients: exact mean, conjugate symmetry of
+    # a real profile, and convergence of uniform staircases towards them
+    import oracle.rcwa_oracle as ro
+    Lx, Ly, R, c = 4e-7, 5e-7, 1.3e-7, (2.1e-7, 2.4e-7)
+    e1, e2, nx, ny = 4.0, 1.0, 4, 3
+    F = ro.circle_fourier2d(Lx, Ly, R, c, e1, e2, nx, ny)
+    assert abs(F[nx - 1, ny - 1] - (e2 + (e1 - e2) * np.pi * R * R / (Lx * Ly))) < 1e-15
+    assert np.allclose(F, np.conj(F[::-1, ::-1]), atol=1e-15)
+    errs = []
+    for cells in (50, 200, 800):
+        cx, cy, eps = ro.circle_staircase(Lx, Ly, R, c, e1, e2, cells)
+        F2D = np.zeros_like(F)
+        for i in range(cells):
+            F2D += np.outer(ro.fourier1d(cx, Lx, eps[i, :], 2 * nx - 1),
+                            ro.fourier1d([cy[i], cy[i + 1]], Ly, [1.0], 2 * ny - 1))
+        errs.append(np.max(np.abs(F2D - F)) / (e1 - e2))
+    assert errs[2] < 1e-4 and errs[2] < errs[1] < errs[0]
+    # the block-Toeplitz convolution matrix of the Laurent rule
+    T = ro.block_toeplitz_dense(F)
+    assert T.shape == (nx * ny, nx * ny) and np.allclose(np.diag(T), F[nx - 1, ny - 1])
