@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--smatrix", default=None, metavar="N,BATCH",
                     help="the z-integrator entry points: BATCH slab S-matrices and star products of order N, "
                          "end to end with host buffers")
+    ap.add_argument("--conv-only", default=None, metavar="NH,POINTS",
+                    help="kernel (a) alone: one plan of POINTS points of the 2D pillar sweep at NH harmonics per "
+                         "axis, executed with stage timing; prints the convolution gather's time and HBM rate")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
                     help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
@@ -247,6 +250,40 @@ def run_smatrix(spec):
     return 0 if out["status_nonzero"] == 0 and out["finite"] else 1
 
 
+def conv_gather_bytes(stacks):
+    """Algorithmic bytes of the convolution gather: three N x N complex128
+    matrices written per distinct patterned layer (row a6 of the path)."""
+    return sum(3 * 16 * s.N * s.N * (s.eps.shape[0] - 2) for s in stacks)
+
+
+def run_conv_only(spec):
+    """Kernel (a), the convolution-matrix gather, on the pillar workload: one
+    plan of POINTS points (one stack, five patterned layers), executed three
+    times with stage timing; the gather's device time of the last execution
+    (CUDA events on the launching stream) and its rate against HBM."""
+    import openrcwa_b200 as o
+    from openrcwa_b200 import workloads
+    nh, npts = (int(x) for x in spec.split(","))
+    stacks, pts, pxy = workloads.pillars_2d(seed=0, nH=nh)
+    eng = o.Engine(0)
+    plan = eng.plan(stacks, pts[:npts], pxy[:npts])
+    plan.set_profiling(True)
+    for _ in range(3):
+        plan.execute()
+        st = plan.stage_times()
+    R, T, _, _, status = plan.results()
+    plan.close()
+    eng.close()
+    peaks, kind = measured_peaks()
+    b = conv_gather_bytes(stacks)
+    gbs = b / (st["conv_gather"] * 1e-3) / 1e9
+    print(json.dumps({"conv_only": {"nh": nh, "points": npts, "gather_ms": st["conv_gather"],
+                                    "tables_ms": st["conv_tables"], "bytes": b, "achieved_gbs": gbs,
+                                    "frac_hbm": gbs / peaks["hbm_gbs"], "peak_source": kind,
+                                    "status_max": int(status.max())}}))
+    return 0 if status.max() == 0 else 1
+
+
 def run_eig_only(spec):
     """One rcwa_zgeev_batched call on seeded random matrices (the kernels of the
     per-layer eigenproblem alone), for counter captures of those kernels."""
@@ -345,6 +382,31 @@ def fp64_gemm_peak_tflops(torch):
     return best
 
 
+def tf32_gemm_peak_tflops(torch):
+    """cuBLAS TF32 GEMM throughput (torch.matmul float32 with TF32 allowed,
+    8192^3, best of 5): the denominator of the 3xTF32 tensor-core products."""
+    n = 8192
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = True
+    a = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float32, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
 def eig_flops(n):
     """Algorithmic real flops of one complex eigen-decomposition with
     eigenvectors, split as in Golub & Van Loan (complex = 4x real counts):
@@ -353,23 +415,31 @@ def eig_flops(n):
     return {"hessenberg": 18.67 * n ** 3, "schur_qr": 81.33 * n ** 3, "total": 100.0 * n ** 3}
 
 
-def cpu_solve_sample(stacks, pts, pxy, count):
-    """Time `count` solves of the oracle on the host (all BLAS threads)."""
+def cpu_solve_sample(stacks, pts, pxy, count, threads=None):
+    """Time `count` solves of the oracle on the host (all BLAS threads, or
+    `threads`).  Returns (seconds, per point: (R, T, REF, TRN) of its
+    polarisations)."""
     import oracle.rcwa_oracle as orc
+    from threadpoolctl import threadpool_limits
     st = stacks[0]
-    t0 = time.perf_counter()
-    for p in range(count):
-        _, lam, kx0, ky0 = pts[p]
-        s = orc.RCWASolver(st.nHx, st.nHy)
-        for l in range(st.eps.shape[0]):
-            s.addLayer(orc.OracleLayer(st.cx, st.cy, st.eps[l]))
-        s.setBlochWavevector(kx0, ky0)
-        s.solve(lam, list(range(st.eps.shape[0])), list(st.thickness))
-        k0 = 2 * np.pi / lam
-        for e in range(pxy.shape[1]):
-            c = s.generateHorizontalPlaneWave(pxy[p, e, 0], pxy[p, e, 1], 0)
-            s.scatterPlaneWave(c, 0, st.eps.shape[0] - 1, k0)
-    return time.perf_counter() - t0
+    out = []
+    with threadpool_limits(limits=threads):
+        t0 = time.perf_counter()
+        for p in range(count):
+            _, lam, kx0, ky0 = pts[p]
+            s = orc.RCWASolver(st.nHx, st.nHy)
+            for l in range(st.eps.shape[0]):
+                s.addLayer(orc.OracleLayer(st.cx, st.cy, st.eps[l]))
+            s.setBlochWavevector(kx0, ky0)
+            s.solve(lam, list(range(st.eps.shape[0])), list(st.thickness))
+            k0 = 2 * np.pi / lam
+            r = []
+            for e in range(pxy.shape[1]):
+                c = s.generateHorizontalPlaneWave(pxy[p, e, 0], pxy[p, e, 1], 0)
+                r.append(s.scatterPlaneWave(c, 0, st.eps.shape[0] - 1, k0))
+            out.append((np.array([a.sum() for a, _ in r]), np.array([b.sum() for _, b in r]),
+                        np.array([a for a, _ in r]), np.array([b for _, b in r])))
+        return time.perf_counter() - t0, out
 
 
 def run_reference(args):
@@ -382,7 +452,7 @@ def run_reference(args):
         cpu_solve_sample(stacks, pts, pxy, 1)
     tt = 0.0
     for k in range(args.steps):
-        tt += cpu_solve_sample(stacks, pts[k:], pxy[k:], 1)
+        tt += cpu_solve_sample(stacks, pts[k:], pxy[k:], 1)[0]
     value = args.steps / tt
     cores = os.cpu_count()
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
@@ -401,6 +471,8 @@ def main():
     args = parse()
     if args.eig_only:
         return run_eig_only(args.eig_only)
+    if args.conv_only:
+        return run_conv_only(args.conv_only)
     if args.gemm_only:
         return run_gemm_only(args.gemm_only)
     if args.smatrix:
@@ -450,6 +522,7 @@ def main():
     bpts, bpxy = workloads.batch_slice(pts, pxy, workloads.shard_start(rank, world, B, 0), B)
     stream = torch.cuda.Stream()
     fp64_peak = fp64_gemm_peak_tflops(torch)
+    tf32_peak = tf32_gemm_peak_tflops(torch)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
 
@@ -458,7 +531,10 @@ def main():
         batch on `stream` (CUDA events, max over ranks).  Stage-timing events
         are on from the start: the second execution captures the launch
         sequence (with its event records) into the CUDA graph that every later
-        execution launches."""
+        execution launches.  The stage times of each execution are read
+        before the next one starts (a host wait on the last stage event
+        inside the timed region): consecutive graph launches therefore do not
+        overlap, which leaves the measured rate slightly pessimistic."""
         tc0 = time.perf_counter()
         plan = eng.plan(stacks, bpts, bpxy, precision=precision)
         plan_info[precision] = {"plan_create_s": time.perf_counter() - tc0, "schedule": plan.schedule()}
@@ -565,14 +641,24 @@ def main():
     n_iface = stacks[0].eps.shape[0] - 1
     tc_ms = per_launch.get("cascade_gemm", 0.0)
     tc_flops = 3 * 4 * 8.0 * n ** 3 * n_iface * B
-    tf32_peak = peaks.get("bf16_tflops", 0.0) / 2 if peaks.get("bf16_tflops") else None
     tensor_gemm = None
     if tc_ms > 0:
         ach = tc_flops / (tc_ms * 1e-3) / 1e12
         tensor_gemm = {"kernel": "zgemm_tf32x3 (tcgen05 kind::tf32)", "bound": "tensor", "achieved": ach,
                        "peak": tf32_peak, "unit": "TFLOP/s", "frac": ach / tf32_peak if tf32_peak else None,
-                       "peak_source": "half the measured dense BF16 rate (TF32 runs at half the BF16 rate)",
+                       "peak_source": "cuBLAS TF32 GEMM measured in this run (torch.matmul float32, TF32 on)",
                        "flops_per_step": tc_flops, "ms_per_step": tc_ms}
+    conv_ms = per_launch.get("conv_gather", 0.0)
+    conv_roof = None
+    if conv_ms > 0:
+        cb = conv_gather_bytes(stacks)
+        ach = cb / (conv_ms * 1e-3) / 1e9
+        conv_roof = {"kernel": "conv_gather_kernel (row a6, block-Toeplitz gather)", "bound": "hbm",
+                     "achieved": ach, "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                     "frac": ach / peaks["hbm_gbs"] if peaks.get("hbm_gbs") else None,
+                     "bytes_per_launch": cb, "ms_per_launch": conv_ms,
+                     "note": "three N x N complex128 matrices written per distinct patterned layer; the sweep "
+                             "shares one stack, so one launch per step"}
     line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128 with tf32x3 cascade products", "data": "synthetic",
@@ -586,6 +672,7 @@ def main():
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d // args.steps,
                     "d2h_bytes_per_step": d2h // args.steps},
             "gpu_launches": launches, "clocks": clk, "roofline": roof, "tensor_gemm": tensor_gemm,
+            "conv_gather": conv_roof,
             "plain_fp64": {"value": value64, "unit": "solves/s", "ms_per_step": t64_ms / args.steps,
                            "stage_ms_per_step": {k: v / args.steps for k, v in stage64_ms.items()}},
             "mixed_error": {"max_abs_dRT_vs_fp64": dRT, "max_abs_dorder_vs_fp64": dorders, "bound": 1e-4,
@@ -595,12 +682,30 @@ def main():
             "tuning": {"mode": args.tuning,
                        "plan_create_s": plan_info[o.RCWA_PREC_MIXED]["plan_create_s"],
                        "entries": tuner.entries() if tuner is not None else []},
-            "stage_ms_per_step": per_launch, "peaks": {"fp64_dgemm_tflops": fp64_peak,
+            "stage_ms_per_step": per_launch, "peaks": {"fp64_dgemm_tflops": fp64_peak, "tf32_gemm_tflops": tf32_peak,
                                                        "hbm_gbs": peaks.get("hbm_gbs"), "source": peak_kind}}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        tcpu = cpu_solve_sample(stacks, pts, pxy, 1)
+        # the oracle on points 0 and 1 of the timed batch: the CPU baseline
+        # (all host threads, then one thread as in the reference's serial
+        # frequency loop), and the error of both engines against it
+        tcpu, ref_pts = cpu_solve_sample(stacks, bpts, bpxy, 1)
+        t1, ref1 = cpu_solve_sample(stacks, bpts[1:], bpxy[1:], 1, threads=1)
         line["cpu_baseline"] = {"value": 1.0 / tcpu, "unit": "solves/s", "cores": os.cpu_count(), "kind": "port",
-                                "sample": "1 solve (point 0) of the sweep through the NumPy oracle, all BLAS threads"}
+                                "sample": "1 solve (point 0 of the timed batch) through the NumPy oracle "
+                                          "(LAPACK zgeev path), all host BLAS threads",
+                                "single_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1,
+                                                  "sample": "point 1 of the timed batch, one BLAS thread"}}
+        N_ = stacks[0].N
+        errs = {"mixed": 0.0, "fp64": 0.0}
+        for k, (Ro, To, REFo, TRNo) in ((0, ref_pts[0]), (1, ref1[0])):
+            for name, res in (("mixed", res_mixed), ("fp64", res_fp64)):
+                R_, T_, REF_, TRN_ = res
+                ords = np.abs(REF_.reshape(B, -1, N_)[k] - REFo).max(), np.abs(TRN_.reshape(B, -1, N_)[k] - TRNo).max()
+                errs[name] = max(errs[name], float(np.abs(R_[k] - Ro).max()), float(np.abs(T_[k] - To).max()),
+                                 float(max(ords)))
+        line["mixed_error"]["max_abs_vs_oracle"] = errs["mixed"]
+        line["mixed_error"]["fp64_max_abs_vs_oracle"] = errs["fp64"]
+        line["mixed_error"]["oracle_points"] = "points 0 and 1 of the timed batch, every R, T and per-order value"
     if rank == 0:
         print(json.dumps(line), flush=True)
     eng.close()

@@ -10,10 +10,13 @@
 // uniform half-spaces is the identity here, so the amplitude vector c of
 // generateHorizontalPlaneWave is [px delta; py delta].
 //
+// Tdd() and Rud() copy the solved scattering matrices from the device on
+// first access after solve().
+//
 // Outside this engine (they report on std::cerr and leave outputs empty):
 // PML (enablePML), layer translations, magnetic layers, non-uniform
-// half-spaces, incident vectors other than generateHorizontalPlaneWave's, the
-// field images (saveFieldImage, saveDeviceImage) and host copies of Tdd/Rud.
+// half-spaces, incident vectors other than generateHorizontalPlaneWave's and
+// the field images (saveFieldImage, saveDeviceImage).
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -146,9 +149,10 @@ class RCWASolver {
     }
   }
 
-  // Not materialised on the host by this engine.
-  const Eigen::MatrixXcs& Tdd() const { return empty_; }
-  const Eigen::MatrixXcs& Rud() const { return empty_; }
+  // rcwa/RCWASolver.h:141-142: the cascade's final Tdd_ and Rud_ (empty
+  // before a successful solve), downloaded once per solve
+  const Eigen::MatrixXcs& Tdd() const { fetch(); return tdd_; }
+  const Eigen::MatrixXcs& Rud() const { fetch(); return rud_; }
 
   template <class... A>
   void saveFieldImage(A&&...) { std::cerr << "[rcwa_b200] saveFieldImage is not provided by this engine\n"; }
@@ -173,6 +177,28 @@ class RCWASolver {
   void release() {
     if (plan_) rcwa_plan_destroy(plan_);
     plan_ = nullptr;
+    fetched_ = false;
+    tdd_.resize(0, 0);
+    rud_.resize(0, 0);
+  }
+  void fetch() const {
+    if (fetched_ || !plan_ || stack_.empty()) return;
+    fetched_ = true;
+    const int n = 2 * nx_ * ny_;
+    std::vector<rcwa_cplx> r((size_t)n * n), t((size_t)n * n);
+    const int rc = rcwa_plan_smatrix(plan_, 0, r.data(), t.data());
+    if (rc != RCWA_OK) {
+      std::cerr << "[rcwa_b200] Tdd/Rud: " << rcwa_status_string(rc) << "\n";
+      return;
+    }
+    rud_.resize(n, n);
+    tdd_.resize(n, n);
+    for (int i = 0; i < n; ++i)
+      for (int j = 0; j < n; ++j) {
+        const rcwa_cplx a = r[(size_t)i * n + j], b = t[(size_t)i * n + j];
+        rud_(i, j) = scalex(a.re, a.im);
+        tdd_(i, j) = scalex(b.re, b.im);
+      }
   }
 
   int nx_, ny_, nX_, nY_;
@@ -183,5 +209,6 @@ class RCWASolver {
   std::vector<double> cx_, cy_, thick_;
   std::vector<rcwa_cplx> eps_;
   rcwa_plan* plan_ = nullptr;
-  Eigen::MatrixXcs empty_;
+  mutable bool fetched_ = false;
+  mutable Eigen::MatrixXcs tdd_, rud_;
 };

@@ -133,6 +133,17 @@ int rcwa_plan_results(rcwa_plan* p, double* R, double* T,
  * rcwa_plan_results. */
 int rcwa_plan_rescatter(rcwa_plan* p, const rcwa_cplx* pxy);
 
+/* The scattering matrix of one point of an executed plan, as the
+ * RCWASolver::Tdd() / Rud() accessors return it (rcwa/RCWASolver.h:141-142;
+ * the RTCM cascade's final Tdd_ and Rud_, rcwa/RCWASolver.cpp:378-492, in the
+ * modal basis of the uniform half-spaces, W = I):
+ *   Rud, Tdd  NULL or host [n*n] row-major complex, n = 2*N of the point's
+ *             stack (either may be NULL)
+ * Waits for the plan's work.  Plans whose points needed more than one
+ * device-memory chunk return RCWA_ERR_UNSUPPORTED (the engine reuses the
+ * workspace chunk by chunk); a point index out of range RCWA_ERR_INVALID. */
+int rcwa_plan_smatrix(rcwa_plan* p, int point, rcwa_cplx* Rud, rcwa_cplx* Tdd);
+
 /* Number of engine kernel launches the last plan_execute enqueued. */
 long long rcwa_plan_launch_count(const rcwa_plan* p);
 /* Schedules the plan uses, per chunk: sched[6] = {matrix order n, points,
@@ -182,6 +193,14 @@ int rcwa_layer_solve(rcwa_engine* e, const double* cx, int ncx, const double* cy
  * VR[batch][n*n] row-major (columns unit 2-norm), info[batch]. */
 int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
                        rcwa_cplx* w, rcwa_cplx* VR, int* info);
+
+/* Failure-injection hook for tests of the RCWA_ERR_NOCONV path (no
+ * counterpart in the reference, whose LAPACK zgeev has a fixed iteration
+ * limit, rcwa/MKLEigenSolver.hpp:131): caps the QR sweeps of every later
+ * eigensolve at `sweeps` (0 restores the built-in budget of 30*max(10, n)).
+ * Process-wide; a plan captured into a CUDA graph keeps the cap that was set
+ * when it was captured.  Returns RCWA_ERR_INVALID for a negative cap. */
+int rcwa_set_qr_sweep_limit(int sweeps);
 
 /* Batched complex GEMM D = alpha*A*B + beta*C (row-major, host buffers
  * [batch][M*K], [batch][K*N], [batch][M*N]; C may be NULL when beta = 0), the
@@ -305,9 +324,13 @@ int rcwa_star_product_batched(rcwa_engine* e, int n, int batch,
  * Limits: n <= RCWA_NOALLOC_MAX_N and batch <= RCWA_NOALLOC_MAX_BATCH, else
  * RCWA_ERR_UNSUPPORTED.  The first call on a device looks up the scratch
  * array's device address (cudaGetSymbolAddress) with that device current;
- * make that first call before any stream capture.  All calls share the one
- * scratch array, so calls whose work overlaps on the GPU (other streams,
- * other threads) race: serialise them. */
+ * under CUDA's lazy module loading (the default since CUDA 12.2) that lookup
+ * is also when the driver reserves the array, so make the first call at
+ * set-up time, before any stream capture; later calls reserve nothing.  A
+ * CUDA error already pending on the calling thread is reported as
+ * RCWA_ERR_CUDA and left pending.  All calls share the one scratch array, so
+ * calls whose work overlaps on the GPU (other streams, other threads) race:
+ * serialise them. */
 #define RCWA_NOALLOC_MAX_N 64
 #define RCWA_NOALLOC_MAX_BATCH 64
 int rcwa_zgeev_batched_noalloc(int n, int batch, rcwa_cplx* A, rcwa_cplx* w,

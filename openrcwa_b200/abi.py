@@ -46,6 +46,7 @@ EXPORTS = [
     "rcwa_plan_schedule", "rcwa_tuner_create", "rcwa_tuner_destroy", "rcwa_tuner_set_sms", "rcwa_tuner_candidates",
     "rcwa_tuner_default", "rcwa_tuner_set", "rcwa_tuner_get", "rcwa_tuner_count", "rcwa_tuner_entry",
     "rcwa_tuner_save", "rcwa_tuner_load", "rcwa_engine_set_tuner", "rcwa_tuner_measure",
+    "rcwa_set_qr_sweep_limit", "rcwa_plan_smatrix",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -158,8 +159,18 @@ def load() -> C.CDLL:
     lib.rcwa_tuner_load.argtypes = [C.c_void_p, C.c_char_p]
     lib.rcwa_engine_set_tuner.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.rcwa_tuner_measure.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, _IP, _DP]
+    lib.rcwa_set_qr_sweep_limit.argtypes = [C.c_int]
+    lib.rcwa_plan_smatrix.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
+
+
+def set_qr_sweep_limit(sweeps: int) -> None:
+    """Cap the QR sweeps of every later eigensolve (0: the built-in budget);
+    the failure-injection hook of the RCWA_ERR_NOCONV path."""
+    rc = load().rcwa_set_qr_sweep_limit(int(sweeps))
+    if rc:
+        raise RcwaError(rc, "set_qr_sweep_limit")
 
 
 def _d(a):
@@ -440,6 +451,15 @@ class Plan:
         """New incident polarisations (n_pts, n_exc, 2) on the kept S-matrices."""
         pxy = np.ascontiguousarray(pxy, dtype=np.complex128).reshape(self.n_pts, self.n_exc, 2)
         self.eng._check(self.eng.lib.rcwa_plan_rescatter(self.h, _v(pxy)), "plan_rescatter")
+
+    def smatrix(self, point):
+        """(Rud, Tdd) of an executed single-chunk plan's point: the
+        RCWASolver::Rud() / Tdd() matrices (rcwa/RCWASolver.h:141-142)."""
+        n = 2 * self.Ns[point]
+        Rud = np.zeros((n, n), dtype=np.complex128)
+        Tdd = np.zeros((n, n), dtype=np.complex128)
+        self.eng._check(self.eng.lib.rcwa_plan_smatrix(self.h, int(point), _v(Rud), _v(Tdd)), "plan_smatrix")
+        return Rud, Tdd
 
     def set_profiling(self, on=True):
         self.eng._check(self.eng.lib.rcwa_plan_set_profiling(self.h, 1 if on else 0), "set_profiling")

@@ -6,6 +6,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <mutex>
+
 #include "../../include/rcwa_b200.h"
 
 typedef double2 cplx;
@@ -79,6 +81,26 @@ inline long long& launch_counter() {
   static thread_local long long count = 0;
   return count;
 }
+
+// Raises a kernel's dynamic shared-memory limit once per device (the
+// attribute is held per device and per kernel).  Several host threads may make
+// their first launch at the same time, so the per-device flags sit behind a
+// mutex; later calls only take the uncontended lock.
+struct SmemAttrOnce {
+  std::mutex mu;
+  bool done[64] = {};
+  template <class Kernel>
+  cudaError_t ensure(Kernel kernel, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+    e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+    return e;
+  }
+};
 
 // Host-side launch check used by the engine.
 #define RCWA_CUDA_TRY(expr)                                   \

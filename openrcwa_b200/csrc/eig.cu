@@ -10,6 +10,8 @@
 //      back-transformed with Z by the tile GEMM and normalised to unit 2-norm.
 // This replaces LAPACK zgeev('N','V') behind MKLEigenSolver
 // (rcwa/MKLEigenSolver.hpp:102-179).  Balancing is not applied.
+#include <atomic>
+
 #include "eig.cuh"
 #include "linalg.cuh"
 #include "tile.cuh"
@@ -535,12 +537,12 @@ __device__ void qr_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, cplx sh
 
 // Returns 0 or RCWA_ERR_NOCONV.
 __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], double* rc, cplx* rs,
-                     int* redi) {
+                     int* redi, int sweep_cap) {
   const double ulp = 2.0 * RCWA_DBL_EPS;
   const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
   int i = n - 1;
   long long total = 0;
-  const long long itmax_total = 30LL * max(10, n);
+  const long long itmax_total = sweep_cap > 0 ? min(30LL * max(10, n), (long long)sweep_cap) : 30LL * max(10, n);
   while (i >= 0) {
     int l = 0;
     bool conv = false;
@@ -580,27 +582,23 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
 // held in shared memory, all bulges of one chain step in parallel (their row
 // pairs and column pairs are disjoint).  Every rotation is logged; after a
 // window pass the log is applied to the rest of T (the rows right of the
-// window, the columns above it) and to Z by the warps, each streaming a
-// 32-column (or 32-row) tile through shared memory bulge by bulge, so an
-// element of T or Z crosses DRAM once per pass instead of once per rotation.
+// window, the columns above it) and to Z, one line of 32 per warp task, with
+// the part of each line the chain spans held in registers (replay_frame), so
+// an element of T or Z crosses memory once per pass instead of once per
+// rotation.
 constexpr int kMsW = 64;           // window order
 constexpr int kMsShifts = 10;      // bulges per sweep
 constexpr int kMsMin = kSchurCrossover;  // smallest crossover: the chase window needs 64 rows
-constexpr int kMsThreads = 192;    // six warps
-constexpr int kMsTileElems = 2112 + 66; // 66 rows x 33 (row tasks) or 32 rows x 67 (column tasks)
+constexpr int kMsThreads = 256;    // eight warps
 constexpr int kMsLog = kMsW + 1;         // rotation log per bulge; slot kMsW holds the identity
 constexpr int kMsMaxSteps = kMsW + 3 * kMsShifts;  // chain steps of one window pass
-constexpr int kMsColPitch = 67;          // column-task tile row pitch (conflict-free 16-byte accesses)
-constexpr int kMsDummy = kMsW;           // tile row / column pair that absorbs inactive bulges
-// replay table entry: tile row (bits 0-7), log slot (8-15), first (16) and last (17) rotation of the bulge
-constexpr int kRepFirst = 1 << 16, kRepLast = 1 << 17;
 
 struct MsSmem {
-  cplx* Wt;      // [kMsW][kMsW + 1]
-  cplx* tiles;   // [kMsThreads / 32][kMsTileElems]
+  cplx* Wt;      // [kMsW][kMsW + 1]  the chase window
+  cplx* work;    // early deflation's window, vectors and reflector; the small shift problem
   double* lc;    // [kMsShifts][kMsLog]  rotation cosines, bulge-major
   cplx* ls;      // [kMsShifts][kMsLog]  rotation sines
-  int* ix;       // [kMsMaxSteps][kMsShifts]  replay table per chain step and bulge
+  int* ix;       // [kMsMaxSteps][kMsShifts]  log slot per chain step and bulge
   int* firstp;   // [kMsShifts] first rotation position of each bulge in the pass
   int* cnt;      // [kMsShifts] rotations of each bulge in the pass
   int* tfirst;   // [kMsShifts] pass step of each bulge's first rotation
@@ -609,21 +607,19 @@ struct MsSmem {
   int* aed;      // [4] early-deflation results: converged flag, undeflated count, shift count
 };
 
-// the window is only used by the in-window chase and the tiles only by the
-// replay that follows it, so the two share one region
-constexpr size_t kMsRegion = sizeof(cplx) * kMsW * (kMsW + 1) > sizeof(cplx) * (kMsThreads / 32) * kMsTileElems
-                                 ? sizeof(cplx) * kMsW * (kMsW + 1)
-                                 : sizeof(cplx) * (kMsThreads / 32) * kMsTileElems;
+// the window is only used by the chase, the work area only by the early
+// deflation and the shift computation between sweeps: they share one region
+constexpr size_t kMsRegion = sizeof(cplx) * kMsW * (kMsW + 1);
 constexpr size_t kMsSmemBytes = kMsRegion +
                                 sizeof(double) * kMsShifts * kMsLog + sizeof(cplx) * kMsShifts * kMsLog +
                                 sizeof(int) * kMsMaxSteps * kMsShifts + sizeof(int) * 3 * kMsShifts +
-                                sizeof(cplx) * kMsShifts + sizeof(int) * 12;
+                                sizeof(cplx) * kMsShifts + sizeof(int) * (kMsThreads / 32 + 4);
 static_assert(kMsSmemBytes <= 232448, "multishift shared memory exceeds the per-block limit");
 
 __device__ MsSmem carve_ms_smem(unsigned char* base) {
   MsSmem sm;
   sm.Wt = (cplx*)base;
-  sm.tiles = (cplx*)base;
+  sm.work = (cplx*)base;
   sm.ls = (cplx*)(base + kMsRegion);
   sm.shifts = sm.ls + kMsShifts * kMsLog;
   sm.lc = (double*)(sm.shifts + kMsShifts);
@@ -704,6 +700,9 @@ __device__ void small_eigs_warp(cplx* B, int ldb, int s, cplx* out) {
 constexpr int kAedW = 32;        // window order (one lane per column)
 constexpr int kAedLd = kAedW + 1;
 constexpr int kAedNibble = 14;   // percent of the window deflated that skips the sweep
+static_assert(sizeof(cplx) * (2 * kAedW * kAedLd + kAedW) <= kMsRegion &&
+                  sizeof(cplx) * kMsShifts * (kMsShifts + 1) <= kMsRegion,
+              "the early-deflation work area must fit in the chase window's region");
 
 #define AW(r, c) W[(r) * kAedLd + (c)]
 #define AV(r, c) V[(r) * kAedLd + (c)]
@@ -859,7 +858,7 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int nw = kAedW;
   const int kw = i - nw + 1;
-  cplx* W = sm.tiles;
+  cplx* W = sm.work;
   cplx* V = W + kAedW * kAedLd;
   cplx* hv = V + kAedW * kAedLd;
   const double ulp = 2.0 * RCWA_DBL_EPS;
@@ -979,6 +978,80 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
 #undef AW
 #undef AV
 
+// Off-window update of one window pass for one lane: the rotations of every
+// bulge, in chain order, on one line of T or Z (a column of T right of the
+// window, a row of T above it, a row of Z), read and written through
+// base + r * stride for index r in [rlo, rhi].  At pass step sg bulge b acts
+// on the pair (p, p+1), p = top0 + sg + 3 (kMsShifts - 1 - b), so the chain
+// spans kMsFrame consecutive indices that slide by one per step.  That span
+// is held in registers: each step loads the index entering at the bottom
+// (kMsPre steps ahead), applies the kMsShifts rotations in registers and
+// stores the index leaving at the top, so every element crosses memory once
+// per pass and the rotations run from registers, not shared memory.
+// Rows: [x; y] <- [c x + s y; -conj(s) x + c y]; columns: the conjugate
+// transpose [c x + conj(s) y; -s x + c y].
+constexpr int kMsFrame = 3 * (kMsShifts - 1) + 2;
+constexpr int kMsPre = 4;
+
+template <bool kRows>
+__device__ __forceinline__ void replay_frame(cplx* base, size_t stride, int top0, int nsteps, int rlo, int rhi,
+                                             const MsSmem& sm) {
+  cplx f[kMsFrame];
+#pragma unroll
+  for (int k = 0; k < kMsFrame - 1; ++k) {
+    const int r = top0 + k;
+    f[k] = (r >= rlo && r <= rhi) ? base[(size_t)r * stride] : mkc(0.0, 0.0);
+  }
+  f[kMsFrame - 1] = mkc(0.0, 0.0);
+  cplx pre[kMsPre];
+#pragma unroll
+  for (int d = 0; d < kMsPre; ++d) {
+    const int r = top0 + d + kMsFrame - 1;
+    pre[d] = (d < nsteps && r >= rlo && r <= rhi) ? base[(size_t)r * stride] : mkc(0.0, 0.0);
+  }
+  for (int sg0 = 0; sg0 < nsteps; sg0 += kMsPre) {
+    cplx cur[kMsPre];
+#pragma unroll
+    for (int d = 0; d < kMsPre; ++d) {
+      cur[d] = pre[d];
+      const int sg = sg0 + kMsPre + d, r = top0 + sg + kMsFrame - 1;
+      pre[d] = (sg < nsteps && r >= rlo && r <= rhi) ? base[(size_t)r * stride] : mkc(0.0, 0.0);
+    }
+#pragma unroll
+    for (int d = 0; d < kMsPre; ++d) {
+      const int sg = sg0 + d;
+      if (sg < nsteps) {
+        f[kMsFrame - 1] = cur[d];
+        const int* e = sm.ix + sg * kMsShifts;
+#pragma unroll
+        for (int b = 0; b < kMsShifts; ++b) {
+          const int slot = e[b];
+          const double c = sm.lc[b * kMsLog + slot];
+          const cplx sn = sm.ls[b * kMsLog + slot];
+          const int kb = 3 * (kMsShifts - 1 - b);
+          const cplx x = f[kb], y = f[kb + 1];
+          if (kRows) {
+            f[kb] = cfma(sn, y, cscale(x, c));
+            f[kb + 1] = cfma(cneg(cconj(sn)), x, cscale(y, c));
+          } else {
+            f[kb] = cfma(cconj(sn), y, cscale(x, c));
+            f[kb + 1] = cfma(cneg(sn), x, cscale(y, c));
+          }
+        }
+        const int rt = top0 + sg;
+        if (rt >= rlo && rt <= rhi) base[(size_t)rt * stride] = f[0];
+#pragma unroll
+        for (int k = 0; k < kMsFrame - 1; ++k) f[k] = f[k + 1];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kMsFrame - 1; ++k) {
+    const int r = top0 + nsteps + k;
+    if (r >= rlo && r <= rhi) base[(size_t)r * stride] = f[k];
+  }
+}
+
 // One multishift sweep over the active block [l, i] with sm.shifts[0..s).
 // Bulge b sits at position p = l + t - 3b at chain step t; it is active while
 // l <= p <= i-1 and its rotation acts on rows/columns (p, p+1).
@@ -1071,125 +1144,35 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
     int rlo = i + 1, rhi = -1;
     for (int b = 0; b < s; ++b)
       if (sm.cnt[b] > 0) { rlo = min(rlo, sm.firstp[b]); rhi = max(rhi, sm.firstp[b] + sm.cnt[b]); }
-    const int nr = rhi - rlo + 1;
     const int nsteps = t1 - t;
-    // replay table per chain step and bulge: the tile row of the bulge's row
-    // pair, its log slot and whether the rotation is its first or last in the
-    // pass; inactive bulges rotate the dummy pair by the identity slot, so the
+    // replay table per chain step and bulge: the log slot of the bulge's
+    // rotation at that step (the identity slot while it is inactive), so the
     // chains interleave without branches
     for (int idx = tid; idx < nsteps * kMsShifts; idx += nthr) {
       const int sg = idx / kMsShifts, b = idx % kMsShifts;
-      int v = kMsDummy | (kMsW << 8);
+      int slot = kMsW;
       if (b < s) {
-        const int k = sg - sm.tfirst[b], cnt = sm.cnt[b];
-        if (k >= 0 && k < cnt)
-          v = (sm.firstp[b] - rlo + k) | (k << 8) | (k == 0 ? kRepFirst : 0) | (k == cnt - 1 ? kRepLast : 0);
+        const int k = sg - sm.tfirst[b];
+        if (k >= 0 && k < sm.cnt[b]) slot = k;
       }
-      sm.ix[idx] = v;
+      sm.ix[idx] = slot;
     }
     __syncthreads();
+    const int top0 = l + t - 3 * (kMsShifts - 1);
     const int nR = (n - 1 - we + 31) / 32, nU = (ws + 31) / 32, nZ = (n + 31) / 32;
-    cplx* tile = sm.tiles + warp * kMsTileElems;
     for (int task = warp; task < nR + nU + nZ; task += nwarp) {
       if (task < nR) {
-        // T(rlo..rhi, j): row rotations, lane = column, chain order
+        // T(rlo..rhi, j), j right of the window: row rotations, lane = column
         const int j = we + 1 + 32 * task + lane;
-#ifdef RCWA_EIG_STATS
-        long long q0c = clock64();
-#endif
-        if (j < n) {
-          for (int r = 0; r < nr; ++r) cp_async16(&tile[r * 33 + lane], &T[(size_t)(rlo + r) * ldt + j]);
-          cp_async_wait_all();
-#ifdef RCWA_EIG_STATS
-          if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[5], (unsigned long long)(q1c - q0c)); q0c = q1c; }
-#endif
-          cplx xc[kMsShifts];
-#pragma unroll
-          for (int b = 0; b < kMsShifts; ++b) xc[b] = mkc(0.0, 0.0);
-          for (int sg = 0; sg < nsteps; ++sg) {
-            const int* e = sm.ix + sg * kMsShifts;
-            int v[kMsShifts];
-            cplx* px[kMsShifts];
-            cplx x[kMsShifts], y[kMsShifts], sn[kMsShifts];
-            double c[kMsShifts];
-#pragma unroll
-            for (int b = 0; b < kMsShifts; ++b) {
-              v[b] = e[b];
-              const int k = (v[b] >> 8) & 0xff;
-              px[b] = tile + (v[b] & 0xff) * 33 + lane;
-              c[b] = sm.lc[b * kMsLog + k];
-              sn[b] = sm.ls[b * kMsLog + k];
-              y[b] = px[b][33];
-              x[b] = (v[b] & kRepFirst) ? px[b][0] : xc[b];
-            }
-#pragma unroll
-            for (int b = 0; b < kMsShifts; ++b) {
-              px[b][0] = cfma(sn[b], y[b], cscale(x[b], c[b]));
-              xc[b] = cfma(cneg(cconj(sn[b])), x[b], cscale(y[b], c[b]));
-              if (v[b] & kRepLast) px[b][33] = xc[b];
-            }
-          }
-#ifdef RCWA_EIG_STATS
-          if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[6], (unsigned long long)(q1c - q0c)); q0c = q1c; }
-#endif
-          for (int r = 0; r < nr; ++r) T[(size_t)(rlo + r) * ldt + j] = tile[r * 33 + lane];
-#ifdef RCWA_EIG_STATS
-          if (lane == 0 && warp == 0) { long long q1c = clock64(); atomicAdd(&g_eig_stats[7], (unsigned long long)(q1c - q0c)); }
-#endif
-        }
+        if (j < n) replay_frame<true>(T + j, (size_t)ldt, top0, nsteps, rlo, rhi, sm);
+      } else if (task < nR + nU) {
+        // T(r, rlo..rhi), r above the window: column rotations, lane = row
+        const int r = 32 * (task - nR) + lane;
+        if (r < ws) replay_frame<false>(T + (size_t)r * ldt, (size_t)1, top0, nsteps, rlo, rhi, sm);
       } else {
-        // column rotations on T(rows above the window, rlo..rhi) or Z(:, rlo..rhi); lane = row
-        const bool isZ = task >= nR + nU;
-        const int r0 = 32 * (isZ ? task - nR - nU : task - nR);
-        const int rows = isZ ? n : ws;
-        if (!isZ) {
-          for (int rr = 0; rr < 32 && r0 + rr < rows; ++rr)
-            for (int c = lane; c < nr; c += 32)
-              cp_async16(&tile[rr * kMsColPitch + c], &T[(size_t)(r0 + rr) * ldt + rlo + c]);
-        } else {
-          if (r0 + lane < rows)
-            for (int c = 0; c < nr; ++c) cp_async16(&tile[lane * kMsColPitch + c], &Z[(size_t)(rlo + c) * n + r0 + lane]);
-        }
-        cp_async_wait_all();
-        __syncwarp();
-        if (r0 + lane < rows) {
-          cplx* row = tile + lane * kMsColPitch;
-          cplx xc[kMsShifts];
-#pragma unroll
-          for (int b = 0; b < kMsShifts; ++b) xc[b] = mkc(0.0, 0.0);
-          for (int sg = 0; sg < nsteps; ++sg) {
-            const int* e = sm.ix + sg * kMsShifts;
-            int v[kMsShifts];
-            cplx* px[kMsShifts];
-            cplx x[kMsShifts], y[kMsShifts], sn[kMsShifts];
-            double c[kMsShifts];
-#pragma unroll
-            for (int b = 0; b < kMsShifts; ++b) {
-              v[b] = e[b];
-              const int k = (v[b] >> 8) & 0xff;
-              px[b] = row + (v[b] & 0xff);
-              c[b] = sm.lc[b * kMsLog + k];
-              sn[b] = sm.ls[b * kMsLog + k];
-              y[b] = px[b][1];
-              x[b] = (v[b] & kRepFirst) ? px[b][0] : xc[b];
-            }
-#pragma unroll
-            for (int b = 0; b < kMsShifts; ++b) {
-              px[b][0] = cfma(cconj(sn[b]), y[b], cscale(x[b], c[b]));
-              xc[b] = cfma(cneg(sn[b]), x[b], cscale(y[b], c[b]));
-              if (v[b] & kRepLast) px[b][1] = xc[b];
-            }
-          }
-        }
-        __syncwarp();
-        if (!isZ) {
-          for (int rr = 0; rr < 32 && r0 + rr < rows; ++rr)
-            for (int c = lane; c < nr; c += 32) T[(size_t)(r0 + rr) * ldt + rlo + c] = tile[rr * kMsColPitch + c];
-        } else {
-          if (r0 + lane < rows)
-            for (int c = 0; c < nr; ++c) Z[(size_t)(rlo + c) * n + r0 + lane] = tile[lane * kMsColPitch + c];
-        }
-        __syncwarp();
+        // Z(r, rlo..rhi) (column-major): column rotations, lane = row
+        const int r = 32 * (task - nR - nU) + lane;
+        if (r < n) replay_frame<false>(Z + r, (size_t)n, top0, nsteps, rlo, rhi, sm);
       }
     }
     __syncthreads();
@@ -1203,13 +1186,13 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
 // Schur form by multishift sweeps on active blocks of at least ms_min rows
 // (ms_min >= kMsMin) and single-shift sweeps on smaller ones.  Returns 0 or
 // RCWA_ERR_NOCONV.
-__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSmem& sm) {
+__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSmem& sm, int sweep_cap) {
   const double ulp = 2.0 * RCWA_DBL_EPS;
   const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
   const int tid = threadIdx.x;
   int i = n - 1;
   long long sweeps = 0;
-  const long long budget = 30LL * max(10, n);
+  const long long budget = sweep_cap > 0 ? min(30LL * max(10, n), (long long)sweep_cap) : 30LL * max(10, n);
   int stall = 0, last_i = -1, last_l = -1;
   while (i >= 0) {
     int best = 0;
@@ -1281,7 +1264,7 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
     {
       STAT_ADD(0, 1);
       if (tid < 32) {
-        cplx* B = sm.tiles;  // s x s, stride s + 1
+        cplx* B = sm.work;  // s x s, stride s + 1
         const int o = ib - s + 1;
         if (stall > 0 && stall % 6 == 0) {
           for (int k = tid; k < s; k += 32)
@@ -1302,8 +1285,23 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
   return 0;
 }
 
+// True when every entry of the Hessenberg matrix is finite (whole CTA).  A
+// NaN or Inf never passes the deflation tests, so such a matrix would only
+// burn the sweep budget; it is reported as RCWA_ERR_NONFINITE instead.
+__device__ bool hessenberg_finite(const cplx* T, int ldt, int n, int* redi) {
+  int bad = 0;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx % n;
+    if (r <= c + 1) {
+      const cplx v = T[(size_t)r * ldt + c];
+      if (!isfinite(v.x) || !isfinite(v.y)) bad = 1;
+    }
+  }
+  return block_max_int(bad, redi) == 0;
+}
+
 __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr, int n, int lda, cplx* w_all,
-                                                             void* work, int* info_all, int ms_min) {
+                                                             void* work, int* info_all, int ms_min, int sweep_cap) {
   extern __shared__ __align__(16) unsigned char dsm[];
   const MsSmem sm = carve_ms_smem(dsm);
   // identity slot of every bulge's rotation log (inactive chain steps)
@@ -1317,7 +1315,8 @@ __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr,
 #ifdef RCWA_EIG_STATS
   const long long c_schur = clock64();
 #endif
-  const int status = schur_ms(A, lda, s.Z, n, ms_min, sm);
+  const int status = hessenberg_finite(A, lda, n, sm.redi) ? schur_ms(A, lda, s.Z, n, ms_min, sm, sweep_cap)
+                                                          : RCWA_ERR_NONFINITE;
 #ifdef RCWA_EIG_STATS
   STAT_ADD(10, clock64() - c_schur);
 #endif
@@ -1418,14 +1417,15 @@ __global__ void __launch_bounds__(kHessThreads) hessenberg_kernel(cplx* const* A
 }
 
 __global__ void __launch_bounds__(kEigThreads) schur_kernel(cplx* const* Aarr, int n, int lda, cplx* w_all,
-                                                           void* work, int* info_all) {
+                                                           void* work, int* info_all, int sweep_cap) {
   __shared__ cplx Wt[kWin][kWin + 1];
   __shared__ int redi[kEigThreads / 32];
   __shared__ double rc[kWin];
   __shared__ cplx rs[kWin];
   cplx* A = Aarr[blockIdx.x];
   const Scratch s = scratch_for(work, n, blockIdx.x);
-  const int status = schur(A, lda, s.Z, n, Wt, rc, rs, redi);
+  const int status = hessenberg_finite(A, lda, n, redi) ? schur(A, lda, s.Z, n, Wt, rc, rs, redi, sweep_cap)
+                                                       : RCWA_ERR_NONFINITE;
   cplx* w = w_all + (size_t)blockIdx.x * n;
   for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = A[(size_t)k * lda + k];
   if (threadIdx.x == 0) info_all[blockIdx.x] = status;
@@ -1455,29 +1455,36 @@ __global__ void normalize_kernel(cplx* const* VRarr, int n, int ldv, const cplx*
 }  // namespace
 
 
+namespace {
+// QR sweep cap of every later eigensolve (0: the built-in budget), set by
+// rcwa_set_qr_sweep_limit; read when the Schur kernels are launched.
+std::atomic<int> g_qr_sweep_cap{0};
+}  // namespace
+
+extern "C" int rcwa_set_qr_sweep_limit(int sweeps) {
+  if (sweeps < 0) return RCWA_ERR_INVALID;
+  g_qr_sweep_cap.store(sweeps);
+  return RCWA_OK;
+}
+
 cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* VR, int ldv, void* work,
                           int* info, int batch, cudaStream_t st, StageProf* prof, int ms_min) {
   if (batch <= 0 || n <= 0) return cudaSuccess;
   ms_min = max(ms_min, kMsMin);
+  const int sweep_cap = g_qr_sweep_cap.load();
   StageProf none;
   StageProf& P = prof ? *prof : none;
   hessenberg_kernel<<<batch, kHessThreads, 0, st>>>(A, n, lda, work);
   ++launch_counter();
   P.mark(st, kStHessenberg);
   if (n < ms_min) {
-    schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info);
+    schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info, sweep_cap);
     ++launch_counter();
   } else {
-    static bool attr_set[64] = {};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-      cudaError_t e = cudaFuncSetAttribute(schur_ms_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kMsSmemBytes);
-      if (e != cudaSuccess) return e;
-      if (dev >= 0 && dev < 64) attr_set[dev] = true;
-    }
-    schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info, ms_min);
+    static SmemAttrOnce attr;
+    cudaError_t e = attr.ensure(schur_ms_kernel, (int)kMsSmemBytes);
+    if (e != cudaSuccess) return e;
+    schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info, ms_min, sweep_cap);
     ++launch_counter();
   }
   P.mark(st, kStSchur);

@@ -164,7 +164,7 @@ int validate_stack(const rcwa_stack& s, std::string& why) {
   for (int l = 0; l < s.n_layers; ++l) {
     for (size_t c = 0; c < cells; ++c) {
       const rcwa_cplx z = s.eps[(size_t)l * cells + c];
-      if (!finite_c(z)) { why = "non-finite permittivity"; return RCWA_ERR_INVALID; }
+      if (!finite_c(z)) { why = "non-finite permittivity"; return RCWA_ERR_NONFINITE; }
       if (z.re == 0.0 && z.im == 0.0) { why = "zero permittivity"; return RCWA_ERR_INVALID; }
     }
     if (l == 0 || l == s.n_layers - 1) {
@@ -633,7 +633,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       P->steps.push_back([plan, CL, jobs_meta](cudaStream_t st, StageProf& pf) {
         ConvLaunch cl = CL;
         cl.jobs = (ConvJob*)((char*)plan->meta.p + jobs_meta);
-        cudaError_t err = conv_matrices(cl, st);
+        cudaError_t err = conv_matrices(cl, st, &pf);
         pf.mark(st, kStConvGather);
         return err;
       });
@@ -1114,6 +1114,24 @@ extern "C" int rcwa_plan_rescatter(rcwa_plan* p, const rcwa_cplx* pxy) {
     return RCWA_ERR_CUDA;
   // the host copy must outlive the asynchronous upload
   return cudaStreamSynchronize(st) == cudaSuccess ? RCWA_OK : RCWA_ERR_CUDA;
+}
+
+extern "C" int rcwa_plan_smatrix(rcwa_plan* p, int point, rcwa_cplx* Rud, rcwa_cplx* Tdd) {
+  if (!p) return RCWA_ERR_INVALID;
+  if (point < 0 || point >= p->n_pts) return fail(p->e, RCWA_ERR_INVALID, "point index out of range");
+  if (p->chunks != 1) return fail(p->e, RCWA_ERR_UNSUPPORTED, "the S-matrix of a multi-chunk plan is not kept");
+  if (cudaSetDevice(p->e->device) != cudaSuccess) return RCWA_ERR_CUDA;
+  const ScatterItem* it = nullptr;
+  for (const ScatterItem& s : p->scatter_items)
+    if (s.point == point) { it = &s; break; }
+  if (!it) return fail(p->e, RCWA_ERR_INVALID, "point not found in the plan");
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, "execution failed");
+  const size_t n = 2 * (size_t)p->point_N[point];
+  if (Rud && cudaMemcpy(Rud, it->Rud, sizeof(cplx) * n * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(p->e, RCWA_ERR_CUDA, "download failed");
+  if (Tdd && cudaMemcpy(Tdd, it->Tdd, sizeof(cplx) * n * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return fail(p->e, RCWA_ERR_CUDA, "download failed");
+  return RCWA_OK;
 }
 
 extern "C" int rcwa_plan_schedule(const rcwa_plan* p, int chunk, int* sched) {

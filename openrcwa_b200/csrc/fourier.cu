@@ -9,8 +9,10 @@
 // the cell grid into small tables: the 2D Laurent table, the strip-indicator
 // coefficients, and the Toeplitz matrices of the 1/eps coefficients of every
 // strip.  Stage 2 inverts those Toeplitz matrices with the batched LU.  Stage 3
-// is the HBM-bound gather that writes the three N x N matrices, each output
-// element a short sum over strips read from the L1/L2-resident tables.
+// is the HBM-bound gather that writes the three N x N matrices from tables
+// staged in shared memory, whole rows at a time.
+#include <algorithm>
+
 #include "fourier.cuh"
 #include "linalg.cuh"
 
@@ -113,36 +115,75 @@ __global__ void conv_tables_kernel(ConvJob* jobs, int nx, int ny, int max_ncx, i
   }
 }
 
-// Gather: one thread per output element of each N x N matrix.
+// Gather: the three N x N convolution matrices, written row by row.
 //   fe33(row,col) = F2D[(m-j)+nx-1][(n-l)+ny-1]
 //   fe11(row,col) = sum_i fY_i[(n-l)+ny-1] * TXinv_i[m][j]
 //   fe22(row,col) = sum_i fX_i[(m-j)+nx-1] * TYinv_i[n][l]
-// with m = row/ny, n = row%ny, j = col/ny, l = col%ny.
-__global__ void __launch_bounds__(256) conv_gather_kernel(const ConvJob* jobs, int nx, int ny, int max_ncx,
-                                                         int max_ncy) {
-  const ConvJob J = jobs[blockIdx.y];
+// with m = row/ny, n = row%ny, j = col/ny, l = col%ny.  A CTA owns rows n0..n1
+// of block row m of one layer.  Everything its outputs depend on is staged in
+// shared memory first: the F2D rows m..m+nx-1, the per-(j, q) sums
+// C11[j][q] = sum_i fY_i[q] TXinv_i[m][j] (so fe11 becomes a table look-up),
+// the weights fX_i[m-j+nx-1] and, when they fit, the TYinv blocks.  The output
+// then streams to HBM as whole rows, 16-byte elements on consecutive threads.
+constexpr int kGatherThreads = 256;
+constexpr size_t kGatherSmemMax = 200 * 1024;
+
+__host__ __device__ inline size_t gather_smem_base(int nx, int ny, int max_ncx) {
+  const size_t PY = 2 * (size_t)ny - 1, mxs = (size_t)max(max_ncx - 1, 1);
+  return sizeof(cplx) * (2 * (size_t)nx * PY + (size_t)nx * mxs);
+}
+__host__ __device__ inline size_t gather_smem_ty(int ny, int max_ncx) {
+  return sizeof(cplx) * (size_t)max(max_ncx - 1, 1) * ny * ny;
+}
+
+__global__ void __launch_bounds__(kGatherThreads) conv_gather_kernel(const ConvJob* jobs, int nx, int ny,
+                                                                    int max_ncx, int max_ncy, int rows_per_cta,
+                                                                    int ty_in_smem) {
+  extern __shared__ __align__(16) unsigned char gsm[];
+  const ConvJob J = jobs[blockIdx.z];
   const TabLayout L = tab_layout(nx, ny, max_ncx, max_ncy);
   const cplx* __restrict__ tab = J.tab;
   const int N = nx * ny;
-  const int nxs = J.ncx - 1, nys = J.ncy - 1;
+  const int nxs = J.ncx - 1, nys = J.ncy - 1, mxs = max(max_ncx - 1, 1);
   const int PY = 2 * ny - 1, PX = 2 * nx - 1;
-  const size_t total = (size_t)N * N;
-  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
-    const int row = (int)(e / N), col = (int)(e % N);
-    const int m = row / ny, n = row % ny, j = col / ny, l = col % ny;
-    const int dm = m - j + nx - 1, dn = n - l + ny - 1;
-    if (J.fe33) J.fe33[e] = __ldg(&tab[L.f2d + (size_t)dm * PY + dn]);
-    if (J.fe11) {
-      cplx acc = mkc(0.0, 0.0);
-      for (int i = 0; i < nys; ++i)
-        acc = cfma(__ldg(&tab[L.fy + (size_t)i * PY + dn]), __ldg(&tab[L.txinv + ((size_t)i * nx + m) * nx + j]), acc);
-      J.fe11[e] = acc;
-    }
-    if (J.fe22) {
-      cplx acc = mkc(0.0, 0.0);
-      for (int i = 0; i < nxs; ++i)
-        acc = cfma(__ldg(&tab[L.fx + (size_t)i * PX + dm]), __ldg(&tab[L.tyinv + ((size_t)i * ny + n) * ny + l]), acc);
-      J.fe22[e] = acc;
+  const int m = blockIdx.x;
+  const int n0 = blockIdx.y * rows_per_cta, n1 = min(ny, n0 + rows_per_cta);
+  if (n0 >= n1) return;
+  cplx* F33 = reinterpret_cast<cplx*>(gsm);  // [nx][PY]
+  cplx* C11 = F33 + (size_t)nx * PY;         // [nx][PY]
+  cplx* W22 = C11 + (size_t)nx * PY;         // [nx][mxs]
+  cplx* TYs = W22 + (size_t)nx * mxs;        // [mxs][ny][ny] when staged
+  const cplx* TY = ty_in_smem ? TYs : tab + L.tyinv;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < nx * PY; idx += blockDim.x) {
+    const int j = idx / PY, q = idx % PY;
+    F33[idx] = __ldg(&tab[L.f2d + (size_t)(m - j + nx - 1) * PY + q]);
+    cplx acc = mkc(0.0, 0.0);
+    for (int i = 0; i < nys; ++i)
+      acc = cfma(__ldg(&tab[L.fy + (size_t)i * PY + q]), __ldg(&tab[L.txinv + ((size_t)i * nx + m) * nx + j]), acc);
+    C11[idx] = acc;
+  }
+  for (int idx = tid; idx < nx * mxs; idx += blockDim.x) {
+    const int j = idx / mxs, i = idx % mxs;
+    W22[idx] = i < nxs ? __ldg(&tab[L.fx + (size_t)i * PX + (m - j + nx - 1)]) : mkc(0.0, 0.0);
+  }
+  if (ty_in_smem)
+    for (int idx = tid; idx < nxs * ny * ny; idx += blockDim.x) TYs[idx] = __ldg(&tab[L.tyinv + idx]);
+  __syncthreads();
+  for (int n = n0; n < n1; ++n) {
+    const size_t row = (size_t)(m * ny + n) * N;
+    for (int c = tid; c < N; c += blockDim.x) {
+      const int j = c / ny, l = c - j * ny;
+      const int t = j * PY + (n - l + ny - 1);
+      if (J.fe33) J.fe33[row + c] = F33[t];
+      if (J.fe11) J.fe11[row + c] = C11[t];
+      if (J.fe22) {
+        cplx acc = mkc(0.0, 0.0);
+        const cplx* w = W22 + (size_t)j * mxs;
+        const cplx* ty = TY + (size_t)n * ny + l;
+        for (int i = 0; i < nxs; ++i) acc = cfma(w[i], ty[(size_t)i * ny * ny], acc);
+        J.fe22[row + c] = acc;
+      }
     }
   }
 }
@@ -179,7 +220,7 @@ __global__ void fill_table_ptrs(const ConvJob* jobs, int njobs, int nx, int ny, 
 
 size_t conv_table_elems(int nx, int ny, int ncx, int ncy) { return tab_layout(nx, ny, ncx, ncy).total; }
 
-cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st) {
+cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st, StageProf* prof) {
   if (P.njobs <= 0) return cudaSuccess;
   const int mys = P.max_ncy - 1, mxs = P.max_ncx - 1;
   conv_tables_kernel<<<P.njobs, 256, 0, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy);
@@ -197,10 +238,25 @@ cudaError_t conv_matrices(const ConvLaunch& P, cudaStream_t st) {
   if ((err = zgetrs_batched(P.ty_ptrs, P.ny, P.ny, P.ipiv, P.tyinv_ptrs, P.ny, P.ny, P.njobs * mxs, st)) !=
       cudaSuccess)
     return err;
-  const size_t NN = (size_t)P.nx * P.ny * P.nx * P.ny;
-  const size_t nblk = (NN + 255) / 256;
-  dim3 grid((unsigned)(nblk < 2048 ? nblk : 2048), P.njobs);
-  conv_gather_kernel<<<grid, 256, 0, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy);
+  if (prof) prof->mark(st, kStConvTables);
+  // rows of a block row split so that the grid covers the SMs about twice
+  int sms = 148;
+  {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  }
+  const long long per_split = (long long)P.nx * P.njobs;
+  int nsplit = (int)std::min<long long>(P.ny, std::max<long long>(1, (2LL * sms + per_split - 1) / per_split));
+  const int rows = (P.ny + nsplit - 1) / nsplit;
+  nsplit = (P.ny + rows - 1) / rows;
+  size_t smem = gather_smem_base(P.nx, P.ny, P.max_ncx);
+  const int ty_in_smem = smem + gather_smem_ty(P.ny, P.max_ncx) <= kGatherSmemMax ? 1 : 0;
+  if (ty_in_smem) smem += gather_smem_ty(P.ny, P.max_ncx);
+  if (smem > kGatherSmemMax) return cudaErrorInvalidValue;  // harmonic grid beyond the staged tables
+  static SmemAttrOnce attr;
+  if ((err = attr.ensure(conv_gather_kernel, (int)kGatherSmemMax)) != cudaSuccess) return err;
+  dim3 grid(P.nx, nsplit, P.njobs);
+  conv_gather_kernel<<<grid, kGatherThreads, smem, st>>>(P.jobs, P.nx, P.ny, P.max_ncx, P.max_ncy, rows, ty_in_smem);
   ++launch_counter();
   return cudaGetLastError();
 }

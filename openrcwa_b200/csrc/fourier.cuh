@@ -36,7 +36,9 @@ struct ConvLaunch {
   int* info;           // device [njobs*max(...)]
 };
 
-cudaError_t conv_matrices(const ConvLaunch& L, cudaStream_t st);
+// With prof, the time up to the gather is charged to the conv_tables stage
+// (tables and Toeplitz inverses); the caller marks the gather's end.
+cudaError_t conv_matrices(const ConvLaunch& L, cudaStream_t st, StageProf* prof = nullptr);
 
 // FourierSolver1D::solve on the device: Ff[M] from edges x[nxe], f[nxe-1].
 cudaError_t fourier1d_device(const double* x, int nxe, double d, const cplx* f, int M, cplx* Ff,

@@ -310,17 +310,11 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
 cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st) {
   if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
   if (g.K <= 0 || g.transA || g.transB || g.s || !err || !scale_ws) return cudaErrorInvalidValue;
-  static bool attr_set[64] = {};
-  int dev = 0;
-  cudaGetDevice(&dev);
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    cudaError_t e = cudaFuncSetAttribute(zgemm_tf32x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)kTcSmem);
-    if (e != cudaSuccess) return e;
-    attr_set[dev] = true;
-  }
+  static SmemAttrOnce attr;
+  cudaError_t e = attr.ensure(zgemm_tf32x3_kernel, (int)kTcSmem);
+  if (e != cudaSuccess) return e;
   // 0x80 bytes: every exponent starts at a very negative value
-  cudaError_t e = cudaMemsetAsync(scale_ws, 0x80, sizeof(int) * 2 * g.batch, st);
+  e = cudaMemsetAsync(scale_ws, 0x80, sizeof(int) * 2 * g.batch, st);
   if (e != cudaSuccess) return e;
   tc_scale_kernel<<<dim3(16, g.batch, 2), 256, 0, st>>>(g, scale_ws);
   ++launch_counter();

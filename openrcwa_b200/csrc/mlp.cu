@@ -658,14 +658,8 @@ extern "C" {
 int rcwa_mlp_predict(rcwa_mlp* m, const float* X, int n, float* Y) {
   if (!m || !X || !Y || n < 1) return RCWA_ERR_INVALID;
   if (cudaSetDevice(m->e->device) != cudaSuccess) return RCWA_ERR_CUDA;
-  static bool attr_set[64] = {};
-  const int dev = m->e->device;
-  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
-    if (cudaFuncSetAttribute(mlp_layer_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInfSmem) !=
-        cudaSuccess)
-      return RCWA_ERR_CUDA;
-    attr_set[dev] = true;
-  }
+  static SmemAttrOnce attr;
+  if (attr.ensure(mlp_layer_tc_kernel, (int)kInfSmem) != cudaSuccess) return RCWA_ERR_CUDA;
   const int L = (int)m->dims.size() - 1;
   if (m->Wb.empty()) {
     m->Wb.assign(L, nullptr);

@@ -31,7 +31,11 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
 // Device address of g_noalloc_scratch per device.  In host code the symbol
 // name is only a stand-in, so the address is looked up once per device with
-// that device current.
+// that device current.  Under CUDA's lazy module loading (the default since
+// CUDA 12.2) the driver loads this library's device code, and reserves the
+// array, at that first lookup: the first call on a device is where the
+// reservation can fail (a device already full), and it must not come during
+// a stream capture.  Later calls touch no allocator at all.
 constexpr int kMaxDevices = 64;
 unsigned char* g_scratch_addr[kMaxDevices] = {};
 std::mutex g_scratch_mu;
@@ -51,6 +55,9 @@ extern "C" int rcwa_zgeev_batched_noalloc(int n, int batch, rcwa_cplx* A, rcwa_c
   if (n < 1 || batch < 1 || !A || !w || !VR || !info) return RCWA_ERR_INVALID;
   if (n > kMaxN || batch > kMaxBatch || scratch_bytes_needed(n, batch) > kScratchBytes)
     return RCWA_ERR_UNSUPPORTED;  // beyond the static scratch: n <= 64 and batch <= 64
+  // an error left pending by the caller's own earlier work is reported, not
+  // cleared: it stays readable with cudaGetLastError after this call
+  if (cudaPeekAtLastError() != cudaSuccess) return RCWA_ERR_CUDA;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return RCWA_ERR_CUDA;
   unsigned char* base = nullptr;

@@ -2,6 +2,8 @@
 # Builds the reference-side test binary into oracle/_ref/ (kept out of git,
 # shipped with the tree to the GPU box).  Needs the reference sources at
 # $REF (default /root/reference) and the engine library already built.
+# "build_ref.sh --print-ref" prints the sources' location and exits; without
+# the sources the script prints a note and exits 0 (nothing to build).
 #
 #   rcwa_bridge_dropin : the reference's sol/rcwa_bridge.cpp, unmodified,
 #                        compiled against include/openrcwa_b200/rcwa/*.h and
@@ -13,9 +15,10 @@ set -e
 HERE=$(cd "$(dirname "$0")" && pwd)
 ROOT=$(dirname "$HERE")
 REF=${REF:-/root/reference}
+if [ "$1" = "--print-ref" ]; then echo "$REF"; exit 0; fi
+[ -f "$REF/sol/rcwa_bridge.cpp" ] || { echo "reference sources not found at $REF: nothing to build"; exit 0; }
 OUT="$HERE/_ref"
 mkdir -p "$OUT"
-[ -f "$REF/sol/rcwa_bridge.cpp" ] || { echo "reference sources not found at $REF"; exit 1; }
 CXXFLAGS="-std=c++17 -O2 -DRCWA_B200_NO_EIGEN -I$ROOT/include/openrcwa_b200 -I$REF/include"
 g++ $CXXFLAGS -c "$REF/sol/rcwa_bridge.cpp" -o "$OUT/rcwa_bridge.o"
 g++ $CXXFLAGS -c "$HERE/dropin_harness.cpp" -o "$OUT/dropin_harness.o"

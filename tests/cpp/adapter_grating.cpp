@@ -29,5 +29,13 @@ int main() {
     s.scatterPlaneWave(c, 0, 2, k0, R, T);
     std::printf("%.12f %.12f\n", R.sum(), T.sum());
   }
+  // the solved scattering matrices (RCWASolver::Rud(), Tdd()), row by row
+  const Eigen::MatrixXcs& Rud = s.Rud();
+  const Eigen::MatrixXcs& Tdd = s.Tdd();
+  std::printf("%d %d\n", (int)Rud.rows(), (int)Tdd.cols());
+  for (int i = 0; i < (int)Rud.rows(); ++i)
+    for (int j = 0; j < (int)Rud.cols(); ++j)
+      std::printf("%.17g %.17g %.17g %.17g\n", Rud(i, j).real(), Rud(i, j).imag(), Tdd(i, j).real(),
+                  Tdd(i, j).imag());
   return 0;
 }

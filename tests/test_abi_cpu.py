@@ -72,7 +72,9 @@ def test_cpp_adapters_compile_without_eigen():
                     "-I", os.path.join(ROOT, "include", "openrcwa_b200"), src], check=True)
 
 
-REF = "/root/reference"
+# where the reference sources are mounted: the drop-in recipe knows (REF env var)
+REF = subprocess.run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh"), "--print-ref"], capture_output=True,
+                     text=True).stdout.strip()
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "sol", "rcwa_bridge.cpp")),

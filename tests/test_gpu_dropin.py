@@ -66,9 +66,28 @@ def test_cpp_api_adapter(tmp_path):
                     f"-Wl,-rpath,{lib}", "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
-    vals = [list(map(float, ln.split())) for ln in out.stdout.strip().splitlines()]
+    lines = out.stdout.strip().splitlines()
+    vals = [list(map(float, ln.split())) for ln in lines[:2]]
     ref = rcwa_run(OfdSetup(nHx=5, period_x=3e-7, layers=[L(1, 1, .5, 0), L(4, 1, .5, 2e-7), L(2.25, 2.25, .5, 0)],
                             freqs=[6.5e14]))[0]
+    # Rud() / Tdd(): against the oracle's cascade matrices in field space
+    # (W_top Rud W_top^-1, W_bottom Tdd W_top^-1), which does not depend on
+    # the basis LAPACK picks inside the half-spaces' degenerate eigenspaces
+    rows, cols = map(int, lines[2].split())
+    assert rows == cols == 22
+    m = np.array([list(map(float, ln.split())) for ln in lines[3:3 + rows * cols]]).reshape(rows, cols, 4)
+    Rud, Tdd = m[..., 0] + 1j * m[..., 1], m[..., 2] + 1j * m[..., 3]
+    from oracle.rcwa_oracle import OracleLayer, RCWASolver
+    sol = RCWASolver(5, 0)
+    cx, cy = np.array([0, 1.5e-7, 3e-7]), np.array([0, 3e-7])
+    for e in ([1, 1], [4, 1], [2.25, 2.25]):
+        sol.addLayer(OracleLayer(cx, cy, np.array([e], dtype=complex)))
+    sol.solve(2.99792458e8 / 6.5e14, [0, 1, 2], [0, 2e-7, 0])
+    Wt, Wb = sol.sol[0].W, sol.sol[2].W
+    Rf = Wt @ sol.Rud @ np.linalg.inv(Wt)
+    Tf = Wb @ sol.Tdd @ np.linalg.inv(Wt)
+    assert np.max(np.abs(Rud - Rf)) < 1e-9 * max(1.0, np.abs(Rf).max())
+    assert np.max(np.abs(Tdd - Tf)) < 1e-9 * max(1.0, np.abs(Tf).max())
     assert abs(vals[0][0] - ref["R"][0]) < 1e-9 and abs(vals[1][0] - ref["R"][1]) < 1e-9
     assert abs(vals[0][1] - ref["T"][0]) < 1e-9 and abs(vals[1][1] - ref["T"][1]) < 1e-9
     assert abs(vals[0][0] - 0.138130) < 1e-6 and abs(vals[1][0] - 0.204841) < 1e-6

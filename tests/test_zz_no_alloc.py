@@ -39,9 +39,18 @@ def test_noalloc_matches_allocating_entry_point_twice():
     eng = o.Engine(0)
     lib = o.load()
     rng = np.random.default_rng(5)
-    for (n, b) in [(22, 16), (64, 64)]:
-        A = rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n))
-        w_ref, V_ref, info_ref = eng.zgeev(A.copy())
+    cases = [(22, 16), (64, 64)]
+    # one untimed call per size first: it is where lazy module loading reserves
+    # the static scratch, and it leaves torch's caching pool holding blocks of
+    # every size the checked calls use, so that the free device memory can
+    # only move afterwards if the entry point itself allocates
+    inputs = [rng.normal(size=(b, n, n)) + 1j * rng.normal(size=(b, n, n)) for (n, b) in cases]
+    refs = [eng.zgeev(A.copy()) for A in inputs]
+    for A in inputs:
+        _run_noalloc(lib, torch, A)
+    free0 = torch.cuda.mem_get_info()[0]
+    for A, (w_ref, V_ref, info_ref) in zip(inputs, refs):
+        b, n, _ = A.shape
         w, V, info = _run_noalloc(lib, torch, A)
         assert np.all(info == 0) and np.all(info_ref == 0)
         assert np.max(np.abs(w - w_ref)) < 1e-12 * np.max(np.abs(w_ref))
@@ -49,6 +58,10 @@ def test_noalloc_matches_allocating_entry_point_twice():
         for k in range(b):
             res = np.abs(A[k] @ V[k] - V[k] * w[k][None, :]).max() / np.abs(A[k]).max()
             assert res < 1e-12 * n
+    # the two calls after the warm-up left the device's free memory unchanged
+    # (torch's own buffers of the calls come from its caching pool, whose
+    # blocks were reserved by the warm-up calls of the same sizes)
+    assert torch.cuda.mem_get_info()[0] == free0
     eng.close()
 
 
