@@ -111,6 +111,41 @@ int rcwa_engine_solve_batch(rcwa_engine* e,
                             double* ref_orders, double* trn_orders,
                             int* status);
 
+/* A layer stack whose patterned layers are given by their 2D Laurent
+ * coefficient tables instead of a cell grid: F2D[p][q] =
+ * (1/(Lx Ly)) integral of eps(x,y) exp(-i 2pi (m x/Lx + n y/Ly)), m = p - 2nHx,
+ * n = q - 2nHy, the table layout of FourierSolver2D's ContinuousXY branch
+ * (rcwa/FourierSolver2D.cpp:250-349).  All three convolution matrices of such a
+ * layer are the table's block-Toeplitz matrix (the Laurent rule for every
+ * tensor), e.g. the closed-form disk transform of circular pillars, which the
+ * reference only approximates by staircasing (rcwa/RCWADriver.cpp:19-37).
+ * Layers 0 and n_layers-1 are uniform half-spaces of permittivity eps_half[0]
+ * and eps_half[1]. */
+typedef struct {
+  int nHx, nHy;              /* harmonics: 2*nHx+1 by 2*nHy+1 orders            */
+  double Lx, Ly;             /* periods                                          */
+  int n_layers;              /* >= 2                                             */
+  const rcwa_cplx* eps_half; /* [2] incidence and transmission half-spaces      */
+  const rcwa_cplx* f2d;      /* [n_layers-2][(4nHx+1)*(4nHy+1)] row-major        */
+  const double* thickness;   /* [n_layers] (0 < l < n_layers-1 used)             */
+} rcwa_table_stack;
+
+/* rcwa_engine_solve_batch / rcwa_plan_create for Laurent-table stacks
+ * (same points, outputs and precision modes). */
+int rcwa_engine_solve_tables(rcwa_engine* e,
+                             const rcwa_table_stack* stacks, int n_stacks,
+                             const rcwa_point* pts, int n_pts,
+                             int n_exc, const rcwa_cplx* pxy,
+                             int precision,
+                             double* R, double* T,
+                             double* ref_orders, double* trn_orders,
+                             int* status);
+int rcwa_plan_create_tables(rcwa_engine* e,
+                            const rcwa_table_stack* stacks, int n_stacks,
+                            const rcwa_point* pts, int n_pts,
+                            int n_exc, const rcwa_cplx* pxy, int precision,
+                            rcwa_plan** out);
+
 /* The same solve split in three so that a caller can keep the inputs resident
  * and time the device work alone: plan_create uploads the inputs and sizes the
  * workspace, plan_execute enqueues every kernel on `stream` (a cudaStream_t,
@@ -220,8 +255,10 @@ int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch, const rcw
  *                      single-shift sweeps (64, 96, 128, 192; only 64 for
  *                      n < 64 and n >= 512; default 128 for 64 <= n < 128,
  *                      else 64)
- *   RCWA_TUNE_PRODUCT  mixed plans' cascade products, 0: 3xTF32 on tcgen05,
- *                      1: FP64 tensor path
+ *   RCWA_TUNE_PRODUCT  mixed plans' cascade products and their tile shape,
+ *                      0: 3xTF32 on tcgen05 with 128 x 128 output tiles,
+ *                      1: FP64 tensor path, 2: 3xTF32 on tcgen05 with
+ *                      128 x 256 output tiles
  * Every choice computes the same quantities (LU: same pivoting rule; Schur:
  * same convergence tests; products: within the mixed tolerance), so a tuner
  * changes speed, not results beyond rounding.
@@ -279,6 +316,13 @@ int rcwa_mlp_train(rcwa_mlp* m, int epochs, int batch, float lr, unsigned long l
 int rcwa_mlp_loss_grad(rcwa_mlp* m, const float* X, const float* Y, int n, double* loss, float* grad);
 int rcwa_mlp_predict_fp32(rcwa_mlp* m, const float* X, int n, float* Y);
 int rcwa_mlp_predict(rcwa_mlp* m, const float* X, int n, float* Y);
+/* Squared Euclidean distance from each query row Q [n][n_in] (host floats,
+ * the features the network was trained on) to its nearest row of the
+ * training set given to rcwa_mlp_set_data, into d2[n] (host).  skip_self
+ * ignores distances of exactly 0, so training rows passed as queries get
+ * their leave-one-out distance.  n_in <= 32.  The surrogate's test of whether
+ * a query lies where the network has seen data. */
+int rcwa_mlp_nn_distance(rcwa_mlp* m, const float* Q, int n, int skip_self, float* d2);
 
 /* ---- slab S-matrices and the Redheffer star product -------------------------
  * Batched, FP64, host buffers; every matrix row-major [batch][n*n].
@@ -314,7 +358,7 @@ int rcwa_star_product_batched(rcwa_engine* e, int n, int batch,
  * an allocation may stall, hosts that fix their device footprint up front):
  * the same batched eigensolver as rcwa_zgeev_batched, on caller-owned DEVICE
  * buffers, with its scratch in a static device array of the library that every
- * GPU loading it holds until exit (about 22 MB).  Allocates nothing.
+ * GPU loading it holds until exit (about 38 MB).  Allocates nothing.
  *   A     device [batch][n*n] row-major, overwritten (Schur form on return)
  *   w     device [batch][n] eigenvalues
  *   VR    device [batch][n*n] row-major unit-norm right eigenvectors

@@ -46,7 +46,8 @@ EXPORTS = [
     "rcwa_plan_schedule", "rcwa_tuner_create", "rcwa_tuner_destroy", "rcwa_tuner_set_sms", "rcwa_tuner_candidates",
     "rcwa_tuner_default", "rcwa_tuner_set", "rcwa_tuner_get", "rcwa_tuner_count", "rcwa_tuner_entry",
     "rcwa_tuner_save", "rcwa_tuner_load", "rcwa_engine_set_tuner", "rcwa_tuner_measure",
-    "rcwa_set_qr_sweep_limit", "rcwa_plan_smatrix",
+    "rcwa_set_qr_sweep_limit", "rcwa_plan_smatrix", "rcwa_mlp_nn_distance", "rcwa_engine_solve_tables",
+    "rcwa_plan_create_tables",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -61,6 +62,11 @@ class rcwa_stack(C.Structure):
     _fields_ = [("nHx", C.c_int), ("nHy", C.c_int), ("ncx", C.c_int), ("ncy", C.c_int),
                 ("cx", C.c_void_p), ("cy", C.c_void_p), ("n_layers", C.c_int),
                 ("eps", C.c_void_p), ("thickness", C.c_void_p)]
+
+
+class rcwa_table_stack(C.Structure):
+    _fields_ = [("nHx", C.c_int), ("nHy", C.c_int), ("Lx", C.c_double), ("Ly", C.c_double),
+                ("n_layers", C.c_int), ("eps_half", C.c_void_p), ("f2d", C.c_void_p), ("thickness", C.c_void_p)]
 
 
 class rcwa_point(C.Structure):
@@ -105,6 +111,12 @@ def load() -> C.CDLL:
                                             C.c_int, C.c_int, C.c_void_p, C.c_int, _DP, _DP, _DP, _DP, _IP]
     lib.rcwa_plan_create.argtypes = [C.c_void_p, C.POINTER(rcwa_stack), C.c_int, C.POINTER(rcwa_point), C.c_int,
                                      C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_void_p)]
+    lib.rcwa_engine_solve_tables.argtypes = [C.c_void_p, C.POINTER(rcwa_table_stack), C.c_int,
+                                             C.POINTER(rcwa_point), C.c_int, C.c_int, C.c_void_p, C.c_int, _DP, _DP,
+                                             _DP, _DP, _IP]
+    lib.rcwa_plan_create_tables.argtypes = [C.c_void_p, C.POINTER(rcwa_table_stack), C.c_int,
+                                            C.POINTER(rcwa_point), C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                            C.POINTER(C.c_void_p)]
     lib.rcwa_plan_execute.argtypes = [C.c_void_p, C.c_void_p]
     lib.rcwa_plan_results.argtypes = [C.c_void_p, _DP, _DP, _DP, _DP, _IP]
     lib.rcwa_plan_launch_count.argtypes = [C.c_void_p]
@@ -144,6 +156,7 @@ def load() -> C.CDLL:
     lib.rcwa_mlp_loss_grad.argtypes = [C.c_void_p, _FP, _FP, C.c_int, _DP, _FP]
     lib.rcwa_mlp_predict_fp32.argtypes = [C.c_void_p, _FP, C.c_int, _FP]
     lib.rcwa_mlp_predict.argtypes = [C.c_void_p, _FP, C.c_int, _FP]
+    lib.rcwa_mlp_nn_distance.argtypes = [C.c_void_p, _FP, C.c_int, C.c_int, _FP]
     lib.rcwa_plan_schedule.argtypes = [C.c_void_p, C.c_int, _IP]
     lib.rcwa_tuner_create.argtypes = [C.POINTER(C.c_void_p)]
     lib.rcwa_tuner_destroy.argtypes = [C.c_void_p]
@@ -212,6 +225,29 @@ class Stack:
                           self.eps.shape[0], self.eps.ctypes.data, self.thickness.ctypes.data)
 
 
+class TableStack:
+    """A layer stack whose patterned layers are 2D Laurent coefficient tables
+    (rcwa_table_stack): f2d [n_layers - 2, 4nHx + 1, 4nHy + 1], the uniform
+    half-spaces' permittivities eps_half (2), thickness [n_layers]."""
+
+    def __init__(self, nHx, nHy, Lx, Ly, eps_half, f2d, thickness):
+        self.nHx, self.nHy = int(nHx), int(nHy)
+        self.Lx, self.Ly = float(Lx), float(Ly)
+        self.eps_half = np.ascontiguousarray(eps_half, dtype=np.complex128)
+        self.f2d = np.ascontiguousarray(f2d, dtype=np.complex128)
+        self.thickness = np.ascontiguousarray(thickness, dtype=np.float64)
+        assert self.eps_half.shape == (2,)
+        assert self.f2d.shape == (self.thickness.size - 2, 4 * self.nHx + 1, 4 * self.nHy + 1)
+
+    @property
+    def N(self):
+        return (2 * self.nHx + 1) * (2 * self.nHy + 1)
+
+    def c_struct(self):
+        return rcwa_table_stack(self.nHx, self.nHy, self.Lx, self.Ly, self.thickness.size, self.eps_half.ctypes.data,
+                                self.f2d.ctypes.data, self.thickness.ctypes.data)
+
+
 class Engine:
     def __init__(self, device: int = 0):
         self.lib = load()
@@ -254,7 +290,8 @@ class Engine:
     # -- batched solve ------------------------------------------------------
     @staticmethod
     def _pack(stacks: Sequence[Stack], points, pxy):
-        st = (rcwa_stack * len(stacks))(*[s.c_struct() for s in stacks])
+        kind = rcwa_table_stack if isinstance(stacks[0], TableStack) else rcwa_stack
+        st = (kind * len(stacks))(*[s.c_struct() for s in stacks])
         pts = np.asarray(points, dtype=np.float64).reshape(-1, 4)
         cp = (rcwa_point * len(pts))(*[rcwa_point(int(p[0]), p[1], p[2], p[3]) for p in pts])
         pxy = np.ascontiguousarray(pxy, dtype=np.complex128)
@@ -275,9 +312,9 @@ class Engine:
         ref = np.zeros(max(tot, 1)) if orders else None
         trn = np.zeros(max(tot, 1)) if orders else None
         status = np.zeros(npt, dtype=np.int32)
-        rc = self.lib.rcwa_engine_solve_batch(self.h, st, len(stacks), cp, npt, n_exc, _v(pxy), precision, _d(R),
-                                              _d(T), _d(ref) if orders else None, _d(trn) if orders else None,
-                                              _i(status))
+        fn = self.lib.rcwa_engine_solve_tables if isinstance(stacks[0], TableStack) else self.lib.rcwa_engine_solve_batch
+        rc = fn(self.h, st, len(stacks), cp, npt, n_exc, _v(pxy), precision, _d(R), _d(T),
+                _d(ref) if orders else None, _d(trn) if orders else None, _i(status))
         if rc and not np.any(status):
             self._check(rc, "solve_batch")
         REF = TRN = None
@@ -424,7 +461,8 @@ class Plan:
         self.n_pts, self.n_exc = len(cp), n_exc
         self.Ns = [stacks[int(p.stack)].N for p in cp]
         h = C.c_void_p()
-        rc = eng.lib.rcwa_plan_create(eng.h, st, len(stacks), cp, len(cp), n_exc, _v(pxy), precision, C.byref(h))
+        fn = eng.lib.rcwa_plan_create_tables if isinstance(stacks[0], TableStack) else eng.lib.rcwa_plan_create
+        rc = fn(eng.h, st, len(stacks), cp, len(cp), n_exc, _v(pxy), precision, C.byref(h))
         eng._check(rc, "plan_create")
         self.h = h
         eng._children.add(self)
@@ -548,6 +586,14 @@ class Mlp:
         fn = self.eng.lib.rcwa_mlp_predict if tensor_cores else self.eng.lib.rcwa_mlp_predict_fp32
         self.eng._check(fn(self.h, _f(X), X.shape[0], _f(Y)), "mlp_predict")
         return Y
+
+    def nn_distance(self, X, skip_self=False):
+        """Squared distance of every row of X to its nearest training row."""
+        X = np.ascontiguousarray(X, dtype=np.float32)
+        d2 = np.zeros(X.shape[0], dtype=np.float32)
+        self.eng._check(self.eng.lib.rcwa_mlp_nn_distance(self.h, _f(X), X.shape[0], 1 if skip_self else 0, _f(d2)),
+                        "mlp_nn_distance")
+        return d2
 
     def close(self):
         if self.h:

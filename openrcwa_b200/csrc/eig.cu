@@ -43,8 +43,9 @@ struct Scratch {
 };
 
 #ifdef RCWA_EIG_STATS
-// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 deferred cycles, 5 shift cycles, 6 split cycles,
-// 8 early-deflation cycles, 9 single-shift cycles, 10 Schur cycles, 11 early deflations, 12 deflated by them
+// counters: 0 ms sweeps, 1 ss sweeps, 2 passes, 3 chase cycles, 4 replay cycles, 5 window-Schur cycles,
+// 6 reordering and re-Hessenberg cycles, 7 early-deflation update cycles, 8 early-deflation cycles,
+// 9 single-shift cycles, 10 Schur cycles, 11 early deflations, 12 deflated by them
 __device__ unsigned long long g_eig_stats[32];
 #define STAT_ADD(i, v) do { if (threadIdx.x == 0) atomicAdd(&g_eig_stats[i], (unsigned long long)(v)); } while (0)
 #else
@@ -369,17 +370,6 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
 }
 
 // ---------------------------------------------------------------- QR
-__device__ __forceinline__ void givens(cplx x, cplx y, double& c, cplx& s) {
-  const double ax = cabs(x), ay = cabs(y);
-  if (ay == 0.0) { c = 1.0; s = mkc(0.0, 0.0); }
-  else if (ax == 0.0) { c = 0.0; s = mkc(1.0, 0.0); }
-  else {
-    const double nrm = hypot(ax, ay);
-    c = ax / nrm;
-    s = cscale(cmul(cscale(x, 1.0 / ax), cconj(y)), 1.0 / nrm);
-  }
-}
-
 // Rotation [c s; -conj(s) c] (c real) with G [x; y] = [r; 0], evaluated
 // with two reciprocal square roots after scaling both inputs by a power of
 // two: c = |x| / |(x, y)|, s = x conj(y) / (|x| |(x, y)|).
@@ -464,7 +454,7 @@ __device__ void qr_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, cplx sh
         }
         double c;
         cplx sn;
-        givens(x, y, c, sn);
+        givens_fast(x, y, c, sn);
         const int j0 = (r == l) ? r : r - 1;
         const int jj = j0 - ws + lane;
         if (jj < w) {
@@ -586,7 +576,10 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
 // the part of each line the chain spans held in registers (replay_frame), so
 // an element of T or Z crosses memory once per pass instead of once per
 // rotation.
-constexpr int kMsW = 64;           // window order
+#ifndef RCWA_MS_WINDOW
+#define RCWA_MS_WINDOW 64
+#endif
+constexpr int kMsW = RCWA_MS_WINDOW;  // window order (a build-time parameter)
 constexpr int kMsShifts = 10;      // bulges per sweep
 constexpr int kMsMin = kSchurCrossover;  // smallest crossover: the chase window needs 64 rows
 constexpr int kMsThreads = 256;    // eight warps
@@ -666,7 +659,7 @@ __device__ void small_eigs_warp(cplx* B, int ldb, int s, cplx* out) {
       else { x = B[r * ldb + r - 1]; y = B[(r + 1) * ldb + r - 1]; }
       double c;
       cplx sn;
-      givens(x, y, c, sn);
+      givens_fast(x, y, c, sn);
       __syncwarp();
       const int j = ((r == lo) ? r : r - 1) + lane;
       if (j <= hi) {
@@ -743,7 +736,7 @@ __device__ bool aed_window_schur(cplx* W, cplx* V, int nw) {
       else { x = AW(p, p - 1); y = AW(p + 1, p - 1); }
       double c;
       cplx sn;
-      givens(x, y, c, sn);
+      givens_fast(x, y, c, sn);
       __syncwarp();
       if (lane >= (p == lo ? p : p - 1) && lane < nw) {
         const cplx a = AW(p, lane), b = AW(p + 1, lane);
@@ -779,7 +772,7 @@ __device__ void aed_swap(cplx* W, cplx* V, int nw, int k) {
   const cplx t11 = AW(k, k), t22 = AW(k + 1, k + 1);
   double c;
   cplx sn;
-  givens(AW(k, k + 1), csub(t22, t11), c, sn);
+  givens_fast(AW(k, k + 1), csub(t22, t11), c, sn);
   __syncwarp();
   if (lane >= k + 2 && lane < nw) {
     const cplx a = AW(k, lane), b = AW(k + 1, lane);
@@ -872,7 +865,13 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
   __syncthreads();
   if (tid < 32) {
     const int lane = tid;
+#ifdef RCWA_EIG_STATS
+    long long c_w0 = clock64();
+#endif
     const bool ok = aed_window_schur(W, V, nw);
+#ifdef RCWA_EIG_STATS
+    if (lane == 0) { const long long c_w1 = clock64(); atomicAdd(&g_eig_stats[5], (unsigned long long)(c_w1 - c_w0)); c_w0 = c_w1; }
+#endif
     int ns = nw;
     if (ok) {
       // deflation test from the bottom, undeflatable eigenvalues moved up
@@ -920,12 +919,18 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
       }
     }
     if (lane == 0) { sm.aed[0] = ok ? 1 : 0; sm.aed[1] = ns; }
+#ifdef RCWA_EIG_STATS
+    if (lane == 0) atomicAdd(&g_eig_stats[6], (unsigned long long)(clock64() - c_w0));
+#endif
   }
   __syncthreads();
   const bool ok = sm.aed[0] != 0;
   const int ns = sm.aed[1];
   if (!ok) return -1;
   if (ns == nw && (s.x != 0.0 || s.y != 0.0)) return 0;
+#ifdef RCWA_EIG_STATS
+  const long long c_off = clock64();
+#endif
   // window, spike and the off-window blocks
   for (int idx = tid; idx < nw * nw; idx += nthr) {
     const int r = idx / nw, c = idx % nw;
@@ -972,6 +977,9 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
     }
   }
   __syncthreads();
+#ifdef RCWA_EIG_STATS
+  STAT_ADD(7, clock64() - c_off);
+#endif
   return nw - ns;
 }
 

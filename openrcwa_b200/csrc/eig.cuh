@@ -2,15 +2,15 @@
 #pragma once
 #include "common.cuh"
 
-constexpr int kEigPanel = 32;  // Hessenberg panel width
+constexpr int kEigPanel = 64;  // Hessenberg panel width
 // Default active-block size below which the Schur iteration switches from
 // multishift sweeps with early deflation to single-shift sweeps (also its
 // smallest allowed value).
 constexpr int kSchurCrossover = 64;
 
 // Workspace bytes per matrix for zgeev_batched at order n: Schur vectors and
-// eigenvector matrix (2 n^2), work vectors (4 n), panel buffers (4 n x 32 and
-// max(n, 32) x 32), the triangular factors of all panels, and the reflector
+// eigenvector matrix (2 n^2), work vectors (4 n), panel buffers (4 n x 64 and
+// max(n, 64) x 64), the triangular factors of all panels, and the reflector
 // scalars.
 __host__ __device__ constexpr size_t zgeev_workspace_bytes(int n) {
   return ((2 * (size_t)n * n + 4 * (size_t)n + 4 * (size_t)n * kEigPanel +

@@ -98,6 +98,10 @@ struct StackInfo {
   std::vector<cplx> eps;   // L * cells
   std::vector<double> thick;
   int ncx, ncy;
+  // stacks given by Laurent tables: one (2nx-1) x (2ny-1) table per
+  // patterned layer (layers 1..L-2); the cell grid is then one cell per layer
+  bool tables = false;
+  std::vector<cplx> f2d;
 };
 
 }  // namespace
@@ -117,7 +121,8 @@ struct rcwa_plan {
   int* dTcErr = nullptr;   // set when a tensor-core completion wait ran out
   int* dTcScale = nullptr; // operand scale exponents of the tensor-core products (2 x 1024)
   // per chunk: n, points, interface LU schedule, tau LU schedule, Schur
-  // crossover, product path (0: 3xTF32, 1: FP64 tensor path)
+  // crossover, product path (0: 3xTF32 on 128 x 128 tiles, 1: FP64 tensor
+  // path, 2: 3xTF32 on 128 x 256 tiles)
   std::vector<std::array<int, 6>> sched;
   int precision = RCWA_PREC_FP64;
   std::vector<std::function<cudaError_t(cudaStream_t, StageProf&)>> steps;
@@ -394,15 +399,63 @@ static size_t chunk_bytes_per_point(int N, int Lp) {
   return (size_t)(13 * nn + per_job * std::max(Lp - 2, 0));
 }
 
+namespace {
+int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcwa_point* pts, int n_pts, int n_exc,
+                     const rcwa_cplx* pxy, int precision, rcwa_plan** out);
+
+// A Laurent-table stack as a StackInfo: a one-cell grid per layer (the
+// half-spaces' permittivity, the patterned layers' mean permittivity, which
+// only decides whether a mixed plan keeps FP64 products for the stack) and
+// the tables themselves.
+int table_stack_info(const rcwa_table_stack& t, StackInfo& si, std::string& why) {
+  if (t.nHx < 0 || t.nHy < 0) { why = "negative harmonic count"; return RCWA_ERR_INVALID; }
+  if (!(t.Lx > 0) || !(t.Ly > 0) || !std::isfinite(t.Lx) || !std::isfinite(t.Ly)) {
+    why = "invalid period";
+    return RCWA_ERR_INVALID;
+  }
+  if (t.n_layers < 2 || !t.eps_half || !t.thickness || (t.n_layers > 2 && !t.f2d)) {
+    why = "need >= 2 layers and their tables";
+    return RCWA_ERR_INVALID;
+  }
+  si = StackInfo();
+  si.nx = 2 * t.nHx + 1;
+  si.ny = 2 * t.nHy + 1;
+  si.N = si.nx * si.ny;
+  si.L = t.n_layers;
+  si.ncx = si.ncy = 2;
+  si.cx = {0.0, t.Lx};
+  si.cy = {0.0, t.Ly};
+  si.Lx = t.Lx;
+  si.Ly = t.Ly;
+  si.tables = true;
+  const size_t tab = (size_t)(2 * si.nx - 1) * (2 * si.ny - 1);
+  si.f2d.resize(tab * (size_t)(t.n_layers - 2));
+  for (size_t i = 0; i < si.f2d.size(); ++i) {
+    if (!finite_c(t.f2d[i])) { why = "non-finite Laurent coefficient"; return RCWA_ERR_NONFINITE; }
+    si.f2d[i] = mkc(t.f2d[i].re, t.f2d[i].im);
+  }
+  si.eps.resize(t.n_layers);
+  for (int side = 0; side < 2; ++side) {
+    const rcwa_cplx z = t.eps_half[side];
+    if (!finite_c(z)) { why = "non-finite permittivity"; return RCWA_ERR_NONFINITE; }
+    if (z.re == 0.0 && z.im == 0.0) { why = "zero permittivity"; return RCWA_ERR_INVALID; }
+    si.eps[side == 0 ? 0 : t.n_layers - 1] = mkc(z.re, z.im);
+  }
+  const size_t mid = (size_t)(si.nx - 1) * (2 * si.ny - 1) + (si.ny - 1);  // F2D[0][0]
+  for (int l = 1; l + 1 < t.n_layers; ++l) si.eps[l] = si.f2d[(size_t)(l - 1) * tab + mid];
+  si.thick.assign(t.thickness, t.thickness + t.n_layers);
+  for (int l = 1; l + 1 < t.n_layers; ++l)
+    if (!std::isfinite(si.thick[l]) || si.thick[l] < 0) { why = "invalid thickness"; return RCWA_ERR_INVALID; }
+  return RCWA_OK;
+}
+}  // namespace
+
 extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_stacks, const rcwa_point* pts,
                                 int n_pts, int n_exc, const rcwa_cplx* pxy, int precision, rcwa_plan** out) {
   if (!e || !out) return RCWA_ERR_INVALID;
   *out = nullptr;
   if (n_stacks <= 0 || !stacks || n_pts <= 0 || !pts || n_exc <= 0 || !pxy)
     return fail(e, RCWA_ERR_INVALID, "empty batch or null pointer");
-  if (precision != RCWA_PREC_FP64 && precision != RCWA_PREC_MIXED)
-    return fail(e, RCWA_ERR_INVALID, "unknown precision mode");
-  if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, RCWA_ERR_CUDA, "cudaSetDevice failed");
   std::vector<StackInfo> si;
   for (int s = 0; s < n_stacks; ++s) {
     std::string why;
@@ -410,6 +463,32 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
     if (rc) return fail(e, rc, "stack " + std::to_string(s) + ": " + why);
     si.push_back(make_stack_info(stacks[s]));
   }
+  return plan_create_impl(e, si, pts, n_pts, n_exc, pxy, precision, out);
+}
+
+extern "C" int rcwa_plan_create_tables(rcwa_engine* e, const rcwa_table_stack* stacks, int n_stacks,
+                                       const rcwa_point* pts, int n_pts, int n_exc, const rcwa_cplx* pxy,
+                                       int precision, rcwa_plan** out) {
+  if (!e || !out) return RCWA_ERR_INVALID;
+  *out = nullptr;
+  if (n_stacks <= 0 || !stacks || n_pts <= 0 || !pts || n_exc <= 0 || !pxy)
+    return fail(e, RCWA_ERR_INVALID, "empty batch or null pointer");
+  std::vector<StackInfo> si(n_stacks);
+  for (int s = 0; s < n_stacks; ++s) {
+    std::string why;
+    int rc = table_stack_info(stacks[s], si[s], why);
+    if (rc) return fail(e, rc, "stack " + std::to_string(s) + ": " + why);
+  }
+  return plan_create_impl(e, si, pts, n_pts, n_exc, pxy, precision, out);
+}
+
+namespace {
+int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcwa_point* pts, int n_pts, int n_exc,
+                     const rcwa_cplx* pxy, int precision, rcwa_plan** out) {
+  const int n_stacks = (int)si.size();
+  if (precision != RCWA_PREC_FP64 && precision != RCWA_PREC_MIXED)
+    return fail(e, RCWA_ERR_INVALID, "unknown precision mode");
+  if (cudaSetDevice(e->device) != cudaSuccess) return fail(e, RCWA_ERR_CUDA, "cudaSetDevice failed");
   for (int p = 0; p < n_pts; ++p) {
     const rcwa_point& q = pts[p];
     if (q.stack < 0 || q.stack >= n_stacks) return fail(e, RCWA_ERR_INVALID, "point stack index out of range");
@@ -433,11 +512,12 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
 
   // ---- inputs: stack arrays and per-point alpha/beta
   Layout il;
-  std::vector<size_t> cx_off(n_stacks), cy_off(n_stacks), eps_off(n_stacks);
+  std::vector<size_t> cx_off(n_stacks), cy_off(n_stacks), eps_off(n_stacks), f2d_off(n_stacks);
   for (int s = 0; s < n_stacks; ++s) {
     cx_off[s] = il.take(sizeof(double) * si[s].cx.size());
     cy_off[s] = il.take(sizeof(double) * si[s].cy.size());
     eps_off[s] = il.take(sizeof(cplx) * si[s].eps.size());
+    f2d_off[s] = il.take(sizeof(cplx) * si[s].f2d.size());
   }
   std::vector<size_t> ab_off(n_pts);
   for (int p = 0; p < n_pts; ++p) ab_off[p] = il.take(sizeof(cplx) * 2 * P->point_N[p]);
@@ -448,6 +528,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
       std::memcpy(h.data() + cx_off[s], si[s].cx.data(), sizeof(double) * si[s].cx.size());
       std::memcpy(h.data() + cy_off[s], si[s].cy.data(), sizeof(double) * si[s].cy.size());
       std::memcpy(h.data() + eps_off[s], si[s].eps.data(), sizeof(cplx) * si[s].eps.size());
+      if (!si[s].f2d.empty()) std::memcpy(h.data() + f2d_off[s], si[s].f2d.data(), sizeof(cplx) * si[s].f2d.size());
     }
     for (int p = 0; p < n_pts; ++p) alpha_beta(si[pts[p].stack], pts[p].kx0, pts[p].ky0, (cplx*)(h.data() + ab_off[p]));
     if (cudaMemcpy(P->inputs.p, h.data(), il.off, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -612,6 +693,8 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         jobs[j].fe22 = W_(c.fe22) + NN * j;
         jobs[j].fe33 = W_(c.fe33) + NN * j;
         jobs[j].tab = W_(c.tab) + c.tab_elems * j;
+        jobs[j].f2d = si[s].tables ? (const cplx*)(inb + f2d_off[s]) + (size_t)(l - 1) * (2 * nx - 1) * (2 * ny - 1)
+                                   : nullptr;
       }
       // ConvJob array lives in the workspace (uploaded by a memcpy step)
       const size_t jobs_meta = meta.add_vec(jobs);
@@ -823,7 +906,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         const int k = (int)part.size();
         if (k == 0) continue;
         // points whose products run in 3xTF32 first, the FP64 ones after them
-        const bool tc_plan = precision == RCWA_PREC_MIXED && c.prod == 0;
+        const bool tc_plan = precision == RCWA_PREC_MIXED && c.prod != 1;
         std::stable_partition(part.begin(), part.end(), [&](int lp) { return tc_plan && !c.fp64_pt[lp]; });
         int kt = 0;
         for (int lp : part) kt += (tc_plan && !c.fp64_pt[lp]) ? 1 : 0;
@@ -904,6 +987,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
         int* tcerr = P->dTcErr;
         int* tcscale = P->dTcScale;
         const int lu_if = c.lu_if, lu_tau = c.lu_tau;
+        const int tile_n = c.prod == 2 ? 256 : 128;
         P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
           // the cascade products: items [0, kt) in 3xTF32 on tcgen05, the
           // rest on the FP64 tensor path
@@ -912,7 +996,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
             if (kt > 0) {
               GemmArgs t = ga;
               t.batch = kt;
-              x = zgemm_tf32x3_batched(t, tcscale, tcerr, st);
+              x = zgemm_tf32x3_batched(t, tcscale, tcerr, st, tile_n);
             }
             if (x == cudaSuccess && kt < ga.batch) {
               GemmArgs f = ga;
@@ -1030,6 +1114,7 @@ extern "C" int rcwa_plan_create(rcwa_engine* e, const rcwa_stack* stacks, int n_
   *out = P.release();
   return RCWA_OK;
 }
+}  // namespace
 
 namespace {
 // The plan's launch sequence on stream st (status reset, then every step).
@@ -1199,6 +1284,19 @@ extern "C" void rcwa_plan_destroy(rcwa_plan* p) {
   if (!p) return;
   cudaSetDevice(p->e->device);
   delete p;
+}
+
+extern "C" int rcwa_engine_solve_tables(rcwa_engine* e, const rcwa_table_stack* stacks, int n_stacks,
+                                        const rcwa_point* pts, int n_pts, int n_exc, const rcwa_cplx* pxy,
+                                        int precision, double* R, double* T, double* ref_orders,
+                                        double* trn_orders, int* status) {
+  rcwa_plan* p = nullptr;
+  int rc = rcwa_plan_create_tables(e, stacks, n_stacks, pts, n_pts, n_exc, pxy, precision, &p);
+  if (rc) return rc;
+  rc = rcwa_plan_execute(p, nullptr);
+  if (rc == RCWA_OK) rc = rcwa_plan_results(p, R, T, ref_orders, trn_orders, status);
+  rcwa_plan_destroy(p);
+  return rc;
 }
 
 extern "C" int rcwa_engine_solve_batch(rcwa_engine* e, const rcwa_stack* stacks, int n_stacks, const rcwa_point* pts,

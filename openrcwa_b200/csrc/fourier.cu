@@ -64,6 +64,21 @@ __global__ void conv_tables_kernel(ConvJob* jobs, int nx, int ny, int max_ncx, i
   const double dy = J.cy[J.ncy - 1] - J.cy[0];
   const int PX = 2 * nx - 1, PY = 2 * ny - 1;
   const int hx = (PX - 1) / 2, hy = (PY - 1) / 2;
+  if (J.f2d) {
+    // a given Laurent table: copied; the strip tables stay identity / zero
+    for (int idx = threadIdx.x; idx < PX * PY; idx += blockDim.x) tab[L.f2d + idx] = J.f2d[idx];
+    for (int idx = threadIdx.x; idx < mys * PY; idx += blockDim.x) tab[L.fy + idx] = mkc(0.0, 0.0);
+    for (int idx = threadIdx.x; idx < mxs * PX; idx += blockDim.x) tab[L.fx + idx] = mkc(0.0, 0.0);
+    for (int idx = threadIdx.x; idx < mys * nx * nx; idx += blockDim.x) {
+      const int r = (idx / nx) % nx, c = idx % nx;
+      tab[L.tx + idx] = tab[L.txinv + idx] = mkc(r == c ? 1.0 : 0.0, 0.0);
+    }
+    for (int idx = threadIdx.x; idx < mxs * ny * ny; idx += blockDim.x) {
+      const int r = (idx / ny) % ny, c = idx % ny;
+      tab[L.ty + idx] = tab[L.tyinv + idx] = mkc(r == c ? 1.0 : 0.0, 0.0);
+    }
+    return;
+  }
   // strip indicators: fY[i][q] (y strip i), fX[i][p] (x strip i)
   for (int idx = threadIdx.x; idx < mys * PY; idx += blockDim.x) {
     const int i = idx / PY, q = idx % PY;
@@ -154,6 +169,7 @@ __global__ void __launch_bounds__(kGatherThreads) conv_gather_kernel(const ConvJ
   cplx* W22 = C11 + (size_t)nx * PY;         // [nx][mxs]
   cplx* TYs = W22 + (size_t)nx * mxs;        // [mxs][ny][ny] when staged
   const cplx* TY = ty_in_smem ? TYs : tab + L.tyinv;
+  const bool laurent = J.f2d != nullptr;  // all three matrices from the F2D table
   const int tid = threadIdx.x;
   for (int idx = tid; idx < nx * PY; idx += blockDim.x) {
     const int j = idx / PY, q = idx % PY;
@@ -176,6 +192,11 @@ __global__ void __launch_bounds__(kGatherThreads) conv_gather_kernel(const ConvJ
       const int j = c / ny, l = c - j * ny;
       const int t = j * PY + (n - l + ny - 1);
       if (J.fe33) J.fe33[row + c] = F33[t];
+      if (laurent) {
+        if (J.fe11) J.fe11[row + c] = F33[t];
+        if (J.fe22) J.fe22[row + c] = F33[t];
+        continue;
+      }
       if (J.fe11) J.fe11[row + c] = C11[t];
       if (J.fe22) {
         cplx acc = mkc(0.0, 0.0);

@@ -15,6 +15,10 @@ struct ConvJob {
   cplx* fe33;          // ContinuousXY rule
   // per-job table scratch (see conv_table_elems)
   cplx* tab;
+  // a caller-given 2D Laurent table ((2nx-1) x (2ny-1), row p = x order
+  // p-nx+1) instead of the cells: all three matrices are its block-Toeplitz
+  // matrix (the Laurent rule for every tensor); nullptr for cell layers
+  const cplx* f2d = nullptr;
 };
 
 // complex elements of table scratch needed by one job

@@ -1,6 +1,6 @@
 // 3xTF32 complex GEMM on tcgen05.
 //
-// One CTA (four warps) computes a 128 x 128 complex output tile.  For each
+// One CTA (four warps) computes a 128 x 128 (or 128 x 256) complex output tile.  For each
 // 8-deep K slab the CTA converts its FP64 operand tiles into eight TF32
 // planes in shared memory (A: re hi/lo, im hi/lo; B likewise), laid out as
 // K-major, unswizzled UMMA core matrices (8 rows x 16 bytes; 8-row groups
@@ -14,6 +14,8 @@
 // is refilled only after its last commit completed.  The two stages take
 // 64 KB, so two CTAs share an SM (512 tensor-memory columns) and overlap too.  The epilogue reads the accumulators with
 // tcgen05.ld (warp w owns rows 32w..32w+31) and writes alpha*acc + beta*C.
+// The accumulators restart every kTcKBlock of K, their block sums being added
+// into D in FP64, which bounds the FP32 accumulation error independently of K.
 // Every wait is bounded: a wait that runs out sets the error flag, waits
 // (bounded) for the MMAs in flight, frees the tensor memory and skips the
 // tile's stores.
@@ -23,30 +25,47 @@
 
 namespace {
 
-constexpr int kTcM = 128, kTcN = 128, kTcK = 8;
+// Tile: kTcM rows of D by N columns (N = 128 or 256, the tile-shape choice of
+// the engine's tuner).  A plane holds rows x kTcK TF32 values; the K-major
+// planes' leading byte offset (between 4-value K chunks) is rows x 16 bytes.
+constexpr int kTcM = 128, kTcK = 8;
 constexpr int kTcThreads = 128;
-constexpr int kPlaneFloats = kTcM * kTcK;                // 1024 floats = 4 KB
-constexpr int kLbo = 2048, kSbo = 128;                   // bytes
-constexpr size_t kTcSmem = 2 * 8 * kPlaneFloats * sizeof(float) + 64;  // two stages
-constexpr uint32_t kTmemCols = 256;
+constexpr int kPlaneA = kTcM * kTcK;                     // 1024 floats = 4 KB
+constexpr int kSbo = 128;                                // bytes between 8-row groups
+template <int N> struct TcTile {
+  static constexpr int kPlaneB = N * kTcK;
+  static constexpr int kStageFloats = 4 * kPlaneA + 4 * kPlaneB;
+  // two stages + barriers; the 256-wide tile takes all 512 tensor-memory
+  // columns of an SM, so it asks for enough shared memory to be alone there
+  static constexpr size_t kSmemUsed = 2 * kStageFloats * sizeof(float) + 64;
+  static constexpr size_t kSmem = N == 256 && kSmemUsed < 120 * 1024 ? 120 * 1024 : kSmemUsed;
+  static constexpr uint32_t kTmemCols = 2 * N;                              // Re and Im accumulators
+  static constexpr int kLboB = N * 16;
+  // instruction descriptor: D F32, A/B TF32, both K-major, N, M = 128
+  static constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+                                     ((uint32_t)(kTcM >> 4) << 24);
+  static constexpr uint32_t kIdescNegA = kIdesc | (1u << 13);
+};
+constexpr int kLboA = kTcM * 16;
 constexpr long kWaitLimit = 1L << 22;
-
-// instruction descriptor: D F32, A/B TF32, both K-major, N = 128, M = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
-                            ((uint32_t)(kTcM >> 4) << 24);
-constexpr uint32_t kIdescNegA = kIdesc | (1u << 13);
+// K-block of the FP32 accumulators: after every kTcKBlock of K the tensor-
+// memory sums are added into D in FP64 and the accumulators restart.  The
+// tensor cores' FP32 accumulation is not round-to-nearest: its error grows
+// with the number of MMAs accumulated (six per 8-deep K step), so bounding
+// that number bounds the product's error independently of K.
+constexpr int kTcKBlock = 128;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// byte offset of (row r, k) in a plane
-__device__ __forceinline__ int plane_off(int r, int k) {
-  return (k >> 2) * kLbo + (r >> 3) * kSbo + (r & 7) * 16 + (k & 3) * 4;
+// byte offset of (row r, k) in a plane whose K chunks are lbo bytes apart
+__device__ __forceinline__ int plane_off(int r, int k, int lbo) {
+  return (k >> 2) * lbo + (r >> 3) * kSbo + (r & 7) * 16 + (k & 3) * 4;
 }
 
 // shared-memory matrix descriptor (sm100 layout: start >> 4 at [0,14), LBO >> 4
 // at [16,30), SBO >> 4 at [32,46), version 1 at [46,48), no swizzle)
-__device__ __forceinline__ uint64_t make_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((kLbo >> 4) & 0x3FFF) << 16) |
+__device__ __forceinline__ uint64_t make_desc(uint32_t saddr, int lbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
          ((uint64_t)((kSbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
@@ -121,17 +140,72 @@ __global__ void tc_scale_kernel(GemmArgs g, int* exps) {
   }
 }
 
-__global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g, const int* exps, int* err) {
+// Accumulators -> D for one K-block (whole CTA; warp w reads tensor-memory
+// lanes 32w..32w+31, i.e. tile rows): the first block writes
+// alpha*acc*2^eAB + beta*C + gammaI*I, every later block adds alpha*acc*2^eAB
+// to D in FP64.
+template <int N>
+__device__ __forceinline__ void tc_epilogue(const GemmArgs& g, int b, int m0, int n0, uint32_t tRe, uint32_t tIm,
+                                            int eAB, bool first) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = m0 + 32 * warp + lane;
+  const uint32_t row_addr = (uint32_t)(32 * warp) << 16;
+  for (int cb = 0; cb < N; cb += 16) {
+    uint32_t re[16], im[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(re[0]), "=r"(re[1]), "=r"(re[2]), "=r"(re[3]), "=r"(re[4]), "=r"(re[5]), "=r"(re[6]), "=r"(re[7]),
+          "=r"(re[8]), "=r"(re[9]), "=r"(re[10]), "=r"(re[11]), "=r"(re[12]), "=r"(re[13]), "=r"(re[14]),
+          "=r"(re[15])
+        : "r"(tRe + row_addr + cb));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(im[0]), "=r"(im[1]), "=r"(im[2]), "=r"(im[3]), "=r"(im[4]), "=r"(im[5]), "=r"(im[6]), "=r"(im[7]),
+          "=r"(im[8]), "=r"(im[9]), "=r"(im[10]), "=r"(im[11]), "=r"(im[12]), "=r"(im[13]), "=r"(im[14]),
+          "=r"(im[15])
+        : "r"(tIm + row_addr + cb));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    if (m < g.M) {
+      cplx* Drow = (g.D ? g.D[b] : g.D0 + b * g.sD) + g.offD + (size_t)m * g.ldd;
+      const cplx* Crow =
+          (first && (g.beta.x != 0.0 || g.beta.y != 0.0)) ? g.C[b] + g.offC + (size_t)m * g.ldc : nullptr;
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = n0 + cb + j;
+        if (n < g.N) {
+          cplx v = cmul(g.alpha, mkc(ldexp((double)__uint_as_float(re[j]), eAB),
+                                     ldexp((double)__uint_as_float(im[j]), eAB)));
+          if (first) {
+            if (Crow) v = cfma(g.beta, Crow[n], v);
+            if (m == n) v = cadd(v, g.gammaI);
+          } else {
+            v = cadd(v, Drow[n]);
+          }
+          Drow[n] = v;
+        }
+      }
+    }
+  }
+}
+
+template <int N>
+__global__ void __launch_bounds__(kTcThreads, N == 128 ? 2 : 1) zgemm_tf32x3_kernel(GemmArgs g, const int* exps,
+                                                                                   int* err) {
+  using Tile = TcTile<N>;
+  constexpr int kPlaneB = Tile::kPlaneB;
+  constexpr int kLboB = Tile::kLboB;
+  constexpr uint32_t kTmemCols = Tile::kTmemCols;
+  constexpr uint32_t kIdesc = Tile::kIdesc, kIdescNegA = Tile::kIdescNegA;
   extern __shared__ __align__(1024) unsigned char tsm[];
   // two stages of eight planes (A: re hi, re lo, im hi, im lo; then B)
   float* planes = reinterpret_cast<float*>(tsm);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 2 * 8 * kPlaneFloats * sizeof(float));  // one per stage
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tsm + 2 * Tile::kStageFloats * sizeof(float));  // one per stage
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(mbar + 2);
   int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
 
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5;
   const int b = blockIdx.z;
-  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * kTcN;
+  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * N;
   const cplx* A = (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
   const cplx* B = (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB;
   const uint32_t mb0 = smem_u32(mbar), mb1 = smem_u32(mbar + 1);
@@ -156,7 +230,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
-  const uint32_t tRe = tmem, tIm = tmem + kTcN;
+  const uint32_t tRe = tmem, tIm = tmem + N;
 
   // slab i goes to stage i % 2; before stage s is refilled, the MMAs of slab
   // i - 2 (its previous contents) must have completed.  The conversion of
@@ -164,6 +238,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
   uint32_t phase[2] = {0u, 0u};
   int pending[2] = {0, 0};  // uniform across the CTA
   int slab = 0;
+  int kblock0 = 0;          // first K of the accumulators' current block
   for (int k0 = 0; k0 < g.K; k0 += kTcK, ++slab) {
     const int st = slab & 1;
     const uint32_t mbs = st ? mb1 : mb0;
@@ -177,10 +252,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
     }
     __syncthreads();
     if (*s_fail) break;
-    float* P = planes + st * 8 * kPlaneFloats;
-    float *Arh = P, *Arl = P + kPlaneFloats, *Aih = P + 2 * kPlaneFloats, *Ail = P + 3 * kPlaneFloats;
-    float *Brh = P + 4 * kPlaneFloats, *Brl = P + 5 * kPlaneFloats, *Bih = P + 6 * kPlaneFloats,
-          *Bil = P + 7 * kPlaneFloats;
+    float* P = planes + st * Tile::kStageFloats;
+    float *Arh = P, *Arl = P + kPlaneA, *Aih = P + 2 * kPlaneA, *Ail = P + 3 * kPlaneA;
+    float* PB = P + 4 * kPlaneA;
+    float *Brh = PB, *Brl = PB + kPlaneB, *Bih = PB + 2 * kPlaneB, *Bil = PB + 3 * kPlaneB;
     // A: row tid, K chunks q (4 consecutive k each)
     {
       const int gm = m0 + tid;
@@ -195,16 +270,18 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
           split_tf32(v.x * sA, rh[j], rl[j]);
           split_tf32(v.y * sA, ih[j], il[j]);
         }
-        const int off = plane_off(tid, 4 * q);
+        const int off = plane_off(tid, 4 * q, kLboA);
         st_plane4(Arh, off, rh[0], rh[1], rh[2], rh[3]);
         st_plane4(Arl, off, rl[0], rl[1], rl[2], rl[3]);
         st_plane4(Aih, off, ih[0], ih[1], ih[2], ih[3]);
         st_plane4(Ail, off, il[0], il[1], il[2], il[3]);
       }
     }
-    // B: column tid (row of the K-major plane), K chunks q
-    {
-      const int gn = n0 + tid;
+    // B: columns tid + 128 c (rows of the K-major plane), K chunks q
+#pragma unroll
+    for (int cc = 0; cc < N / kTcThreads; ++cc) {
+      const int col = tid + kTcThreads * cc;
+      const int gn = n0 + col;
 #pragma unroll
       for (int q = 0; q < kTcK / 4; ++q) {
         float rh[4], rl[4], ih[4], il[4];
@@ -216,7 +293,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
           split_tf32(v.x * sB, rh[j], rl[j]);
           split_tf32(v.y * sB, ih[j], il[j]);
         }
-        const int off = plane_off(tid, 4 * q);
+        const int off = plane_off(col, 4 * q, kLboB);
         st_plane4(Brh, off, rh[0], rh[1], rh[2], rh[3]);
         st_plane4(Brl, off, rl[0], rl[1], rl[2], rl[3]);
         st_plane4(Bih, off, ih[0], ih[1], ih[2], ih[3]);
@@ -230,12 +307,12 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
       for (int ks = 0; ks < kTcK / 8; ++ks) {
-        const uint32_t off = (uint32_t)(2 * ks * kLbo);
-        const uint64_t arh = make_desc(smem_u32(Arh) + off), arl = make_desc(smem_u32(Arl) + off);
-        const uint64_t aih = make_desc(smem_u32(Aih) + off), ail = make_desc(smem_u32(Ail) + off);
-        const uint64_t brh = make_desc(smem_u32(Brh) + off), brl = make_desc(smem_u32(Brl) + off);
-        const uint64_t bih = make_desc(smem_u32(Bih) + off), bil = make_desc(smem_u32(Bil) + off);
-        const uint32_t acc = (k0 > 0 || ks > 0) ? 1u : 0u;
+        const uint32_t oa = (uint32_t)(2 * ks * kLboA), ob = (uint32_t)(2 * ks * kLboB);
+        const uint64_t arh = make_desc(smem_u32(Arh) + oa, kLboA), arl = make_desc(smem_u32(Arl) + oa, kLboA);
+        const uint64_t aih = make_desc(smem_u32(Aih) + oa, kLboA), ail = make_desc(smem_u32(Ail) + oa, kLboA);
+        const uint64_t brh = make_desc(smem_u32(Brh) + ob, kLboB), brl = make_desc(smem_u32(Brl) + ob, kLboB);
+        const uint64_t bih = make_desc(smem_u32(Bih) + ob, kLboB), bil = make_desc(smem_u32(Bil) + ob, kLboB);
+        const uint32_t acc = (k0 > kblock0 || ks > 0) ? 1u : 0u;
         mma_tf32(tRe, arh, brh, kIdesc, acc);
         mma_tf32(tRe, arh, brl, kIdesc, 1u);
         mma_tf32(tRe, arl, brh, kIdesc, 1u);
@@ -252,6 +329,28 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
       mma_commit(mbs);
     }
     pending[st] = 1;
+    if (k0 + kTcK < g.K && k0 + kTcK - kblock0 >= kTcKBlock) {
+      // end of a K-block: wait for its MMAs, add the accumulators into D in
+      // FP64, and let the next slab's MMAs start fresh accumulators
+      for (int s2 = 0; s2 < 2; ++s2) {
+        if (!pending[s2]) continue;
+        if (mbar_wait(s2 ? mb1 : mb0, phase[s2])) {
+          phase[s2] ^= 1u;
+          pending[s2] = 0;
+        } else {
+          *s_fail = 1;
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (*s_fail) break;
+      tc_epilogue<N>(g, b, m0, n0, tRe, tIm, eAB, kblock0 == 0);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncthreads();
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      kblock0 = k0 + kTcK;
+    }
   }
   // the outstanding slabs' MMAs (after a failure too: nothing may still write
   // the tensor memory or the planes when they are freed); the commit of the
@@ -264,41 +363,7 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const bool good = *s_fail == 0;
   if (!good && tid == 0) atomicExch(err, 1);
-  if (good) {
-    const int m = m0 + 32 * warp + lane;
-    const uint32_t row_addr = (uint32_t)(32 * warp) << 16;
-    for (int cb = 0; cb < kTcN; cb += 16) {
-      uint32_t re[16], im[16];
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(re[0]), "=r"(re[1]), "=r"(re[2]), "=r"(re[3]), "=r"(re[4]), "=r"(re[5]), "=r"(re[6]), "=r"(re[7]),
-            "=r"(re[8]), "=r"(re[9]), "=r"(re[10]), "=r"(re[11]), "=r"(re[12]), "=r"(re[13]), "=r"(re[14]),
-            "=r"(re[15])
-          : "r"(tRe + row_addr + cb));
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-          : "=r"(im[0]), "=r"(im[1]), "=r"(im[2]), "=r"(im[3]), "=r"(im[4]), "=r"(im[5]), "=r"(im[6]), "=r"(im[7]),
-            "=r"(im[8]), "=r"(im[9]), "=r"(im[10]), "=r"(im[11]), "=r"(im[12]), "=r"(im[13]), "=r"(im[14]),
-            "=r"(im[15])
-          : "r"(tIm + row_addr + cb));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-      if (m < g.M) {
-        cplx* Drow = (g.D ? g.D[b] : g.D0 + b * g.sD) + g.offD + (size_t)m * g.ldd;
-        const cplx* Crow = (g.beta.x != 0.0 || g.beta.y != 0.0) ? g.C[b] + g.offC + (size_t)m * g.ldc : nullptr;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int n = n0 + cb + j;
-          if (n < g.N) {
-            cplx v = cmul(g.alpha, mkc(ldexp((double)__uint_as_float(re[j]), eAB),
-                                       ldexp((double)__uint_as_float(im[j]), eAB)));
-            if (Crow) v = cfma(g.beta, Crow[n], v);
-            if (m == n) v = cadd(v, g.gammaI);
-            Drow[n] = v;
-          }
-        }
-      }
-    }
-  }
+  if (good) tc_epilogue<N>(g, b, m0, n0, tRe, tIm, eAB, kblock0 == 0);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
@@ -307,19 +372,24 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_kernel(GemmArgs g,
 
 }  // namespace
 
-cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st) {
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st, int tile_n) {
   if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
-  if (g.K <= 0 || g.transA || g.transB || g.s || !err || !scale_ws) return cudaErrorInvalidValue;
-  static SmemAttrOnce attr;
-  cudaError_t e = attr.ensure(zgemm_tf32x3_kernel, (int)kTcSmem);
+  if (g.K <= 0 || g.transA || g.transB || g.s || !err || !scale_ws || (tile_n != 128 && tile_n != 256))
+    return cudaErrorInvalidValue;
+  static SmemAttrOnce attr128, attr256;
+  cudaError_t e = tile_n == 128 ? attr128.ensure(zgemm_tf32x3_kernel<128>, (int)TcTile<128>::kSmem)
+                                : attr256.ensure(zgemm_tf32x3_kernel<256>, (int)TcTile<256>::kSmem);
   if (e != cudaSuccess) return e;
   // 0x80 bytes: every exponent starts at a very negative value
   e = cudaMemsetAsync(scale_ws, 0x80, sizeof(int) * 2 * g.batch, st);
   if (e != cudaSuccess) return e;
   tc_scale_kernel<<<dim3(16, g.batch, 2), 256, 0, st>>>(g, scale_ws);
   ++launch_counter();
-  dim3 grid((g.N + kTcN - 1) / kTcN, (g.M + kTcM - 1) / kTcM, g.batch);
-  zgemm_tf32x3_kernel<<<grid, kTcThreads, kTcSmem, st>>>(g, scale_ws, err);
+  dim3 grid((g.N + tile_n - 1) / tile_n, (g.M + kTcM - 1) / kTcM, g.batch);
+  if (tile_n == 128)
+    zgemm_tf32x3_kernel<128><<<grid, kTcThreads, TcTile<128>::kSmem, st>>>(g, scale_ws, err);
+  else
+    zgemm_tf32x3_kernel<256><<<grid, kTcThreads, TcTile<256>::kSmem, st>>>(g, scale_ws, err);
   ++launch_counter();
   return cudaGetLastError();
 }

@@ -11,4 +11,6 @@
 // scaled back exactly; scale_ws is device scratch of 2*batch ints.  err
 // (device int) is set to 1 if a tensor-core completion wait runs out; the
 // affected tile is then not written.
-cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st);
+// tile_n: columns of D per CTA, 128 (two CTAs per SM) or 256 (one CTA per SM,
+// every converted A slab serves twice the columns).
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st, int tile_n = 128);

@@ -12,6 +12,7 @@
 // No counterpart in the reference; the engine's plain FP64 solve is the
 // surrogate's fallback and the reference for its error (host side,
 // openrcwa_b200/surrogate.py).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -520,6 +521,92 @@ int rcwa_mlp_set_params(rcwa_mlp* m, const float* params) {
   if (cudaSetDevice(m->e->device) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return RCWA_ERR_CUDA;
   return cudaMemcpy(m->params, params, sizeof(float) * m->n_params, cudaMemcpyHostToDevice) == cudaSuccess
              ? RCWA_OK : RCWA_ERR_CUDA;
+}
+
+}  // extern "C"
+
+namespace {
+// Squared distance from every query row to its nearest row of the training
+// set (both n_in features, FP32).  A block takes 128 queries and a slice of
+// the training rows, staged through shared memory 128 rows at a time; the
+// per-slice minima combine by atomicMin on the (non-negative) float bits.
+// With skip_self, a training row at distance exactly 0 (the query itself,
+// for leave-one-out distances of training rows) is not counted.
+constexpr int kNnThreads = 128;
+constexpr int kNnMaxDim = 32;
+
+__global__ void __launch_bounds__(kNnThreads) nn_distance_kernel(const float* __restrict__ ref, int n_ref,
+                                                                 const float* __restrict__ q, int n_q, int dim,
+                                                                 int slice, int skip_self, unsigned* d2_bits) {
+  __shared__ float tile[kNnThreads * kNnMaxDim];
+  const int qi = blockIdx.x * kNnThreads + threadIdx.x;
+  float x[kNnMaxDim];
+#pragma unroll
+  for (int k = 0; k < kNnMaxDim; ++k) x[k] = (qi < n_q && k < dim) ? q[(size_t)qi * dim + k] : 0.0f;
+  float best = INFINITY;
+  const int r0 = blockIdx.y * slice, r1 = min(n_ref, r0 + slice);
+  for (int t0 = r0; t0 < r1; t0 += kNnThreads) {
+    const int rows = min(kNnThreads, r1 - t0);
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < rows * dim; idx += kNnThreads) tile[idx] = ref[(size_t)t0 * dim + idx];
+    __syncthreads();
+    for (int r = 0; r < rows; ++r) {
+      float d = 0.0f;
+#pragma unroll
+      for (int k = 0; k < kNnMaxDim; ++k)
+        if (k < dim) {
+          const float e = x[k] - tile[r * dim + k];
+          d = fmaf(e, e, d);
+        }
+      if (!(skip_self && d == 0.0f)) best = fminf(best, d);
+    }
+  }
+  if (qi < n_q) atomicMin(&d2_bits[qi], __float_as_uint(best));
+}
+}  // namespace
+
+extern "C" {
+
+// Nearest-neighbour distances of query rows Q [n][n_in] (host, the features
+// the network was trained on) to the training set of rcwa_mlp_set_data: d2[n]
+// receives the squared Euclidean distance to the nearest training row.  With
+// skip_self, distances of exactly 0 are ignored (queries that are training
+// rows get their leave-one-out distance).  The surrogate's hull test.
+int rcwa_mlp_nn_distance(rcwa_mlp* m, const float* Q, int n, int skip_self, float* d2) {
+  if (!m || !Q || !d2 || n < 1) return RCWA_ERR_INVALID;
+  if (!m->X || m->n_data < 1) return mlp_fail(m, RCWA_ERR_INVALID, "no training set");
+  if (m->n_in > kNnMaxDim) return mlp_fail(m, RCWA_ERR_UNSUPPORTED, "more than 32 input features");
+  if (cudaSetDevice(m->e->device) != cudaSuccess) return RCWA_ERR_CUDA;
+  float* dq = nullptr;
+  unsigned* dd = nullptr;
+  if (!dalloc(&dq, (size_t)n * m->n_in) || !dalloc(&dd, (size_t)n)) {
+    cudaFree(dq);
+    return mlp_fail(m, RCWA_ERR_NOMEM, "query allocation failed");
+  }
+  cudaStream_t st = m->e->stream;
+  int rc = RCWA_OK;
+  if (cudaMemcpyAsync(dq, Q, sizeof(float) * n * m->n_in, cudaMemcpyHostToDevice, st) != cudaSuccess ||
+      cudaMemsetAsync(dd, 0x7f, sizeof(unsigned) * n, st) != cudaSuccess) {
+    rc = RCWA_ERR_CUDA;
+  } else {
+    // training rows split into slices so that the grid covers the SMs
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->e->device);
+    const int qblocks = (n + kNnThreads - 1) / kNnThreads;
+    const int nslices = std::max(1, std::min((m->n_data + kNnThreads - 1) / kNnThreads, (4 * sms + qblocks - 1) / qblocks));
+    const int slice = ((m->n_data + nslices - 1) / nslices + kNnThreads - 1) / kNnThreads * kNnThreads;
+    const int ns = (m->n_data + slice - 1) / slice;
+    nn_distance_kernel<<<dim3(qblocks, ns), kNnThreads, 0, st>>>(m->X, m->n_data, dq, n, m->n_in, slice,
+                                                                 skip_self ? 1 : 0, dd);
+    ++launch_counter();
+    if (cudaGetLastError() != cudaSuccess ||
+        cudaMemcpyAsync(d2, dd, sizeof(float) * n, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      rc = RCWA_ERR_CUDA;
+  }
+  cudaFree(dq);
+  cudaFree(dd);
+  return rc;
 }
 
 int rcwa_mlp_set_data(rcwa_mlp* m, const float* X, const float* Y, int n) {

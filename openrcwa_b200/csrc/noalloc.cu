@@ -24,7 +24,7 @@ constexpr size_t kPtrBytes = 2 * sizeof(void*) * kMaxBatch;
 size_t scratch_bytes_needed(int n, int batch) { return kPtrBytes + zgeev_workspace_bytes(n) * (size_t)batch; }
 
 // pointer tables (A and VR per matrix) followed by the eigensolver workspace;
-// sized for the largest accepted call: n = 64, batch = 64 (about 22 MB)
+// sized for the largest accepted call: n = 64, batch = 64 (about 38 MB)
 constexpr size_t kScratchBytes = kPtrBytes + zgeev_workspace_bytes(kMaxN) * kMaxBatch;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];

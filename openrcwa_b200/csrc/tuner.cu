@@ -109,7 +109,7 @@ int tune_candidates(int op, int n, int* out) {
       if (n < kSchurCrossover || n >= kSchurTuneMax) { out[0] = kSchurCrossover; return 1; }
       for (int i = 0; i < kTuneMaxCand; ++i) out[i] = kSchurCand[i];
       return kTuneMaxCand;
-    case kTuneProduct: out[0] = 0; out[1] = 1; return 2;
+    case kTuneProduct: out[0] = 0; out[1] = 1; out[2] = 2; return 3;
     default: return 0;
   }
 }
@@ -220,7 +220,9 @@ cudaError_t tune_measure(rcwa_engine* e, int op, int n, int batch, TuneEntry& ou
       auto run = [&](int b) {
         GemmArgs x = g;
         x.batch = b;
-        return out.cand[c] == 0 ? zgemm_tf32x3_batched(x, scale.as<int>(), tcerr.as<int>(), st) : zgemm_batched(x, st);
+        return out.cand[c] == 1 ? zgemm_batched(x, st)
+                                : zgemm_tf32x3_batched(x, scale.as<int>(), tcerr.as<int>(), st,
+                                                       out.cand[c] == 2 ? 256 : 128);
       };
       double warm = 0.0;
       err = timed(nop, [&]() { return run(1); }, 1, warm);

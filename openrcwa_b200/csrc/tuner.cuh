@@ -5,8 +5,9 @@
 //                 by panel over all SMs)
 //   kTuneSchur    Schur crossover: active blocks below it use single-shift
 //                 sweeps, larger ones multishift sweeps with early deflation
-//   kTuneProduct  cascade products of mixed plans (0: 3xTF32 on tcgen05,
-//                 1: FP64 tensor path)
+//   kTuneProduct  cascade products of mixed plans and their tile shape
+//                 (0: 3xTF32 on tcgen05, 128 x 128 tiles; 1: FP64 tensor path;
+//                 2: 3xTF32 on tcgen05, 128 x 256 tiles)
 // The table is host data (thread-safe); measuring needs the engine's device.
 #pragma once
 #include <map>

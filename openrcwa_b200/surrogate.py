@@ -1,4 +1,4 @@
-"""Learned surrogate of the RCWA efficiencies, with the FP64 solve as its
+"""Learned surrogate of the RCWA efficiencies, with the engine's solve as its
 fallback and the reference for its error.
 
 The network (rcwa_mlp_*: GPU training and tensor-core inference) maps eleven
@@ -9,11 +9,18 @@ of the 25 lowest orders (m, n in [-2, 2]^2) and the total R and T (52 outputs).
 Training data come from this engine's FP64 solve.  A query goes to the
 engine instead of the network when
 
-* a parameter lies outside the training set's range (the hull check),
+* it lies outside the training data (the hull check): a parameter outside the
+  training set's range, or a squared feature-space distance to the nearest
+  training row above the ``hull_quantile`` of the training rows' own
+  leave-one-out nearest-neighbour distances (a GPU brute-force search),
 * the stack is lossless (Im eps1 = 0, eps2 real) and the predicted total
   R + T misses 1 by more than ``energy_tol`` (1e-3),
 * it is drawn for the random audit (``audit`` fraction, 2% by default); the
   audited rows report the network's error against the solve.
+
+Fallbacks and audits run through the mixed-precision engine by default
+(``fallback_precision``): within 1e-4 of the FP64 solve and faster, which is
+what lets a surrogate with a 2% audit approach a 100x speed-up at all.
 """
 from __future__ import annotations
 
@@ -22,7 +29,7 @@ from typing import Dict, Optional
 
 import numpy as np
 
-from .abi import Engine, Mlp, RCWA_PREC_FP64
+from .abi import Engine, Mlp, RCWA_PREC_FP64, RCWA_PREC_MIXED
 from .workloads import pol_vectors, rect_stack
 
 PARAMS = ("fill_x", "fill_y", "thickness", "eps_re", "eps_im", "eps2", "lambda", "theta", "phi", "period_x",
@@ -77,11 +84,14 @@ def solve(eng: Engine, P: np.ndarray, nh: int, chunk: int = 512, precision: int 
 
 
 class Surrogate:
-    def __init__(self, eng: Engine, nh: int, hidden: int = 256, layers: int = 4, seed: int = 0):
+    def __init__(self, eng: Engine, nh: int, hidden: int = 256, layers: int = 4, seed: int = 0,
+                 fallback_precision: int = RCWA_PREC_MIXED):
         self.eng, self.nh = eng, nh
         self.net = Mlp(eng, len(PARAMS), hidden, layers, N_OUT, seed=seed)
         self.lo: Optional[np.ndarray] = None
         self.hi: Optional[np.ndarray] = None
+        self.fallback_precision = fallback_precision
+        self.hull_d2: Optional[float] = None
 
     def features(self, P: np.ndarray) -> np.ndarray:
         """Parameters scaled to [-1, 1] over the training range."""
@@ -89,11 +99,17 @@ class Surrogate:
         return (2.0 * (P - self.lo) / span - 1.0).astype(np.float32)
 
     def fit(self, P: np.ndarray, Y: np.ndarray, epochs: int = 60, batch: int = 256, lr: float = 2e-3,
-            seed: int = 0) -> np.ndarray:
+            seed: int = 0, hull_quantile: float = 0.999, hull_sample: int = 8192) -> np.ndarray:
         """Train on parameter rows P and their solved targets Y; returns the
-        per-epoch loss."""
+        per-epoch loss.  The hull threshold is the ``hull_quantile`` of the
+        leave-one-out nearest-neighbour distances of ``hull_sample`` training
+        rows."""
         self.lo, self.hi = P.min(axis=0), P.max(axis=0)
-        self.net.set_data(self.features(P), Y.astype(np.float32))
+        F = self.features(P)
+        self.net.set_data(F, Y.astype(np.float32))
+        rng = np.random.default_rng(seed)
+        pick = rng.choice(len(F), size=min(hull_sample, len(F)), replace=False)
+        self.hull_d2 = float(np.quantile(self.net.nn_distance(F[pick], skip_self=True), hull_quantile))
         return self.net.train(epochs, batch, lr, seed)
 
     def predict(self, P: np.ndarray) -> np.ndarray:
@@ -108,6 +124,8 @@ class Surrogate:
         Y = self.predict(P)
         src = np.full(P.shape[0], SOURCE_NET)
         outside = np.any((P < self.lo) | (P > self.hi), axis=1)
+        if self.hull_d2 is not None:
+            outside |= self.net.nn_distance(self.features(P)) > self.hull_d2
         src[outside] = SOURCE_HULL
         lossless = (P[:, 4] == 0.0)
         bad_energy = lossless & (np.abs(Y[:, 50] + Y[:, 51] - 1.0) > energy_tol) & (src == SOURCE_NET)
@@ -118,7 +136,7 @@ class Surrogate:
         fall = src != SOURCE_NET
         audit_err = np.zeros(0)
         if np.any(fall):
-            Ys = solve(self.eng, P[fall], self.nh)
+            Ys = solve(self.eng, P[fall], self.nh, chunk=4096, precision=self.fallback_precision)
             idx = np.nonzero(fall)[0]
             aud = src[idx] == SOURCE_AUDIT
             audit_err = np.max(np.abs(Y[idx[aud]] - Ys[aud]), axis=1) if np.any(aud) else np.zeros(0)

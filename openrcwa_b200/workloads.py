@@ -11,7 +11,7 @@ import math
 
 import numpy as np
 
-from .abi import Stack
+from .abi import Stack, TableStack
 
 PI = 3.1415926535897932
 
@@ -124,6 +124,49 @@ def uneven_batch(seed=0, n_instances=4096, nh_range=(3, 15), max_layers=10, peri
         pts.append((i, lam, k0 * math.sin(math.radians(th)), 0.0))
         pxy.append(pol_vectors(th, 0.0))
     return stacks, np.array(pts), np.array(pxy, dtype=complex)
+
+
+def disk_laurent_table(Lx, Ly, radius, center, eps1, eps2, nH):
+    """Laurent coefficients of a circular pillar (eps1 in a disk of the given
+    radius and center, eps2 elsewhere) for 2nH+1 orders per axis:
+    F[m + 2nH, n + 2nH] = (1/(Lx Ly)) integral eps exp(-i (gx x + gy y)) =
+    eps2 delta_mn + (eps1 - eps2) pi R^2 (2 J1(g R)/(g R)) exp(-i g.c)/(Lx Ly),
+    g = 2 pi (m/Lx, n/Ly) (the Fourier transform of a disk, an Airy pattern)."""
+    from scipy.special import j1
+    m = np.arange(-2 * nH, 2 * nH + 1)[:, None]
+    n = np.arange(-2 * nH, 2 * nH + 1)[None, :]
+    gx, gy = 2 * PI * m / Lx, 2 * PI * n / Ly
+    gr = np.hypot(gx, gy) * radius
+    safe = np.where(gr > 0, gr, 1.0)
+    airy = np.where(gr > 0, 2.0 * j1(safe) / safe, 1.0)
+    F = (eps1 - eps2) * PI * radius * radius * airy * np.exp(-1j * (gx * center[0] + gy * center[1])) / (Lx * Ly)
+    F[2 * nH, 2 * nH] += eps2
+    return F.astype(np.complex128)
+
+
+def circular_pillars(seed=0, nH=25, n_lambda=32, n_layers=20, period=4e-7):
+    """Large-order single structure: n_layers circular-pillar layers (one disk
+    per layer centred in the cell, radius/period ~U(0.2, 0.45), thickness
+    ~U(20, 100) nm, eps1 alternating 4.0 and 2.1+0.01i, eps2 = 1) between a
+    superstrate of eps 1 and a substrate of 2.25, period x period cells
+    (400 nm), 2nH+1 orders per axis; n_lambda wavelengths 500-900 nm at normal
+    incidence, TE and TM.  The layers' Laurent tables are the closed-form disk
+    transform.  Returns ([TableStack], points, pxy)."""
+    rng = np.random.default_rng(seed)
+    f2d, thick = [], [0.0]
+    for k in range(n_layers):
+        r = rng.uniform(0.2, 0.45) * period
+        d = rng.uniform(20e-9, 100e-9)
+        e1 = 4.0 if k % 2 == 0 else complex(2.1, 0.01)
+        f2d.append(disk_laurent_table(period, period, r, (0.5 * period, 0.5 * period), e1, 1.0, nH))
+        thick.append(d)
+    thick.append(0.0)
+    st = TableStack(nH, nH, period, period, np.array([1.0, 2.25], dtype=complex), np.array(f2d), thick)
+    lam = np.linspace(500e-9, 900e-9, n_lambda)
+    te, tm = pol_vectors(0.0, 0.0)
+    pts = np.array([(0, l, 0.0, 0.0) for l in lam])
+    pxy = np.array([[te, tm]] * len(lam), dtype=complex)
+    return [st], pts, pxy
 
 
 def batch_slice(points, pxy, start, count):

@@ -200,15 +200,22 @@ def _solve(A, B, lstsq=False):
     return np.linalg.solve(A, B)
 
 
-def wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq=False):
+def wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq=False, f2d=None):
     """Layer::waveEqnCoeff, non-magnetic branch (rcwa/Layer.cpp:75-253).
 
     Kx, Ky are the dense diagonal matrices of RCWASolver::evaluateKMatrices
     (rcwa/RCWASolver.cpp:150-185, PML disabled).  Returns (P, Q, fe11, fe22, fe33).
+    With f2d (a (2nx-1) x (2ny-1) Laurent table, e.g. circle_fourier2d), the
+    three convolution matrices are its block-Toeplitz matrix (the Laurent rule
+    for every tensor; the reference has no such layer, it staircases curved
+    shapes, rcwa/RCWADriver.cpp:19-37).
     """
-    fe11 = fourier2d(cx, cy, eps, nx, ny, DiscontinuousX)  # :102-105
-    fe22 = fourier2d(cx, cy, eps, nx, ny, DiscontinuousY)  # :109-112
-    fe33 = fourier2d(cx, cy, eps, nx, ny, ContinuousXY)    # :116-119
+    if f2d is not None:
+        fe11 = fe22 = fe33 = block_toeplitz_dense(np.asarray(f2d, dtype=np.complex128))
+    else:
+        fe11 = fourier2d(cx, cy, eps, nx, ny, DiscontinuousX)  # :102-105
+        fe22 = fourier2d(cx, cy, eps, nx, ny, DiscontinuousY)  # :109-112
+        fe33 = fourier2d(cx, cy, eps, nx, ny, ContinuousXY)    # :116-119
     N = nx * ny
     Kx = np.diag(np.asarray(alpha, dtype=np.complex128))
     Ky = np.diag(np.asarray(beta, dtype=np.complex128))
@@ -268,9 +275,9 @@ class LayerSolution:
     Q: np.ndarray = None
 
 
-def layer_solve(cx, cy, eps, alpha, beta, lam, nx, ny, keep=False, lstsq=False):
+def layer_solve(cx, cy, eps, alpha, beta, lam, nx, ny, keep=False, lstsq=False, f2d=None):
     """Layer::solve (rcwa/Layer.cpp:255-273)."""
-    P, Q, fe11, fe22, fe33 = wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq)
+    P, Q, fe11, fe22, fe33 = wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq, f2d)
     PQ, W, V, keff, ev = wave_equation_solve(P, Q)
     k0 = 2 * PI / lam
     sol = LayerSolution(W=W, V=V, gamma=keff / k0, eigenvalues=ev)
@@ -309,6 +316,7 @@ class OracleLayer:
     cx: np.ndarray
     cy: np.ndarray
     eps: np.ndarray  # (len(cy)-1, len(cx)-1)
+    f2d: np.ndarray = None  # optional Laurent table replacing the cells' three rules
 
 
 class RCWASolver:
@@ -355,7 +363,7 @@ class RCWASolver:
         self.alpha, self.beta = alpha_beta(self.nx, self.ny, self.Lx, self.Ly, self.kx0, self.ky0)
         # solveLayers (:194-210): every layer type, half-spaces included
         self.sol = [layer_solve(L.cx, L.cy, L.eps, self.alpha, self.beta, lam, self.nx, self.ny,
-                                keep=self.keep, lstsq=self.lstsq) for L in self.layers]
+                                keep=self.keep, lstsq=self.lstsq, f2d=L.f2d) for L in self.layers]
         self._interfaces(stack)
         self._scatter_matrix(stack, thickness)
 

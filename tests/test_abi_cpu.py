@@ -134,3 +134,14 @@ def test_surrogate_sampler_ranges():
     assert P.shape == (5000, len(surrogate.PARAMS))
     lo, hi = surrogate.RANGES[:, 0], surrogate.RANGES[:, 1]
     assert np.all(P >= lo) and np.all(P <= hi)
+
+
+def test_circular_pillar_tables_match_the_oracle_closed_form():
+    import oracle.rcwa_oracle as ro
+    from openrcwa_b200 import workloads
+    L, R = 4e-7, 1.3e-7
+    F = workloads.disk_laurent_table(L, L, R, (0.5 * L, 0.5 * L), complex(2.1, 0.01), 1.0, 6)
+    Fo = ro.circle_fourier2d(L, L, R, (0.5 * L, 0.5 * L), complex(2.1, 0.01), 1.0, 13, 13)
+    assert F.shape == (25, 25) and np.max(np.abs(F - Fo)) < 1e-14
+    st, pts, pxy = workloads.circular_pillars(seed=0, nH=3, n_lambda=4, n_layers=5)
+    assert st[0].f2d.shape == (5, 13, 13) and pts.shape == (4, 4) and st[0].N == 49

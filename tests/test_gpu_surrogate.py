@@ -56,8 +56,42 @@ def test_fallback_rules(trained):
     src, Yq = r["source"], r["Y"]
     assert np.all(src[:20] == sg.SOURCE_HULL)
     fell = src != sg.SOURCE_NET
-    Ys = sg.solve(eng, Pq[fell], sur.nh)
+    # fallbacks come from the mixed-precision solve, within 1e-4 of FP64
+    Ys = sg.solve(eng, Pq[fell], sur.nh, chunk=4096, precision=o.RCWA_PREC_MIXED)
     assert np.max(np.abs(Yq[fell] - Ys)) < 1e-12
+    assert np.max(np.abs(Yq[fell] - sg.solve(eng, Pq[fell], sur.nh))) < 1e-4
     net_lossless = (src == sg.SOURCE_NET) & (Pq[:, 4] == 0.0)
     assert np.all(np.abs(Yq[net_lossless, 50] + Yq[net_lossless, 51] - 1.0) <= 1e-3)
     assert np.any(src == sg.SOURCE_AUDIT) and len(r["audit_err"]) == int(np.sum(src == sg.SOURCE_AUDIT))
+
+
+def test_hull_rule_flags_queries_far_from_the_training_data(trained):
+    # a training set on a diagonal band of the box: every parameter spans its
+    # full range, so the range check passes everywhere, but a query at the
+    # opposite corner of the box is far from every training row
+    eng, sur, P, Y, loss, rng = trained
+    lo, hi = sg.RANGES[:, 0], sg.RANGES[:, 1]
+    t = rng.random((4096, 1))
+    Pb = lo + (hi - lo) * np.clip(t + 0.03 * rng.standard_normal((4096, len(lo))), 0.0, 1.0)
+    Pb[:, 7] = lo[7] + (hi[7] - lo[7]) * t[:, 0]
+    band = sg.Surrogate(eng, sur.nh, hidden=32, layers=2, seed=2)
+    band.fit(Pb, sg.solve(eng, Pb, sur.nh, chunk=4096), epochs=1, batch=512, lr=1e-3, seed=5)
+    on_band = lo + (hi - lo) * np.clip(rng.random((32, 1)) + np.zeros((32, len(lo))), 0.05, 0.95)
+    off_band = lo + (hi - lo) * np.where(np.arange(len(lo)) % 2 == 0, 0.1, 0.9)[None, :].repeat(32, axis=0)
+    r = band.query(np.vstack([on_band, off_band]), audit=0.0)
+    assert np.all(r["source"][32:] == sg.SOURCE_HULL)
+    assert np.mean(r["source"][:32] == sg.SOURCE_NET) > 0.9
+    band.close()
+
+
+def test_audited_error_bounds_the_unaudited_rows(trained):
+    # the audit is a random sample of the network's answers: the largest of
+    # about 400 audited errors bounds all but the top 2% of the unaudited ones
+    # (it falls below that quantile with probability 0.98^400, about 3e-4)
+    eng, sur, P, Y, loss, rng = trained
+    Pq = sg.sample(8192, rng)
+    r = sur.query(Pq, audit=0.05, seed=7)
+    net = r["source"] == sg.SOURCE_NET
+    err = np.max(np.abs(r["Y"][net] - sg.solve(eng, Pq[net], sur.nh, chunk=4096)), axis=1)
+    assert len(r["audit_err"]) > 200
+    assert np.quantile(err, 0.98) <= np.max(r["audit_err"])

@@ -86,6 +86,28 @@ def test_mixed_plan_with_fp64_products_equals_fp64_plan(eng, case):
     assert np.array_equal(Rm, R6) and np.array_equal(Tm, T6)
 
 
+def test_wide_tensor_core_tiles_match_the_oracle(eng, case):
+    # product choice 2: 3xTF32 on 128 x 256 output tiles (one CTA per SM)
+    st, pts, pxy, ref = case
+    n = 2 * st.N
+    t = o.Tuner()
+    t.set("product", n, len(pts), 2)
+    eng.set_tuner(t, o.RCWA_TUNING_TABLE)
+    try:
+        plan = eng.plan([st], pts, pxy, o.RCWA_PREC_MIXED)
+        assert plan.schedule()[0]["product"] == 2
+        plan.execute()
+        R, T, ref_o, trn_o, status = plan.results(orders=True)
+        plan.close()
+        R0, T0, _, _, s0 = eng.solve_batch([st], pts, pxy, orders=False, precision=o.RCWA_PREC_MIXED)
+    finally:
+        eng.set_tuner(None, o.RCWA_TUNING_OFF)
+    assert not np.any(status) and not np.any(s0)
+    for p, r in enumerate(ref):
+        assert np.max(np.abs(R[p] - r["R"])) < 1e-4 and np.max(np.abs(T[p] - r["T"])) < 1e-4
+    assert np.max(np.abs(R - R0)) < 1e-5 and np.max(np.abs(T - T0)) < 1e-5
+
+
 def test_auto_mode_records_and_stays_exact(eng, case, tmp_path):
     st, pts, pxy, ref = case
     n = 2 * st.N

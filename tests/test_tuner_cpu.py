@@ -20,7 +20,7 @@ def tuner():
 def test_candidates(tuner):
     o, t = tuner
     assert t.candidates("lu", 882) == [0, 1]
-    assert t.candidates("product", 98) == [0, 1]
+    assert t.candidates("product", 98) == [0, 1, 2]
     assert t.candidates("schur", 242) == [64, 96, 128, 192]
     assert t.candidates("schur", 882) == [64]  # large matrices: multishift phase dominates
     assert t.candidates("schur", 40) == [64]   # below the crossover: single-shift only
