@@ -327,6 +327,7 @@ struct ChunkWork {
   std::vector<int> points;                        // global point index
   size_t hW0 = 0, hV0 = 0, hWL = 0, hVL = 0, hg0 = 0, hgL = 0;
   size_t Rud = 0, Tdd = 0, F = 0, G = 0, tau = 0, IE = 0, IH = 0, WLU = 0, VLU = 0, pipiv = 0, pinfo = 0;
+  size_t planes = 0, planes_bytes = 0;  // mixed plans: pre-split TF32 planes of one batched product
   size_t total = 0;
   // mixed plans: per chunk point, whether its products stay FP64 (its stack
   // has a layer with Re(eps) < 0, whose cascade the 3xTF32 products cannot
@@ -339,7 +340,7 @@ struct ChunkWork {
 
 }  // namespace
 
-static size_t chunk_layout(ChunkWork& c, const std::vector<StackInfo>& stacks, int N) {
+static size_t chunk_layout(ChunkWork& c, const std::vector<StackInfo>& stacks, int N, bool mixed) {
   const size_t n = 2 * (size_t)N;
   const size_t NN = (size_t)N * N, nn = n * n;
   const size_t cs = sizeof(cplx);
@@ -388,15 +389,18 @@ static size_t chunk_layout(ChunkWork& c, const std::vector<StackInfo>& stacks, i
   c.VLU = L.take(cs * nn * np);
   c.pipiv = L.take(sizeof(int) * n * 3 * np);
   c.pinfo = L.take(sizeof(int) * 3 * np);
+  c.planes_bytes = mixed ? zgemm_tf32x3_planes_bytes((int)n, (int)n, (int)n, (int)np) : 0;
+  c.planes = L.take(std::max<size_t>(c.planes_bytes, 16));
   c.total = L.off;
   return L.off;
 }
 
-static size_t chunk_bytes_per_point(int N, int Lp) {
+static size_t chunk_bytes_per_point(int N, int Lp, bool mixed) {
   const double n = 2.0 * N;
   const double nn = n * n * sizeof(cplx), NN = (double)N * N * sizeof(cplx);
   const double per_job = 2 * NN + 3 * nn + zgeev_workspace_bytes((int)n) + 4 * NN;
-  return (size_t)(13 * nn + per_job * std::max(Lp - 2, 0));
+  const double planes = mixed ? (double)zgemm_tf32x3_planes_bytes((int)n, (int)n, (int)n, 1) : 0.0;
+  return (size_t)(13 * nn + planes + per_job * std::max(Lp - 2, 0));
 }
 
 namespace {
@@ -590,7 +594,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       used = 0;
     };
     for (int p : g.second) {
-      const size_t need = chunk_bytes_per_point(N, si[pts[p].stack].L);
+      const size_t need = chunk_bytes_per_point(N, si[pts[p].stack].L, precision == RCWA_PREC_MIXED);
       if (!cur.points.empty() && (used + need > budget || cur.points.size() >= 1024)) flush();
       cur.points.push_back(p);
       used += need;
@@ -630,7 +634,8 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
     P->sched.push_back({n, np, c.lu_if, c.lu_tau, c.ms_min, c.prod});
   }
   size_t wbytes = 0;
-  for (size_t ci = 0; ci < chunks.size(); ++ci) wbytes = std::max(wbytes, chunk_layout(chunks[ci], si, chunk_N[ci]));
+  for (size_t ci = 0; ci < chunks.size(); ++ci)
+    wbytes = std::max(wbytes, chunk_layout(chunks[ci], si, chunk_N[ci], precision == RCWA_PREC_MIXED));
   const size_t wneed = std::max<size_t>(wbytes, 256);
   if (!e->work_cache_busy) {
     if (e->work_cache_bytes < wneed) {
@@ -988,6 +993,8 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         int* tcscale = P->dTcScale;
         const int lu_if = c.lu_if, lu_tau = c.lu_tau;
         const int tile_n = c.prod == 2 ? 256 : 128;
+        float* planes = (float*)(wb + c.planes);
+        const size_t planes_bytes = c.planes_bytes;
         P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
           // the cascade products: items [0, kt) in 3xTF32 on tcgen05, the
           // rest on the FP64 tensor path
@@ -996,7 +1003,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
             if (kt > 0) {
               GemmArgs t = ga;
               t.batch = kt;
-              x = zgemm_tf32x3_batched(t, tcscale, tcerr, st, tile_n);
+              x = zgemm_tf32x3_batched(t, tcscale, tcerr, st, tile_n, planes, planes_bytes);
             }
             if (x == cudaSuccess && kt < ga.batch) {
               GemmArgs f = ga;

@@ -19,6 +19,7 @@
 // Every wait is bounded: a wait that runs out sets the error flag, waits
 // (bounded) for the MMAs in flight, frees the tensor memory and skips the
 // tile's stores.
+#include <algorithm>
 #include <cstdint>
 
 #include "gemm_tc.cuh"
@@ -53,7 +54,10 @@ constexpr long kWaitLimit = 1L << 22;
 // tensor cores' FP32 accumulation is not round-to-nearest: its error grows
 // with the number of MMAs accumulated (six per 8-deep K step), so bounding
 // that number bounds the product's error independently of K.
-constexpr int kTcKBlock = 128;
+#ifndef RCWA_TC_KBLOCK
+#define RCWA_TC_KBLOCK 128
+#endif
+constexpr int kTcKBlock = RCWA_TC_KBLOCK;  // a build-time parameter
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -370,12 +374,237 @@ __global__ void __launch_bounds__(kTcThreads, N == 128 ? 2 : 1) zgemm_tf32x3_ker
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
 }
 
+// ------------------------------------------------------------ pre-split operands
+// The operands are split into TF32 planes once per product instead of once
+// per output tile: for row tile rt (128 rows of op(A), or 128 columns of B)
+// and K slab ks (8 values) each plane (re hi, re lo, im hi, im lo) holds a
+// 4 KB block already in the UMMA no-swizzle K-major layout, so a CTA moves a
+// slab into shared memory with plain bulk copies (cp.async.bulk, the TMA
+// engine, from this GPU's memory; no tensor map, no multicast) and its
+// threads do no conversion at all.
+constexpr int kV2Stages = 3;
+constexpr size_t kV2StageBytes = 8 * 4096;  // 4 A planes + 4 B planes
+constexpr size_t kV2Smem = kV2Stages * kV2StageBytes + 64;
+
+__host__ __device__ inline size_t plane_blocks(int rows, int K) {
+  return (size_t)((rows + kTcM - 1) / kTcM) * ((K + kTcK - 1) / kTcK);
+}
+
+// Planes of op A (isB = 0: rows = M, A row-major) or of B (isB = 1: rows = N,
+// B row-major K x N, read column-wise) for every batch item, scaled by the
+// item's power of two; zero outside the matrix.  One thread per (row, 4-value
+// K chunk) of a (row tile, K slab) block.
+__global__ void tc_split_kernel(GemmArgs g, const int* exps, int isB, float* planes) {
+  const int b = blockIdx.y;
+  const int rows = isB ? g.N : g.M;
+  const int RT = (rows + kTcM - 1) / kTcM, KS = (g.K + kTcK - 1) / kTcK;
+  const size_t nblk = (size_t)RT * KS;
+  const int e = max(exps[isB * g.batch + b], -1000);
+  const double sc = ldexp(1.0, e > -1000 ? -e : 0);
+  const cplx* X = isB ? (g.B ? g.B[b] : g.B0 + b * g.sB) + g.offB : (g.A ? g.A[b] : g.A0 + b * g.sA) + g.offA;
+  float* P = planes + (size_t)b * 4 * nblk * 1024;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nblk * 256; t += (size_t)gridDim.x * blockDim.x) {
+    const size_t blk = t / 256;
+    const int within = (int)(t % 256);
+    const int r = within % kTcM, q = within / kTcM;  // row in the tile, K chunk (0 or 1)
+    const int rt = (int)(blk / KS), ks = (int)(blk % KS);
+    const int gr = rt * kTcM + r;
+    float rh[4], rl[4], ih[4], il[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gk = ks * kTcK + 4 * q + j;
+      cplx v = mkc(0.0, 0.0);
+      if (gr < rows && gk < g.K) v = isB ? X[(size_t)gk * g.ldb + gr] : X[(size_t)gr * g.lda + gk];
+      split_tf32(v.x * sc, rh[j], rl[j]);
+      split_tf32(v.y * sc, ih[j], il[j]);
+    }
+    const int off = plane_off(r, 4 * q, kLboA) / 4;
+    float* base = P + blk * 1024 + off;
+    *reinterpret_cast<float4*>(base) = make_float4(rh[0], rh[1], rh[2], rh[3]);
+    *reinterpret_cast<float4*>(base + nblk * 1024) = make_float4(rl[0], rl[1], rl[2], rl[3]);
+    *reinterpret_cast<float4*>(base + 2 * nblk * 1024) = make_float4(ih[0], ih[1], ih[2], ih[3]);
+    *reinterpret_cast<float4*>(base + 3 * nblk * 1024) = make_float4(il[0], il[1], il[2], il[3]);
+  }
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// 128 x 128 output tile from pre-split planes.  Thread 0 runs a three-stage
+// pipeline: the bulk copies of slab i are issued while the MMAs of slab
+// i - 2 run; a stage is refilled once the commit of its previous MMAs has
+// arrived.  At each K-block boundary the whole CTA adds the accumulators
+// into D in FP64 (tc_epilogue).  Every wait is bounded.
+__global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_split_kernel(GemmArgs g, const int* exps,
+                                                                          const float* planesA,
+                                                                          const float* planesB, int* err) {
+  using Tile = TcTile<128>;
+  constexpr uint32_t kIdesc = Tile::kIdesc, kIdescNegA = Tile::kIdescNegA;
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(tsm + kV2Stages * kV2StageBytes);
+  uint64_t* empty = full + kV2Stages;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(empty + kV2Stages);
+  int* s_fail = reinterpret_cast<int*>(tmem_slot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int b = blockIdx.z;
+  const int m0 = blockIdx.y * kTcM, n0 = blockIdx.x * 128;
+  const int KS = (g.K + kTcK - 1) / kTcK;
+  const size_t nblkA = plane_blocks(g.M, g.K), nblkB = plane_blocks(g.N, g.K);
+  const float* PA = planesA + (size_t)b * 4 * nblkA * 1024 + (size_t)blockIdx.y * KS * 1024;
+  const float* PB = planesB + (size_t)b * 4 * nblkB * 1024 + (size_t)blockIdx.x * KS * 1024;
+  const int eA = max(exps[b], -1000), eB = max(exps[g.batch + b], -1000);
+  const int eAB = (eA > -1000 ? eA : 0) + (eB > -1000 ? eB : 0);
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(Tile::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < kV2Stages; ++i) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(full + i)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(empty + i)) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t tRe = tmem, tIm = tmem + 128;
+  uint32_t fphase[kV2Stages] = {}, ephase[kV2Stages] = {};
+  int epending[kV2Stages] = {};  // a commit on empty[s] not yet waited for (thread 0)
+  int fpending[kV2Stages] = {};  // bulk copies into stage s not yet waited for (thread 0)
+  const int slabs_per_block = kTcKBlock / kTcK;
+  for (int kb0 = 0; kb0 < KS; kb0 += slabs_per_block) {
+    const int kb1 = min(KS, kb0 + slabs_per_block);
+    if (tid == 0 && !*s_fail) {
+      bool fail = false;
+      // pipeline over the block's slabs: copies run kV2Stages - 1 slabs ahead
+      for (int i = kb0; i < kb1 + kV2Stages - 1 && !fail; ++i) {
+        if (i < kb1) {
+          const int stg = i % kV2Stages;
+          if (epending[stg]) {
+            if (!mbar_wait(smem_u32(empty + stg), ephase[stg])) { fail = true; break; }
+            ephase[stg] ^= 1u;
+            epending[stg] = 0;
+          }
+          const uint32_t fb = smem_u32(full + stg);
+          mbar_expect_tx(fb, (uint32_t)kV2StageBytes);
+          const uint32_t dst = smem_u32(tsm + stg * kV2StageBytes);
+          for (int p = 0; p < 4; ++p) {
+            bulk_g2s(dst + p * 4096, PA + (size_t)p * nblkA * 1024 + (size_t)i * 1024, 4096, fb);
+            bulk_g2s(dst + (4 + p) * 4096, PB + (size_t)p * nblkB * 1024 + (size_t)i * 1024, 4096, fb);
+          }
+          fpending[stg] = 1;
+        }
+        const int j = i - (kV2Stages - 1);
+        if (j >= kb0 && j < kb1) {
+          const int stg = j % kV2Stages;
+          if (!mbar_wait(smem_u32(full + stg), fphase[stg])) { fail = true; break; }
+          fphase[stg] ^= 1u;
+          fpending[stg] = 0;
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t base = smem_u32(tsm + stg * kV2StageBytes);
+          const uint64_t arh = make_desc(base, kLboA), arl = make_desc(base + 4096, kLboA);
+          const uint64_t aih = make_desc(base + 8192, kLboA), ail = make_desc(base + 12288, kLboA);
+          const uint64_t brh = make_desc(base + 16384, kLboA), brl = make_desc(base + 20480, kLboA);
+          const uint64_t bih = make_desc(base + 24576, kLboA), bil = make_desc(base + 28672, kLboA);
+          const uint32_t acc = j > kb0 ? 1u : 0u;
+          mma_tf32(tRe, arh, brh, kIdesc, acc);
+          mma_tf32(tRe, arh, brl, kIdesc, 1u);
+          mma_tf32(tRe, arl, brh, kIdesc, 1u);
+          mma_tf32(tRe, aih, bih, kIdescNegA, 1u);
+          mma_tf32(tRe, aih, bil, kIdescNegA, 1u);
+          mma_tf32(tRe, ail, bih, kIdescNegA, 1u);
+          mma_tf32(tIm, arh, bih, kIdesc, acc);
+          mma_tf32(tIm, arh, bil, kIdesc, 1u);
+          mma_tf32(tIm, arl, bih, kIdesc, 1u);
+          mma_tf32(tIm, aih, brh, kIdesc, 1u);
+          mma_tf32(tIm, aih, brl, kIdesc, 1u);
+          mma_tf32(tIm, ail, brh, kIdesc, 1u);
+          mma_commit(smem_u32(empty + stg));
+          epending[stg] = 1;
+        }
+      }
+      // the block's MMAs complete before the accumulators are read: the
+      // commit of its last slab covers every earlier MMA
+      for (int s2 = 0; s2 < kV2Stages && !fail; ++s2) {
+        if (!epending[s2]) continue;
+        if (!mbar_wait(smem_u32(empty + s2), ephase[s2])) { fail = true; break; }
+        ephase[s2] ^= 1u;
+        epending[s2] = 0;
+      }
+      if (fail) *s_fail = 1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (*s_fail) break;
+    tc_epilogue<128>(g, b, m0, n0, tRe, tIm, eAB, kb0 == 0);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  }
+  if (*s_fail) {
+    // nothing may still write the stages or the tensor memory when they are
+    // released: wait (bounded) for every outstanding copy and commit
+    if (tid == 0) {
+      for (int s2 = 0; s2 < kV2Stages; ++s2) {
+        if (fpending[s2]) mbar_wait(smem_u32(full + s2), fphase[s2]);
+        if (epending[s2]) mbar_wait(smem_u32(empty + s2), ephase[s2]);
+      }
+      atomicExch(err, 1);
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Tile::kTmemCols)
+                 : "memory");
+}
+
 }  // namespace
 
-cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st, int tile_n) {
+size_t zgemm_tf32x3_planes_bytes(int M, int N, int K, int batch) {
+  return sizeof(float) * 4 * 1024 * (plane_blocks(M, K) + plane_blocks(N, K)) * (size_t)batch;
+}
+
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st, int tile_n,
+                                 float* planes, size_t planes_bytes) {
   if (g.batch <= 0 || g.M <= 0 || g.N <= 0) return cudaSuccess;
   if (g.K <= 0 || g.transA || g.transB || g.s || !err || !scale_ws || (tile_n != 128 && tile_n != 256))
     return cudaErrorInvalidValue;
+  if (planes && tile_n == 128 && planes_bytes >= zgemm_tf32x3_planes_bytes(g.M, g.N, g.K, g.batch)) {
+    // operands split once into TF32 planes, slabs moved by bulk copies
+    static SmemAttrOnce attr_split;
+    cudaError_t e = attr_split.ensure(zgemm_tf32x3_split_kernel, (int)kV2Smem);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(scale_ws, 0x80, sizeof(int) * 2 * g.batch, st);
+    if (e != cudaSuccess) return e;
+    tc_scale_kernel<<<dim3(16, g.batch, 2), 256, 0, st>>>(g, scale_ws);
+    ++launch_counter();
+    float* pA = planes;
+    float* pB = planes + 4 * 1024 * plane_blocks(g.M, g.K) * (size_t)g.batch;
+    const size_t thrA = plane_blocks(g.M, g.K) * 256, thrB = plane_blocks(g.N, g.K) * 256;
+    tc_split_kernel<<<dim3((unsigned)std::min<size_t>((thrA + 255) / 256, 4096), g.batch), 256, 0, st>>>(g, scale_ws,
+                                                                                                      0, pA);
+    ++launch_counter();
+    tc_split_kernel<<<dim3((unsigned)std::min<size_t>((thrB + 255) / 256, 4096), g.batch), 256, 0, st>>>(g, scale_ws,
+                                                                                                      1, pB);
+    ++launch_counter();
+    dim3 grid((g.N + 127) / 128, (g.M + kTcM - 1) / kTcM, g.batch);
+    zgemm_tf32x3_split_kernel<<<grid, kTcThreads, kV2Smem, st>>>(g, scale_ws, pA, pB, err);
+    ++launch_counter();
+    return cudaGetLastError();
+  }
   static SmemAttrOnce attr128, attr256;
   cudaError_t e = tile_n == 128 ? attr128.ensure(zgemm_tf32x3_kernel<128>, (int)TcTile<128>::kSmem)
                                 : attr256.ensure(zgemm_tf32x3_kernel<256>, (int)TcTile<256>::kSmem);

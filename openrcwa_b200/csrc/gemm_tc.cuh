@@ -12,5 +12,11 @@
 // (device int) is set to 1 if a tensor-core completion wait runs out; the
 // affected tile is then not written.
 // tile_n: columns of D per CTA, 128 (two CTAs per SM) or 256 (one CTA per SM,
-// every converted A slab serves twice the columns).
-cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st, int tile_n = 128);
+// every converted A slab serves twice the columns).  With planes (device
+// scratch of zgemm_tf32x3_planes_bytes) and tile_n = 128, A and B are first
+// split into TF32 planes once (not once per output tile) and the product
+// kernel moves them into shared memory with bulk copies.
+cudaError_t zgemm_tf32x3_batched(const GemmArgs& g, int* scale_ws, int* err, cudaStream_t st, int tile_n = 128,
+                                 float* planes = nullptr, size_t planes_bytes = 0);
+// Scratch bytes of the pre-split planes of a batched M x N x K product.
+size_t zgemm_tf32x3_planes_bytes(int M, int N, int K, int batch);

@@ -283,8 +283,13 @@ extern "C" int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch
   g.beta = mkc(beta.re, beta.im);
   g.gammaI = mkc(0.0, 0.0);
   g.batch = batch;
-  cudaError_t err = precision == RCWA_PREC_MIXED ? zgemm_tf32x3_batched(g, dscale.as<int>(), derr.as<int>(), e->stream)
-                                                 : zgemm_batched(g, e->stream);
+  const size_t pbytes = precision == RCWA_PREC_MIXED ? zgemm_tf32x3_planes_bytes(M, N, K, batch) : 0;
+  Dev dplanes(pbytes);
+  if (!dplanes.p) return set_err(e, RCWA_ERR_NOMEM, "allocation failed");
+  cudaError_t err = precision == RCWA_PREC_MIXED
+                        ? zgemm_tf32x3_batched(g, dscale.as<int>(), derr.as<int>(), e->stream, 128,
+                                               dplanes.as<float>(), pbytes)
+                        : zgemm_batched(g, e->stream);
   if (err != cudaSuccess || cudaStreamSynchronize(e->stream) != cudaSuccess)
     return set_err(e, RCWA_ERR_CUDA, "GEMM kernel failed");
   int herr = 0;

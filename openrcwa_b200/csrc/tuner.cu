@@ -141,7 +141,7 @@ cudaError_t tune_measure(rcwa_engine* e, int op, int n, int batch, TuneEntry& ou
   // + scratch; products A, B, D
   const size_t per_item = op == kTuneLU ? 2 * per
                           : op == kTuneSchur ? 3 * per + zgeev_workspace_bytes(n) + (size_t)n * sizeof(cplx) + 64
-                                             : 3 * per;
+                                             : 3 * per + zgemm_tf32x3_planes_bytes(n, n, n, 1);
   int mb = op == kTuneSchur ? std::min(batch, sms) : batch;
   mb = (int)std::max<size_t>(1, std::min<size_t>((size_t)mb, kTuneBytes / per_item));
   Events ev;
@@ -202,9 +202,10 @@ cudaError_t tune_measure(rcwa_engine* e, int op, int n, int batch, TuneEntry& ou
       if (err != cudaSuccess) return err;
     }
   } else {
-    Buf A, B, D, scale, tcerr;
+    Buf A, B, D, scale, tcerr, planes;
+    const size_t pbytes = zgemm_tf32x3_planes_bytes(n, n, n, mb);
     if (!A.alloc(per * mb) || !B.alloc(per * mb) || !D.alloc(per * mb) || !scale.alloc(sizeof(int) * 2 * mb) ||
-        !tcerr.alloc(sizeof(int)))
+        !tcerr.alloc(sizeof(int)) || !planes.alloc(pbytes))
       return cudaErrorMemoryAllocation;
     if ((err = fill(A.as<cplx>(), nn * mb, 0xA11ull + n, st)) != cudaSuccess) return err;
     if ((err = fill(B.as<cplx>(), nn * mb, 0xB22ull + n, st)) != cudaSuccess) return err;
@@ -221,8 +222,9 @@ cudaError_t tune_measure(rcwa_engine* e, int op, int n, int batch, TuneEntry& ou
         GemmArgs x = g;
         x.batch = b;
         return out.cand[c] == 1 ? zgemm_batched(x, st)
-                                : zgemm_tf32x3_batched(x, scale.as<int>(), tcerr.as<int>(), st,
-                                                       out.cand[c] == 2 ? 256 : 128);
+               : out.cand[c] == 2 ? zgemm_tf32x3_batched(x, scale.as<int>(), tcerr.as<int>(), st, 256)
+                                  : zgemm_tf32x3_batched(x, scale.as<int>(), tcerr.as<int>(), st, 128,
+                                                         planes.as<float>(), pbytes);
       };
       double warm = 0.0;
       err = timed(nop, [&]() { return run(1); }, 1, warm);

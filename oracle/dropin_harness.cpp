@@ -27,10 +27,6 @@ char Title[256] = "";
 void monitor1(FILE* fp, const char s[]) {
   if (fp) std::fprintf(fp, "%s\n", s);
 }
-int rcwa_write_hdf5(const char*, const rcwa_meta_t*, const rcwa_spectrum_row_t*, int, int, const char* const*) {
-  return 1;  // HDF5 output is outside the engine; the bridge then keeps the CSV
-}
-int rcwa_write_hdf5_orders(const char*, int, int, int, int, const double*, const double*) { return 1; }
 int rcwa_run(FILE* fp_log);
 }
 

@@ -91,3 +91,66 @@ def test_cpp_api_adapter(tmp_path):
     assert abs(vals[0][0] - ref["R"][0]) < 1e-9 and abs(vals[1][0] - ref["R"][1]) < 1e-9
     assert abs(vals[0][1] - ref["T"][0]) < 1e-9 and abs(vals[1][1] - ref["T"][1]) < 1e-9
     assert abs(vals[0][0] - 0.138130) < 1e-6 and abs(vals[1][0] - 0.204841) < 1e-6
+
+
+DRIVER = os.path.join(ROOT, "oracle", "_ref", "rcwa_driver_dropin")
+
+# .orcwa inputs for the reference's orcwa_rcwa (rcwa/RCWAInput.cpp keys):
+# a square lattice of dielectric pillars (z cylinders) on a glass substrate at
+# normal incidence, and a lossy, dispersive sphere above a slab at oblique
+# incidence with circular polarisation
+ORCWA = {
+    "pillars": """OpenRCWA 4 2
+title = drop-in check: pillar metasurface
+xmesh = -2.0e-07 20 2.0e-07
+ymesh = -2.0e-07 20 2.0e-07
+zmesh = -5e-07 10 -1.5e-07 10 0.0 10 4e-07
+material = 1 2.25 0 1 0
+material = 1 6.0 0 1 0
+geometry = 2 1 -2.0e-07 2.0e-07 -2.0e-07 2.0e-07 -5e-07 -1.5e-07
+geometry = 3 11 -1.2e-07 1.2e-07 -1.0e-07 1.0e-07 -1.5e-07 0
+planewave = 0 0 1
+rcwaorder = 3 3
+frequency1 = 3.6e14 5.6e14 4
+end
+""",
+    "sphere": """OpenRCWA 4 2
+title = drop-in check: sphere, oblique circular incidence
+xmesh = -2.5e-07 20 2.5e-07
+ymesh = -2.0e-07 20 2.0e-07
+zmesh = -4e-07 10 -1.2e-07 10 2.0e-07 10 5e-07
+material = 1 2.1 0 1 0
+material = 1 3.0 0 1 0
+material_dispersion = 3 2.0 3.0e15 5.0e13 4.5e15
+geometry = 2 1 -2.5e-07 2.5e-07 -2.0e-07 2.0e-07 -4e-07 -1.2e-07
+geometry = 3 2 -1.5e-07 1.5e-07 -1.2e-07 1.2e-07 -1.2e-07 1.8e-07
+planewave = 25 30 4
+rcwaorder = 2 2
+frequency1 = 4.0e14 5.0e14 2
+end
+""",
+}
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="oracle/_ref not built (oracle/build_ref.sh)")
+@pytest.mark.parametrize("case", sorted(ORCWA))
+def test_reference_driver_unmodified_on_engine(tmp_path, case):
+    # the reference's rcwa/RCWADriver.cpp, rcwa/RCWAInput.cpp and
+    # src/rcwa_Main.cpp, unmodified, on the engine's adapters: the verbose CSV
+    # (8 significant digits) against the oracle's restatement of the driver
+    from oracle import driver_oracle
+    (tmp_path / "in.orcwa").write_text(ORCWA[case])
+    out = subprocess.run([DRIVER, "-v", "-o", "out.csv", "in.orcwa"], cwd=tmp_path, capture_output=True, text=True,
+                         timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    rows = [list(map(float, ln.split(","))) for ln in open(tmp_path / "out.csv") if not ln.startswith("#")]
+    ref = driver_oracle.run(ORCWA[case])
+    assert len(rows) == len(ref)
+    for row, r in zip(rows, ref):
+        nord = r["REF"].size
+        assert abs(row[0] - r["lambda"]) < 1e-7 * r["lambda"]
+        got = np.array(row[1:5])
+        want = np.array([r["R"], r["T"], r["A"], r["R"] + r["T"]])
+        assert np.max(np.abs(got - want)) < 2e-8, (got, want)
+        assert np.max(np.abs(np.array(row[5:5 + nord]) - r["REF"])) < 2e-8
+        assert np.max(np.abs(np.array(row[5 + nord:5 + 2 * nord]) - r["TRN"])) < 2e-8
