@@ -14,8 +14,7 @@
 // first access after solve().
 //
 // Outside this engine (they report on std::cerr and leave outputs empty):
-// PML (enablePML), layer translations, magnetic layers, non-uniform
-// half-spaces, incident vectors other than generateHorizontalPlaneWave's and
+// PML (enablePML), layer translations, non-uniform half-spaces, incident vectors other than generateHorizontalPlaneWave's and
 // the field images (saveFieldImage, saveDeviceImage).
 #pragma once
 #include <algorithm>
@@ -65,27 +64,35 @@ class RCWASolver {
     rcwa_engine* e = rcwa_b200::engine();
     if (!e) return;
     for (int li : layerStack)
-      if (li < 0 || li >= (int)layers_.size() || layers_[(size_t)li].isMagnetic()) {
-        std::cerr << "[rcwa_b200] solve: invalid or magnetic layer in the stack\n";
+      if (li < 0 || li >= (int)layers_.size()) {
+        std::cerr << "[rcwa_b200] solve: invalid layer in the stack\n";
         return;
       }
+    bool magnetic = false;
+    for (int li : layerStack) magnetic = magnetic || layers_[(size_t)li].isMagnetic();
     // common cell grid over every layer of the stack; subdividing a
     // piecewise-constant cell does not change its Fourier coefficients
     cx_ = merged(true, layerStack);
     cy_ = merged(false, layerStack);
     const size_t ncx = cx_.size(), ncy = cy_.size(), cells = (ncx - 1) * (ncy - 1);
     eps_.assign(cells * layerStack.size(), rcwa_cplx{1.0, 0.0});
+    mu_.assign(magnetic ? cells * layerStack.size() : 0, rcwa_cplx{1.0, 0.0});
     for (size_t l = 0; l < layerStack.size(); ++l) {
       const Layer& L = layers_[(size_t)layerStack[l]];
       for (size_t j = 0; j + 1 < ncy; ++j)
         for (size_t i = 0; i + 1 < ncx; ++i) {
-          const scalex v = L.eps(0.5 * (cx_[i] + cx_[i + 1]), 0.5 * (cy_[j] + cy_[j + 1]));
+          const scalar xc = 0.5 * (cx_[i] + cx_[i + 1]), yc = 0.5 * (cy_[j] + cy_[j + 1]);
+          const scalex v = L.eps(xc, yc);
           eps_[l * cells + j * (ncx - 1) + i] = rcwa_cplx{v.real(), v.imag()};
+          if (magnetic) {
+            const scalex m = L.mu(xc, yc);
+            mu_[l * cells + j * (ncx - 1) + i] = rcwa_cplx{m.real(), m.imag()};
+          }
         }
     }
     thick_.assign(thickness.begin(), thickness.end());
     rcwa_stack st{nX_, nY_, (int)ncx, (int)ncy, cx_.data(), cy_.data(), (int)layerStack.size(), eps_.data(),
-                  thick_.data()};
+                  thick_.data(), magnetic ? mu_.data() : nullptr};
     rcwa_point pt{0, lambda, kx0_, ky0_};
     rcwa_cplx pxy[2] = {{1.0, 0.0}, {0.0, 0.0}};
     int rc = rcwa_plan_create(e, &st, 1, &pt, 1, 1, pxy, RCWA_PREC_FP64, &plan_);
@@ -207,7 +214,7 @@ class RCWASolver {
   std::vector<Layer> layers_;
   std::vector<int> stack_;
   std::vector<double> cx_, cy_, thick_;
-  std::vector<rcwa_cplx> eps_;
+  std::vector<rcwa_cplx> eps_, mu_;
   rcwa_plan* plan_ = nullptr;
   mutable bool fetched_ = false;
   mutable Eigen::MatrixXcs tdd_, rud_;

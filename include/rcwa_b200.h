@@ -58,7 +58,12 @@ typedef struct rcwa_plan rcwa_plan;
  * strip, exactly the Layer eps_ matrix.  Layer 0 is the incidence half-space,
  * layer n_layers-1 the transmission half-space; both must be uniform (every
  * cell equal), as sol/rcwa_bridge.cpp:255-259 assumes.  thickness[l] is used
- * for 0 < l < n_layers-1 only (rcwa/RCWASolver.cpp:415-431). */
+ * for 0 < l < n_layers-1 only (rcwa/RCWASolver.cpp:415-431).  mu, when not
+ * NULL, is the relative permeability on the same grid (Layer(coordX, coordY,
+ * eps, mu), rcwa/Layer.cpp:41-72): a layer with a cell whose mu differs from 1
+ * by more than 1e-12 takes the magnetic branch of the wave equation
+ * (rcwa/Layer.cpp:128-164,205-213); the half-spaces' mu enters their modes
+ * and the efficiencies (rcwa/RCWASolver.cpp:1826-1907).  NULL: mu = 1. */
 typedef struct {
   int nHx, nHy;              /* harmonics: 2*nHx+1 by 2*nHy+1 orders            */
   int ncx, ncy;              /* number of cell edges along x and y (>= 2)        */
@@ -67,6 +72,7 @@ typedef struct {
   int n_layers;              /* >= 2                                             */
   const rcwa_cplx* eps;      /* [n_layers][ncy-1][ncx-1]                         */
   const double* thickness;   /* [n_layers]                                       */
+  const rcwa_cplx* mu;       /* [n_layers][ncy-1][ncx-1] or NULL                 */
 } rcwa_stack;
 
 /* One solve point: one RCWASolver::solve (rcwa/RCWASolver.cpp:139-148) of a

@@ -61,7 +61,7 @@ class rcwa_cplx(C.Structure):
 class rcwa_stack(C.Structure):
     _fields_ = [("nHx", C.c_int), ("nHy", C.c_int), ("ncx", C.c_int), ("ncy", C.c_int),
                 ("cx", C.c_void_p), ("cy", C.c_void_p), ("n_layers", C.c_int),
-                ("eps", C.c_void_p), ("thickness", C.c_void_p)]
+                ("eps", C.c_void_p), ("thickness", C.c_void_p), ("mu", C.c_void_p)]
 
 
 class rcwa_table_stack(C.Structure):
@@ -205,9 +205,10 @@ class RcwaError(RuntimeError):
 
 
 class Stack:
-    """A layer stack on a common cell grid (owns its numpy buffers)."""
+    """A layer stack on a common cell grid (owns its numpy buffers); mu, when
+    given, is the relative permeability on the same grid (None: 1)."""
 
-    def __init__(self, nHx, nHy, cx, cy, eps, thickness):
+    def __init__(self, nHx, nHy, cx, cy, eps, thickness, mu=None):
         self.nHx, self.nHy = int(nHx), int(nHy)
         self.cx = np.ascontiguousarray(cx, dtype=np.float64)
         self.cy = np.ascontiguousarray(cy, dtype=np.float64)
@@ -215,6 +216,8 @@ class Stack:
         assert self.eps.ndim == 3 and self.eps.shape[1:] == (self.cy.size - 1, self.cx.size - 1)
         self.thickness = np.ascontiguousarray(thickness, dtype=np.float64)
         assert self.thickness.size == self.eps.shape[0]
+        self.mu = None if mu is None else np.ascontiguousarray(mu, dtype=np.complex128)
+        assert self.mu is None or self.mu.shape == self.eps.shape
 
     @property
     def N(self):
@@ -222,7 +225,8 @@ class Stack:
 
     def c_struct(self):
         return rcwa_stack(self.nHx, self.nHy, self.cx.size, self.cy.size, self.cx.ctypes.data, self.cy.ctypes.data,
-                          self.eps.shape[0], self.eps.ctypes.data, self.thickness.ctypes.data)
+                          self.eps.shape[0], self.eps.ctypes.data, self.thickness.ctypes.data,
+                          None if self.mu is None else self.mu.ctypes.data)
 
 
 class TableStack:

@@ -21,6 +21,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -96,6 +97,11 @@ struct StackInfo {
   double Lx, Ly;
   std::vector<double> cx, cy;
   std::vector<cplx> eps;   // L * cells
+  // relative permeability (L * cells) when some layer is magnetic, else
+  // empty; mag[l]: layer l has a cell with |mu - 1| > 1e-12 (Layer::Layer,
+  // rcwa/Layer.cpp:64-71)
+  std::vector<cplx> mu;
+  std::vector<char> mag;
   std::vector<double> thick;
   int ncx, ncy;
   // stacks given by Laurent tables: one (2nx-1) x (2ny-1) table per
@@ -172,11 +178,21 @@ int validate_stack(const rcwa_stack& s, std::string& why) {
       if (!finite_c(z)) { why = "non-finite permittivity"; return RCWA_ERR_NONFINITE; }
       if (z.re == 0.0 && z.im == 0.0) { why = "zero permittivity"; return RCWA_ERR_INVALID; }
     }
+    if (s.mu)
+      for (size_t c = 0; c < cells; ++c) {
+        const rcwa_cplx z = s.mu[(size_t)l * cells + c];
+        if (!finite_c(z)) { why = "non-finite permeability"; return RCWA_ERR_NONFINITE; }
+        if (z.re == 0.0 && z.im == 0.0) { why = "zero permeability"; return RCWA_ERR_INVALID; }
+      }
     if (l == 0 || l == s.n_layers - 1) {
       const rcwa_cplx z0 = s.eps[(size_t)l * cells];
       for (size_t c = 1; c < cells; ++c) {
         const rcwa_cplx z = s.eps[(size_t)l * cells + c];
         if (z.re != z0.re || z.im != z0.im) { why = "half-spaces must be uniform"; return RCWA_ERR_UNSUPPORTED; }
+        if (s.mu) {
+          const rcwa_cplx m0 = s.mu[(size_t)l * cells], m = s.mu[(size_t)l * cells + c];
+          if (m.re != m0.re || m.im != m0.im) { why = "half-spaces must be uniform"; return RCWA_ERR_UNSUPPORTED; }
+        }
       }
     } else if (!std::isfinite(s.thickness[l]) || s.thickness[l] < 0) {
       why = "invalid thickness";
@@ -202,7 +218,30 @@ StackInfo make_stack_info(const rcwa_stack& s) {
   si.eps.resize(cells * s.n_layers);
   for (size_t i = 0; i < si.eps.size(); ++i) si.eps[i] = mkc(s.eps[i].re, s.eps[i].im);
   si.thick.assign(s.thickness, s.thickness + s.n_layers);
+  si.mag.assign(s.n_layers, 0);
+  bool any = false;
+  if (s.mu)
+    for (int l = 0; l < s.n_layers; ++l)
+      for (size_t c = 0; c < cells; ++c) {
+        const rcwa_cplx z = s.mu[(size_t)l * cells + c];
+        if (std::hypot(z.re - 1.0, z.im) > 1e-12) { si.mag[l] = 1; any = true; break; }
+      }
+  if (any) {
+    si.mu.resize(cells * s.n_layers);
+    for (size_t i = 0; i < si.mu.size(); ++i) si.mu[i] = mkc(s.mu[i].re, s.mu[i].im);
+  }
   return si;
+}
+
+bool is_mag(const StackInfo& si, int l) { return !si.mag.empty() && si.mag[l]; }
+
+// conv jobs of a layer's permeability are keyed (stack, layer + kMuJob)
+constexpr int kMuJob = 1 << 20;
+
+// relative permeability of a uniform layer (the half-spaces): 1 unless given
+cplx layer_mu0(const StackInfo& si, int l) {
+  if (si.mu.empty()) return mkc(1.0, 0.0);
+  return si.mu[(size_t)l * (si.ncx - 1) * (si.ncy - 1)];
 }
 
 // alpha/beta of RCWASolver::evaluateAlphaBeta (rcwa/RCWASolver.cpp:242-266):
@@ -395,12 +434,14 @@ static size_t chunk_layout(ChunkWork& c, const std::vector<StackInfo>& stacks, i
   return L.off;
 }
 
-static size_t chunk_bytes_per_point(int N, int Lp, bool mixed) {
+// Lm: magnetic layers of the stack, each with a second set of four
+// convolution matrices (the permeability's)
+static size_t chunk_bytes_per_point(int N, int Lp, int Lm, bool mixed) {
   const double n = 2.0 * N;
   const double nn = n * n * sizeof(cplx), NN = (double)N * N * sizeof(cplx);
   const double per_job = 2 * NN + 3 * nn + zgeev_workspace_bytes((int)n) + 4 * NN;
   const double planes = mixed ? (double)zgemm_tf32x3_planes_bytes((int)n, (int)n, (int)n, 1) : 0.0;
-  return (size_t)(13 * nn + planes + per_job * std::max(Lp - 2, 0));
+  return (size_t)(13 * nn + planes + per_job * std::max(Lp - 2, 0) + 4 * NN * Lm);
 }
 
 namespace {
@@ -516,12 +557,13 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
 
   // ---- inputs: stack arrays and per-point alpha/beta
   Layout il;
-  std::vector<size_t> cx_off(n_stacks), cy_off(n_stacks), eps_off(n_stacks), f2d_off(n_stacks);
+  std::vector<size_t> cx_off(n_stacks), cy_off(n_stacks), eps_off(n_stacks), f2d_off(n_stacks), mu_off(n_stacks);
   for (int s = 0; s < n_stacks; ++s) {
     cx_off[s] = il.take(sizeof(double) * si[s].cx.size());
     cy_off[s] = il.take(sizeof(double) * si[s].cy.size());
     eps_off[s] = il.take(sizeof(cplx) * si[s].eps.size());
     f2d_off[s] = il.take(sizeof(cplx) * si[s].f2d.size());
+    mu_off[s] = il.take(sizeof(cplx) * si[s].mu.size());
   }
   std::vector<size_t> ab_off(n_pts);
   for (int p = 0; p < n_pts; ++p) ab_off[p] = il.take(sizeof(cplx) * 2 * P->point_N[p]);
@@ -533,6 +575,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       std::memcpy(h.data() + cy_off[s], si[s].cy.data(), sizeof(double) * si[s].cy.size());
       std::memcpy(h.data() + eps_off[s], si[s].eps.data(), sizeof(cplx) * si[s].eps.size());
       if (!si[s].f2d.empty()) std::memcpy(h.data() + f2d_off[s], si[s].f2d.data(), sizeof(cplx) * si[s].f2d.size());
+      if (!si[s].mu.empty()) std::memcpy(h.data() + mu_off[s], si[s].mu.data(), sizeof(cplx) * si[s].mu.size());
     }
     for (int p = 0; p < n_pts; ++p) alpha_beta(si[pts[p].stack], pts[p].kx0, pts[p].ky0, (cplx*)(h.data() + ab_off[p]));
     if (cudaMemcpy(P->inputs.p, h.data(), il.off, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -570,9 +613,12 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
   // chunks with the other points; each cascade product is then two batched
   // calls, one per precision.
   std::vector<char> metallic(n_stacks, 0);
-  for (int s = 0; s < n_stacks; ++s)
+  for (int s = 0; s < n_stacks; ++s) {
     for (const cplx& z : si[s].eps)
       if (z.x < 0.0) { metallic[s] = 1; break; }
+    for (const cplx& z : si[s].mu)
+      if (z.x < 0.0) { metallic[s] = 1; break; }
+  }
   std::map<std::tuple<int, int, int>, std::vector<int>> groups;
   for (int p = 0; p < n_pts; ++p) {
     const int s = pts[p].stack;
@@ -594,7 +640,9 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       used = 0;
     };
     for (int p : g.second) {
-      const size_t need = chunk_bytes_per_point(N, si[pts[p].stack].L, precision == RCWA_PREC_MIXED);
+      const StackInfo& sp = si[pts[p].stack];
+      const int Lm = (int)std::count(sp.mag.begin(), sp.mag.end(), (char)1);
+      const size_t need = chunk_bytes_per_point(N, sp.L, Lm, precision == RCWA_PREC_MIXED);
       if (!cur.points.empty() && (used + need > budget || cur.points.size() >= 1024)) flush();
       cur.points.push_back(p);
       used += need;
@@ -609,11 +657,13 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       c.max_ncx = std::max(c.max_ncx, si[s].ncx);
       c.max_ncy = std::max(c.max_ncy, si[s].ncy);
       for (int l = 1; l + 1 < si[s].L; ++l) {
-        auto key = std::make_pair(s, l);
-        if (!c.conv_index.count(key)) {
-          c.conv_index[key] = (int)c.conv_stack.size();
-          c.conv_stack.push_back(s);
-          c.conv_layer.push_back(l);
+        for (int k = 0; k < (is_mag(si[s], l) ? 2 : 1); ++k) {
+          auto key = std::make_pair(s, l + k * kMuJob);
+          if (!c.conv_index.count(key)) {
+            c.conv_index[key] = (int)c.conv_stack.size();
+            c.conv_stack.push_back(s);
+            c.conv_layer.push_back(l + k * kMuJob);
+          }
         }
         c.job_point.push_back((int)lp);
         c.job_layer.push_back(l);
@@ -687,19 +737,22 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
     if (nconv > 0 && !reuse_conv) {
       std::vector<ConvJob> jobs(nconv);
       for (int j = 0; j < nconv; ++j) {
-        const int s = c.conv_stack[j], l = c.conv_layer[j];
+        const int s = c.conv_stack[j], lk = c.conv_layer[j];
+        const bool of_mu = lk >= kMuJob;
+        const int l = of_mu ? lk - kMuJob : lk;
         const size_t cells = (size_t)(si[s].ncx - 1) * (si[s].ncy - 1);
         jobs[j].cx = (const double*)(inb + cx_off[s]);
         jobs[j].cy = (const double*)(inb + cy_off[s]);
-        jobs[j].eps = (const cplx*)(inb + eps_off[s]) + (size_t)l * cells;
+        jobs[j].eps = (const cplx*)(inb + (of_mu ? mu_off[s] : eps_off[s])) + (size_t)l * cells;
         jobs[j].ncx = si[s].ncx;
         jobs[j].ncy = si[s].ncy;
         jobs[j].fe11 = W_(c.fe11) + NN * j;
         jobs[j].fe22 = W_(c.fe22) + NN * j;
         jobs[j].fe33 = W_(c.fe33) + NN * j;
         jobs[j].tab = W_(c.tab) + c.tab_elems * j;
-        jobs[j].f2d = si[s].tables ? (const cplx*)(inb + f2d_off[s]) + (size_t)(l - 1) * (2 * nx - 1) * (2 * ny - 1)
-                                   : nullptr;
+        jobs[j].f2d = si[s].tables && !of_mu
+                          ? (const cplx*)(inb + f2d_off[s]) + (size_t)(l - 1) * (2 * nx - 1) * (2 * ny - 1)
+                          : nullptr;
       }
       // ConvJob array lives in the workspace (uploaded by a memcpy step)
       const size_t jobs_meta = meta.add_vec(jobs);
@@ -745,8 +798,14 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
 
     // ---------------- modes of the patterned layers
     if (nj > 0) {
-      std::vector<const cplx*> gA(2 * nj), gB(2 * nj), gS(2 * nj);
-      std::vector<cplx*> gD(2 * nj);
+      // non-magnetic layers: the X products and the structured M; magnetic
+      // layers: dense P and Q, M = (P / k0^2) Q and V = Q W as products
+      std::vector<int> jn, jm;
+      for (int j = 0; j < nj; ++j)
+        (is_mag(si[pts[c.points[c.job_point[j]]].stack], c.job_layer[j]) ? jm : jn).push_back(j);
+      const int nn_j = (int)jn.size(), nm_j = (int)jm.size();
+      std::vector<const cplx*> gA(2 * nn_j), gB(2 * nn_j), gS(2 * nn_j);
+      std::vector<cplx*> gD(2 * nn_j);
       std::vector<LayerItem> items(nj);
       std::vector<cplx*> Mp(nj), Wp(nj);
       std::vector<int> jpoint(nj);
@@ -754,14 +813,6 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         const int lp = c.job_point[j], p = c.points[lp], s = pts[p].stack, l = c.job_layer[j];
         const int cj = c.conv_index.at({s, l});
         const cplx* ab = (const cplx*)(inb + ab_off[p]);
-        gA[j] = W_(c.Einv) + NN * cj;
-        gB[j] = W_(c.fe11) + NN * cj;
-        gS[j] = ab;
-        gD[j] = W_(c.X1) + NN * j;
-        gA[nj + j] = W_(c.Einv) + NN * cj;
-        gB[nj + j] = W_(c.fe22) + NN * cj;
-        gS[nj + j] = ab + N;
-        gD[nj + j] = W_(c.X2) + NN * j;
         LayerItem& it = items[j];
         it.fe11 = W_(c.fe11) + NN * cj;
         it.fe22 = W_(c.fe22) + NN * cj;
@@ -779,19 +830,65 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         Wp[j] = it.W;
         jpoint[j] = p;
       }
+      std::vector<LayerItem> itn, itm;
+      for (int q = 0; q < nn_j; ++q) {
+        const int j = jn[q];
+        const int cj = c.conv_index.at({pts[c.points[c.job_point[j]]].stack, c.job_layer[j]});
+        const cplx* ab = items[j].ab;
+        gA[q] = W_(c.Einv) + NN * cj;
+        gB[q] = W_(c.fe11) + NN * cj;
+        gS[q] = ab;
+        gD[q] = W_(c.X1) + NN * j;
+        gA[nn_j + q] = W_(c.Einv) + NN * cj;
+        gB[nn_j + q] = W_(c.fe22) + NN * cj;
+        gS[nn_j + q] = ab + N;
+        gD[nn_j + q] = W_(c.X2) + NN * j;
+        itn.push_back(items[j]);
+      }
+      // magnetic jobs: P / k0^2 into the V buffer and Q into the W buffer,
+      // M = P Q; after the eigensolve Q again into the M buffer and V = Q W
+      std::vector<MagItem> mpq(nm_j), mq(nm_j);
+      std::vector<const cplx*> pA(nm_j), pB(nm_j), qA(nm_j), qB(nm_j);
+      std::vector<cplx*> pD(nm_j), qD(nm_j);
+      for (int q = 0; q < nm_j; ++q) {
+        const int j = jm[q];
+        const int s = pts[c.points[c.job_point[j]]].stack, l = c.job_layer[j];
+        const int ce = c.conv_index.at({s, l}), cm = c.conv_index.at({s, l + kMuJob});
+        MagItem mi;
+        mi.E = W_(c.Einv) + NN * ce;
+        mi.H = W_(c.Einv) + NN * cm;
+        mi.fe11 = W_(c.fe11) + NN * ce;
+        mi.fe22 = W_(c.fe22) + NN * ce;
+        mi.fm11 = W_(c.fe11) + NN * cm;
+        mi.fm22 = W_(c.fe22) + NN * cm;
+        mi.ab = items[j].ab;
+        mi.k0 = items[j].k0;
+        mi.P = items[j].V;
+        mi.Q = items[j].W;
+        mpq[q] = mi;
+        mi.P = nullptr;
+        mi.Q = items[j].M;
+        mq[q] = mi;
+        pA[q] = items[j].V; pB[q] = items[j].W; pD[q] = items[j].M;
+        qA[q] = items[j].M; qB[q] = items[j].W; qD[q] = items[j].V;
+        itm.push_back(items[j]);
+      }
       const size_t oA = meta.add_vec(gA), oB = meta.add_vec(gB), oS = meta.add_vec(gS), oD = meta.add_vec(gD);
-      const size_t oItems = meta.add_vec(items), oM = meta.add_vec(Mp), oW = meta.add_vec(Wp);
+      const size_t oItems = meta.add_vec(itn), oM = meta.add_vec(Mp), oW = meta.add_vec(Wp);
       const size_t oJP = meta.add_vec(jpoint);
+      const size_t oItemsM = meta.add_vec(itm), oMpq = meta.add_vec(mpq), oMq = meta.add_vec(mq);
+      const size_t opA = meta.add_vec(pA), opB = meta.add_vec(pB), opD = meta.add_vec(pD);
+      const size_t oqA = meta.add_vec(qA), oqB = meta.add_vec(qB), oqD = meta.add_vec(qD);
       // V GEMMs: top = fe22 * Wb, bottom = fe11 * Wt
-      std::vector<const cplx*> vA(2 * nj), vB(2 * nj);
-      std::vector<cplx*> vD(2 * nj);
-      for (int j = 0; j < nj; ++j) {
-        vA[j] = items[j].fe22;
-        vB[j] = items[j].W + (size_t)N * n;
-        vD[j] = items[j].V;
-        vA[nj + j] = items[j].fe11;
-        vB[nj + j] = items[j].W;
-        vD[nj + j] = items[j].V + (size_t)N * n;
+      std::vector<const cplx*> vA(2 * nn_j), vB(2 * nn_j);
+      std::vector<cplx*> vD(2 * nn_j);
+      for (int q = 0; q < nn_j; ++q) {
+        vA[q] = itn[q].fe22;
+        vB[q] = itn[q].W + (size_t)N * n;
+        vD[q] = itn[q].V;
+        vA[nn_j + q] = itn[q].fe11;
+        vB[nn_j + q] = itn[q].W;
+        vD[nn_j + q] = itn[q].V + (size_t)N * n;
       }
       const size_t ovA = meta.add_vec(vA), ovB = meta.add_vec(vB), ovD = meta.add_vec(vD);
       cplx* mu = W_(c.mu);
@@ -801,38 +898,65 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       const int ms_min = c.ms_min;
       P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
         char* m = (char*)plan->meta.p;
-        GemmArgs g{};
-        g.A = (const cplx* const*)(m + oA);
-        g.B = (const cplx* const*)(m + oB);
-        g.C = nullptr;
-        g.D = (cplx* const*)(m + oD);
-        g.s = (const cplx* const*)(m + oS);
-        g.M = N; g.N = N; g.K = N;
-        g.lda = N; g.ldb = N; g.ldc = N; g.ldd = N;
-        g.alpha = mkc(1, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
-        g.batch = 2 * nj;
+        auto dense = [&](size_t a, size_t b, size_t d) {
+          GemmArgs q{};
+          q.A = (const cplx* const*)(m + a);
+          q.B = (const cplx* const*)(m + b);
+          q.D = (cplx* const*)(m + d);
+          q.M = n; q.N = n; q.K = n;
+          q.lda = n; q.ldb = n; q.ldc = n; q.ldd = n;
+          q.alpha = mkc(1, 0); q.beta = mkc(0, 0); q.gammaI = mkc(0, 0);
+          q.batch = nm_j;
+          return zgemm_batched(q, st);
+        };
         cudaError_t err;
-        if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
-        pf.mark(st, kStPQGemm);
         const LayerItem* it = (const LayerItem*)(m + oItems);
-        if ((err = assemble_m(it, nj, N, st)) != cudaSuccess) return err;
-        pf.mark(st, kStAssemble);
+        if (nn_j > 0) {
+          GemmArgs g{};
+          g.A = (const cplx* const*)(m + oA);
+          g.B = (const cplx* const*)(m + oB);
+          g.C = nullptr;
+          g.D = (cplx* const*)(m + oD);
+          g.s = (const cplx* const*)(m + oS);
+          g.M = N; g.N = N; g.K = N;
+          g.lda = N; g.ldb = N; g.ldc = N; g.ldd = N;
+          g.alpha = mkc(1, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
+          g.batch = 2 * nn_j;
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          pf.mark(st, kStPQGemm);
+          if ((err = assemble_m(it, nn_j, N, st)) != cudaSuccess) return err;
+          pf.mark(st, kStAssemble);
+        }
+        if (nm_j > 0) {
+          if ((err = assemble_pq((const MagItem*)(m + oMpq), nm_j, N, true, st)) != cudaSuccess) return err;
+          pf.mark(st, kStAssemble);
+          if ((err = dense(opA, opB, opD)) != cudaSuccess) return err;
+          pf.mark(st, kStPQGemm);
+        }
         if ((err = zgeev_batched((cplx* const*)(m + oM), n, n, mu, (cplx* const*)(m + oW), n, eigw, einfo, nj, st,
                                  &pf, ms_min)) != cudaSuccess)
           return err;
         if ((err = fold_info(einfo, (const int*)(m + oJP), nj, 0, status, st)) != cudaSuccess) return err;
-        GemmArgs v{};
-        v.A = (const cplx* const*)(m + ovA);
-        v.B = (const cplx* const*)(m + ovB);
-        v.D = (cplx* const*)(m + ovD);
-        v.M = N; v.N = n; v.K = N;
-        v.lda = N; v.ldb = n; v.ldc = n; v.ldd = n;
-        v.alpha = mkc(1, 0); v.beta = mkc(0, 0); v.gammaI = mkc(0, 0);
-        v.batch = 2 * nj;
-        if ((err = zgemm_batched(v, st)) != cudaSuccess) return err;
-        err = finish_modes(it, nj, N, status, st);
+        if (nn_j > 0) {
+          GemmArgs v{};
+          v.A = (const cplx* const*)(m + ovA);
+          v.B = (const cplx* const*)(m + ovB);
+          v.D = (cplx* const*)(m + ovD);
+          v.M = N; v.N = n; v.K = N;
+          v.lda = N; v.ldb = n; v.ldc = n; v.ldd = n;
+          v.alpha = mkc(1, 0); v.beta = mkc(0, 0); v.gammaI = mkc(0, 0);
+          v.batch = 2 * nn_j;
+          if ((err = zgemm_batched(v, st)) != cudaSuccess) return err;
+          if ((err = finish_modes(it, nn_j, N, status, st)) != cudaSuccess) return err;
+        }
+        if (nm_j > 0) {
+          if ((err = assemble_pq((const MagItem*)(m + oMq), nm_j, N, false, st)) != cudaSuccess) return err;
+          if ((err = dense(oqA, oqB, oqD)) != cudaSuccess) return err;
+          if ((err = finish_modes_scaled((const LayerItem*)(m + oItemsM), nm_j, N, status, st)) != cudaSuccess)
+            return err;
+        }
         pf.mark(st, kStModes);
-        return err;
+        return cudaSuccess;
       });
     }
 
@@ -845,7 +969,10 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         for (int side = 0; side < 2; ++side) {
           HalfItem& h = hs[2 * lp + side];
           h.ab = (const cplx*)(inb + ab_off[p]);
-          h.eps = si[s].eps[(side == 0 ? 0 : (size_t)(si[s].L - 1)) * cells];
+          const int lh = side == 0 ? 0 : si[s].L - 1;
+          h.eps = si[s].eps[(size_t)lh * cells];
+          h.mu = layer_mu0(si[s], lh);
+          h.magnetic = (h.mu.x != 1.0 || h.mu.y != 0.0) ? 1 : 0;
           h.k0 = 2 * kPi / pts[p].lambda;
           h.W = W_(side == 0 ? c.hW0 : c.hWL) + nn * lp;
           h.V = W_(side == 0 ? c.hV0 : c.hVL) + nn * lp;
@@ -1079,8 +1206,14 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           it.Rud = rud[lp];
           it.Tdd = tdd[lp];
           it.ab = (const cplx*)(inb + ab_off[p]);
-          it.eps_ref = si[s].eps[0];
-          it.eps_trn = si[s].eps[(size_t)(si[s].L - 1) * cells];
+          // k^2 = k0^2 eps mu of the half-spaces, and the transmitted flux
+          // ratio |mu_ref / mu_trn| (rcwa/RCWASolver.cpp:1826-1830, 1905-1907)
+          const cplx mr = layer_mu0(si[s], 0), mt = layer_mu0(si[s], si[s].L - 1);
+          it.n2_ref = cmul(si[s].eps[0], mr);
+          it.n2_trn = cmul(si[s].eps[(size_t)(si[s].L - 1) * cells], mt);
+          it.trn_scale = (mr.x == mt.x && mr.y == mt.y)
+                             ? 1.0
+                             : std::abs(std::complex<double>(mr.x, mr.y) / std::complex<double>(mt.x, mt.y));
           it.k0 = 2 * kPi / pts[p].lambda;
           const rcwa_cplx px = pxy[((size_t)p * n_exc + x) * 2], py = pxy[((size_t)p * n_exc + x) * 2 + 1];
           it.px = mkc(px.re, px.im);

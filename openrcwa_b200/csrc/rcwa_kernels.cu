@@ -75,15 +75,70 @@ __global__ void finish_modes_kernel(const LayerItem* items, int N, int* status) 
   }
 }
 
+// Magnetic layers: P / k0^2 and Q element by element (MagItem).  The
+// diagonal matrices Da, Db scale rows and columns of E and H; the
+// permeability and permittivity convolution matrices enter unscaled.
+__global__ void assemble_pq_kernel(const MagItem* items, int N, int with_p) {
+  const MagItem it = items[blockIdx.y];
+  const int n = 2 * N;
+  const double k02 = it.k0 * it.k0, ik02 = 1.0 / k02;
+  const size_t total = (size_t)n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / n), c = (int)(e % n);
+    const int rr = r % N, cc = c % N;
+    const size_t o = (size_t)rr * N + cc;
+    const bool top = r < N, left = c < N;
+    // row factor of block row, column factor of block column
+    const double fr_p = top ? it.ab[rr].x : it.ab[N + rr].x;
+    const double fc_p = left ? it.ab[N + cc].x : it.ab[cc].x;
+    cplx q = cscale(it.H[o], fr_p * fc_p);
+    if (top && left) q = cneg(q);
+    else if (top) q = csub(q, cscale(it.fe22[o], k02));
+    else if (left) q = cadd(cneg(q), cscale(it.fe11[o], k02));
+    it.Q[e] = q;
+    if (with_p) {
+      cplx p = cscale(it.E[o], fr_p * fc_p);
+      if (top && !left) p = csub(cscale(it.fm22[o], k02), p);
+      else if (!top && left) p = csub(p, cscale(it.fm11[o], k02));
+      else if (!top) p = cneg(p);
+      it.P[e] = cscale(p, ik02);
+    }
+  }
+}
+
+// Modes of a magnetic layer: V = (Q W) diag(1/keff) (rcwa/WaveEquationSolver.cpp:36).
+__global__ void finish_modes_scaled_kernel(const LayerItem* items, int N, int* status) {
+  const LayerItem it = items[blockIdx.y];
+  const int n = 2 * N;
+  const size_t total = (size_t)n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / n), c = (int)(e % n);
+    const cplx g = gamma_sqrt(it.mu[c]);
+    const cplx keff = cscale(g, it.k0);
+    if (keff.x == 0.0 && keff.y == 0.0) {
+      set_status(status, it.point, RCWA_ERR_GRAZING);
+      it.V[e] = mkc(0.0, 0.0);
+    } else {
+      it.V[e] = cdiv(it.V[e], keff);
+    }
+    if (r == 0) it.gamma[c] = g;
+  }
+}
+
 // Uniform half-space: P*Q = k0^2 (k0^2 eps - a^2 - b^2) per harmonic for both
 // field components, so W = I, keff = k0*GammaSqrtOp(k0^2 eps - a^2 - b^2) and
 // V = Q / keff with Q's 2x2 block per harmonic
 //   [[-a b, a^2 - k0^2 eps], [k0^2 eps - b^2, a b]].
+// A magnetic half-space (uniform mu): P*Q = k0^2 (k0^2 eps mu - a^2 - b^2)
+// and Q = [[-a b / mu, a^2 / mu - k0^2 eps], [k0^2 eps - b^2 / mu, a b / mu]]
+// (the magnetic branch with Fmu = mu I, H = I / mu).
 __global__ void halfspace_kernel(const HalfItem* items, int N, int* status) {
   const HalfItem it = items[blockIdx.y];
   const int n = 2 * N;
   const double k02 = it.k0 * it.k0;
   const cplx ke = cscale(it.eps, k02);
+  const cplx kem = it.magnetic ? cscale(cmul(it.eps, it.mu), k02) : ke;
+  const cplx minv = it.magnetic ? cdiv(mkc(1.0, 0.0), it.mu) : mkc(1.0, 0.0);
   const size_t total = (size_t)n * n;
   for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
     const int r = (int)(e / n), c = (int)(e % n);
@@ -91,16 +146,23 @@ __global__ void halfspace_kernel(const HalfItem* items, int N, int* status) {
     const int h = c % N;
     cplx v = mkc(0.0, 0.0);
     const cplx a = it.ab[h], b = it.ab[N + h];
-    const cplx mu = csub(csub(ke, cmul(a, a)), cmul(b, b));
+    const cplx mu = csub(csub(kem, cmul(a, a)), cmul(b, b));
     const cplx g = gamma_sqrt(mu);
     const cplx keff = cscale(g, it.k0);
     if (r % N == h) {
       cplx q;
       const bool top = r < N, left = c < N;
-      if (top && left) q = cneg(cmul(a, b));
-      else if (top) q = csub(cmul(a, a), ke);
-      else if (left) q = csub(ke, cmul(b, b));
-      else q = cmul(a, b);
+      if (!it.magnetic) {
+        if (top && left) q = cneg(cmul(a, b));
+        else if (top) q = csub(cmul(a, a), ke);
+        else if (left) q = csub(ke, cmul(b, b));
+        else q = cmul(a, b);
+      } else {
+        if (top && left) q = cneg(cmul(cmul(a, b), minv));
+        else if (top) q = csub(cmul(cmul(a, a), minv), ke);
+        else if (left) q = csub(ke, cmul(cmul(b, b), minv));
+        else q = cmul(cmul(a, b), minv);
+      }
       if (keff.x == 0.0 && keff.y == 0.0) set_status(status, it.point, RCWA_ERR_GRAZING);
       else v = cdiv(q, keff);
     }
@@ -180,7 +242,7 @@ __global__ void scatter_kernel(const ScatterItem* items, int N, int nx, int ny, 
   const int inc = ny * ((nx - 1) / 2) + (ny - 1) / 2;
   const int n = 2 * N;
   const double k02 = it.k0 * it.k0;
-  const cplx kr2 = cscale(it.eps_ref, k02), kt2 = cscale(it.eps_trn, k02);
+  const cplx kr2 = cscale(it.n2_ref, k02), kt2 = cscale(it.n2_trn, k02);
   __shared__ double red[2][256];
   __shared__ int bad;
   if (threadIdx.x == 0) bad = 0;
@@ -210,7 +272,7 @@ __global__ void scatter_kernel(const ScatterItem* items, int N, int nx, int ny, 
     const double r3 = cnorm2(rx) + cnorm2(ry) + cnorm2(rz);
     const double t3 = cnorm2(tx) + cnorm2(ty) + cnorm2(tz);
     const double REF = fabs(kzr.x) * r3 / kzinc;
-    const double TRN = fabs(kzt.x) * t3 / kzinc;
+    const double TRN = it.trn_scale * fabs(kzt.x) * t3 / kzinc;
     if (it.ref) it.ref[h] = REF;
     if (it.trn) it.trn[h] = TRN;
     sr += REF;
@@ -259,6 +321,20 @@ cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st
 cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   finish_modes_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, status);
+  ++launch_counter();
+  return cudaGetLastError();
+}
+
+cudaError_t assemble_pq(const MagItem* items, int count, int N, bool with_p, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  assemble_pq_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, with_p ? 1 : 0);
+  ++launch_counter();
+  return cudaGetLastError();
+}
+
+cudaError_t finish_modes_scaled(const LayerItem* items, int count, int N, int* status, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  finish_modes_scaled_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, status);
   ++launch_counter();
   return cudaGetLastError();
 }

@@ -18,10 +18,30 @@ struct LayerItem {
   int point;
 };
 
+// One magnetic patterned layer (relative permeability != 1 in some cell):
+// the dense P and Q of the magnetic branch of Layer::waveEqnCoeff
+// (rcwa/Layer.cpp:128-164, 205-213), E = fe33^-1, H = fmu33^-1:
+//   P = [[Da E Db, k0^2 Fmu22 - Da E Da], [Db E Db - k0^2 Fmu11, -Db E Da]]
+//   Q = [[-Da H Db, Da H Da - k0^2 Fe22], [-Db H Db + k0^2 Fe11, Db H Da]]
+struct MagItem {
+  const cplx* E;      // N x N  permittivity ContinuousXY inverse
+  const cplx* H;      // N x N  permeability ContinuousXY inverse
+  const cplx* fe11;   // N x N  permittivity DiscontinuousX
+  const cplx* fe22;   // N x N  permittivity DiscontinuousY
+  const cplx* fm11;   // N x N  permeability DiscontinuousX
+  const cplx* fm22;   // N x N  permeability DiscontinuousY
+  const cplx* ab;     // alpha[N] then beta[N]
+  cplx* P;            // n x n  P / k0^2 (written when requested)
+  cplx* Q;            // n x n  Q
+  double k0;
+};
+
 // Uniform half-space of one point.
 struct HalfItem {
   const cplx* ab;
   cplx eps;
+  cplx mu;            // relative permeability (1: the non-magnetic formulas)
+  int magnetic;       // mu != 1
   double k0;
   cplx* W;            // n x n  (identity)
   cplx* V;            // n x n  Q*W/keff, 2x2 blocks per harmonic
@@ -47,7 +67,8 @@ struct ScatterItem {
   const cplx* Rud;
   const cplx* Tdd;
   const cplx* ab;
-  cplx eps_ref, eps_trn;
+  cplx n2_ref, n2_trn;  // eps * mu of the half-spaces: k^2 = k0^2 eps mu
+  double trn_scale;     // |mu_ref / mu_trn|, the flux ratio of the transmitted orders
   double k0;
   cplx px, py;
   double* ref;        // N (device)
@@ -60,6 +81,11 @@ struct ScatterItem {
 cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st);
 cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st);
 cudaError_t halfspace_modes(const HalfItem* items, int count, int N, int* status, cudaStream_t st);
+// P / k0^2 (with_p) and Q of magnetic layers, n x n each
+cudaError_t assemble_pq(const MagItem* items, int count, int N, bool with_p, cudaStream_t st);
+// V <- V diag(1/keff), gamma = GammaSqrtOp(mu): the modes of a layer whose
+// V arrives as the full product Q W
+cudaError_t finish_modes_scaled(const LayerItem* items, int count, int N, int* status, cudaStream_t st);
 cudaError_t apply_phase(const PhaseItem* items, int count, int n, cudaStream_t st);
 // X <- V0^-1 X per item: for each order h, rows h and N+h of X against the 2x2
 // block [V0(h,h) V0(h,N+h); V0(N+h,h) V0(N+h,N+h)] by Gaussian elimination

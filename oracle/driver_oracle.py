@@ -5,11 +5,12 @@ rcwa_oracle.py.  It serves as the reference answer for the drop-in test of the
 unmodified driver compiled against the engine's C++ adapters.
 
 Covered: xmesh/ymesh/zmesh (end points), material, material_eps,
-material_index, material_dispersion, geometry (box, sphere, cylinders along
-z/x/y), planewave (pol 1-5), rcwaorder, frequency1/2 and wavelength,
-background; lengths in micrometres as the parser stores them.  Not covered:
-magnetic materials (the driver's mu branch, rcwa/Layer.cpp:128-164), which
-this engine does not model; a problem that has them raises.
+material_index, material_mu, material_dispersion, geometry (box, sphere,
+cylinders along z/x/y), planewave (pol 1-5), rcwaorder, frequency1/2 and
+wavelength, background; lengths in micrometres as the parser stores them.
+Magnetic materials (relative permeability and magnetic conductivity) follow
+muAt / hasMagneticMaterial (rcwa/RCWADriver.cpp:126-157) into the oracle's
+magnetic branch of the wave equation.
 """
 from __future__ import annotations
 
@@ -24,6 +25,7 @@ from .rcwa_oracle import OracleLayer, RCWASolver
 C0 = 2.99792458e8
 C0_UM = 2.99792458e14   # rcwa/RCWADriver.cpp:15
 EPS0 = 8.854187817e-12  # :16
+MU0 = 1.25663706212e-6  # :17
 M_TO_UM = 1e6
 N_CURVED = 8            # N_CURVED_CELLS / N_CURVED_SLICES (RCWADriver.cpp:21, RCWAInput.cpp:435)
 BOX, SPHERE, CYL_Z, CYL_X, CYL_Y = 1, 2, 11, 12, 13
@@ -124,6 +126,11 @@ def parse(text: str) -> Problem:
             m = int(f[0])
             a, b = f[1], (f[2] if len(f) >= 3 else 0.0)
             p.eps[m] = complex(a, b) ** 2 if key == "material_index" else complex(a, b)
+        elif key == "material_mu" and len(f) >= 2:
+            # rcwa/RCWAInput.cpp:254-268
+            m = int(f[0])
+            if 0 <= m < len(p.mu):
+                p.mu[m] = complex(f[1], f[2] if len(f) >= 3 else 0.0)
         elif key == "material_dispersion" and len(f) >= 5:
             m = int(f[0])
             einf, poles = p.disp[m]
@@ -223,12 +230,33 @@ def eps_at(p: Problem, x, y, z, lam):
     return complex(e)
 
 
+def mu_at(p: Problem, x, y, z, lam):
+    """muAt (rcwa/RCWADriver.cpp:126-147): the last containing box wins; a
+    magnetic conductivity adds i msigma/(w mu0)."""
+    m = 1.0 + 0j
+    for b in p.boxes:
+        if not b.contains_xyz(x, y, z):
+            continue
+        mi = b.material
+        if mi < 0 or mi >= len(p.mu):
+            continue
+        m = p.mu[mi]
+        if mi < len(p.msigma) and p.msigma[mi] != 0.0:
+            w = 2 * math.pi * C0_UM / lam
+            m += complex(0.0, p.msigma[mi] / (w * MU0))
+    return complex(m)
+
+
+def has_magnetic(p: Problem) -> bool:
+    """hasMagneticMaterial (rcwa/RCWADriver.cpp:150-157)."""
+    return any(abs(m - 1.0) > 1e-12 for m in p.mu) or any(s != 0.0 for s in p.msigma)
+
+
 def run(text: str):
     """runRCWA (rcwa/RCWADriver.cpp:196-378) without field output: per
     wavelength (micrometres) R, T, A and the per-order REF/TRN vectors."""
     p = parse(text)
-    if any(abs(m - 1.0) > 1e-12 for m in p.mu) or any(s != 0.0 for s in p.msigma):
-        raise NotImplementedError("magnetic materials")
+    magnetic = has_magnetic(p)
     ze = z_edges(p)
     xg, yg = grid(p, "x"), grid(p, "y")
     centers = [0.5 * (ze[i] + ze[i - 1]) for i in range(len(ze) - 1, 0, -1)]
@@ -251,10 +279,12 @@ def run(text: str):
         sol = RCWASolver(p.nHx, p.nHy)
         for zc in centers:
             eps = np.array([[eps_at(p, x, y, zc, lam) for x in xc] for y in yc])
-            sol.addLayer(OracleLayer(xg, yg, eps))
+            mu = np.array([[mu_at(p, x, y, zc, lam) for x in xc] for y in yc]) if magnetic else None
+            sol.addLayer(OracleLayer(xg, yg, eps, mu=mu))
         k0 = 2 * math.pi / lam
         e_inc = eps_at(p, 0.5 * (p.xmin + p.xmax), 0.5 * (p.ymin + p.ymax), centers[0], lam)
-        n_inc = max(np.sqrt(complex(e_inc)).real, 1e-6)
+        mu_inc = mu_at(p, 0.5 * (p.xmin + p.xmax), 0.5 * (p.ymin + p.ymax), centers[0], lam) if magnetic else 1.0
+        n_inc = max(np.sqrt(complex(e_inc) * complex(mu_inc)).real, 1e-6)  # :305-312
         sol.setBlochWavevector(k0 * n_inc * math.sin(th) * math.cos(ph), k0 * n_inc * math.sin(th) * math.sin(ph))
         stack = list(range(len(centers)))
         sol.solve(lam, stack, thick)

@@ -200,8 +200,8 @@ def _solve(A, B, lstsq=False):
     return np.linalg.solve(A, B)
 
 
-def wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq=False, f2d=None):
-    """Layer::waveEqnCoeff, non-magnetic branch (rcwa/Layer.cpp:75-253).
+def wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq=False, f2d=None, mu=None):
+    """Layer::waveEqnCoeff (rcwa/Layer.cpp:75-253).
 
     Kx, Ky are the dense diagonal matrices of RCWASolver::evaluateKMatrices
     (rcwa/RCWASolver.cpp:150-185, PML disabled).  Returns (P, Q, fe11, fe22, fe33).
@@ -209,7 +209,12 @@ def wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq=False, f2d=None)
     three convolution matrices are its block-Toeplitz matrix (the Laurent rule
     for every tensor; the reference has no such layer, it staircases curved
     shapes, rcwa/RCWADriver.cpp:19-37).
+    With mu (a cell matrix like eps) that differs from 1 anywhere by more than
+    1e-12 (Layer::Layer, rcwa/Layer.cpp:64-71) the magnetic branch applies:
+    the permeability's three convolution matrices replace the identity in P,
+    and mu_zz^-1 Kx, mu_zz^-1 Ky replace Kx, Ky in Q (:128-164, :205-213).
     """
+    magnetic = mu is not None and bool(np.any(np.abs(np.asarray(mu, dtype=np.complex128) - 1.0) > 1e-12))
     if f2d is not None:
         fe11 = fe22 = fe33 = block_toeplitz_dense(np.asarray(f2d, dtype=np.complex128))
     else:
@@ -224,16 +229,26 @@ def wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq=False, f2d=None)
     k0 = 2 * PI / lam
     k02 = k0 * k0
     I = np.eye(N)
+    if magnetic:
+        mu = np.asarray(mu, dtype=np.complex128)
+        fmu11 = fourier2d(cx, cy, mu, nx, ny, DiscontinuousX)  # :132-133
+        fmu22 = fourier2d(cx, cy, mu, nx, ny, DiscontinuousY)  # :135-136
+        fmu33 = fourier2d(cx, cy, mu, nx, ny, ContinuousXY)    # :138-140
+        G1h = _solve(fmu33, Kx, lstsq)  # :143
+        G2h = _solve(fmu33, Ky, lstsq)  # :144
+    else:
+        fmu11 = fmu22 = I
+        G1h, G2h = Kx, Ky
     P = np.empty((2 * N, 2 * N), dtype=np.complex128)
-    P[:N, :N] = Kx @ F2h                # :156
-    P[:N, N:] = -Kx @ F1h + k02 * I     # :157,167
-    P[N:, :N] = Ky @ F2h - k02 * I      # :158,168
-    P[N:, N:] = -Ky @ F1h               # :159
+    P[:N, :N] = Kx @ F2h                   # :156
+    P[:N, N:] = -Kx @ F1h + k02 * fmu22    # :157,162,167
+    P[N:, :N] = Ky @ F2h - k02 * fmu11     # :158,163,168
+    P[N:, N:] = -Ky @ F1h                  # :159
     Q = np.empty_like(P)
-    Q[:N, :N] = -Kx @ Ky                # :216
-    Q[:N, N:] = Kx @ Kx - k02 * fe22    # :217
-    Q[N:, :N] = -Ky @ Ky + k02 * fe11   # :218
-    Q[N:, N:] = Ky @ Kx                 # :219
+    Q[:N, :N] = -Kx @ G2h                  # :209,216
+    Q[:N, N:] = Kx @ G1h - k02 * fe22      # :210,217
+    Q[N:, :N] = -Ky @ G2h + k02 * fe11     # :211,218
+    Q[N:, N:] = Ky @ G1h                   # :212,219
     return P, Q, fe11, fe22, fe33
 
 
@@ -275,9 +290,9 @@ class LayerSolution:
     Q: np.ndarray = None
 
 
-def layer_solve(cx, cy, eps, alpha, beta, lam, nx, ny, keep=False, lstsq=False, f2d=None):
+def layer_solve(cx, cy, eps, alpha, beta, lam, nx, ny, keep=False, lstsq=False, f2d=None, mu=None):
     """Layer::solve (rcwa/Layer.cpp:255-273)."""
-    P, Q, fe11, fe22, fe33 = wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq, f2d)
+    P, Q, fe11, fe22, fe33 = wave_eqn_coeff(cx, cy, eps, alpha, beta, lam, nx, ny, lstsq, f2d, mu)
     PQ, W, V, keff, ev = wave_equation_solve(P, Q)
     k0 = 2 * PI / lam
     sol = LayerSolution(W=W, V=V, gamma=keff / k0, eigenvalues=ev)
@@ -317,6 +332,7 @@ class OracleLayer:
     cy: np.ndarray
     eps: np.ndarray  # (len(cy)-1, len(cx)-1)
     f2d: np.ndarray = None  # optional Laurent table replacing the cells' three rules
+    mu: np.ndarray = None   # optional relative permeability per cell (None: 1)
 
 
 class RCWASolver:
@@ -363,7 +379,7 @@ class RCWASolver:
         self.alpha, self.beta = alpha_beta(self.nx, self.ny, self.Lx, self.Ly, self.kx0, self.ky0)
         # solveLayers (:194-210): every layer type, half-spaces included
         self.sol = [layer_solve(L.cx, L.cy, L.eps, self.alpha, self.beta, lam, self.nx, self.ny,
-                                keep=self.keep, lstsq=self.lstsq, f2d=L.f2d) for L in self.layers]
+                                keep=self.keep, lstsq=self.lstsq, f2d=L.f2d, mu=L.mu) for L in self.layers]
         self._interfaces(stack)
         self._scatter_matrix(stack, thickness)
 
@@ -425,10 +441,13 @@ class RCWASolver:
         Lr, Lt = self.layers[ref], self.layers[trn]
         eps_ref = layer_eps_at(Lr.cx, Lr.cy, Lr.eps, 0.0, 0.0)
         eps_trn = layer_eps_at(Lt.cx, Lt.cy, Lt.eps, 0.0, 0.0)
+        # Layer::mu(x, y), the same cell lookup (rcwa/Layer.cpp:431-450); k^2 = k0^2 eps mu (:1826-1830)
+        mu_ref = 1.0 + 0j if Lr.mu is None else layer_eps_at(Lr.cx, Lr.cy, Lr.mu, 0.0, 0.0)
+        mu_trn = 1.0 + 0j if Lt.mu is None else layer_eps_at(Lt.cx, Lt.cy, Lt.mu, 0.0, 0.0)
         a = self.alpha.astype(np.complex128)
         b = self.beta.astype(np.complex128)
-        kref2 = k0 * k0 * eps_ref
-        ktrn2 = k0 * k0 * eps_trn
+        kref2 = k0 * k0 * eps_ref * mu_ref
+        ktrn2 = k0 * k0 * eps_trn * mu_trn
         Kzref = -np.sqrt(kref2 - a * a - b * b)  # :1835
         Kztrn = np.sqrt(ktrn2 - a * a - b * b)   # :1836
         if np.any(Kzref == 0) or np.any(Kztrn == 0):
@@ -441,7 +460,8 @@ class RCWASolver:
         Kzinc = abs(Kzref[inc].real)
         if Kzinc < 1e-12 * k0:
             return None, None  # :1898-1901
-        return np.abs(Kzref.real) * r / Kzinc, np.abs(Kztrn.real) * t / Kzinc
+        # the transmitted flux carries mu_ref / mu_trn (S_z ~ kz / mu, :1902-1907)
+        return np.abs(Kzref.real) * r / Kzinc, abs(mu_ref / mu_trn) * np.abs(Kztrn.real) * t / Kzinc
 
 
 # --------------------------------------------------------------------------

@@ -15,6 +15,7 @@ import numpy as np
 import pytest
 
 from oracle.rcwa_oracle import OfdSetup, RcwaLayerSpec as L, rcwa_run
+from tests import magnetic_cases
 
 pytestmark = pytest.mark.gpu
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
@@ -97,9 +98,13 @@ DRIVER = os.path.join(ROOT, "oracle", "_ref", "rcwa_driver_dropin")
 
 # .orcwa inputs for the reference's orcwa_rcwa (rcwa/RCWAInput.cpp keys):
 # a square lattice of dielectric pillars (z cylinders) on a glass substrate at
-# normal incidence, and a lossy, dispersive sphere above a slab at oblique
-# incidence with circular polarisation
+# normal incidence, a lossy, dispersive sphere above a slab at oblique
+# incidence with circular polarisation, magnetic pillars with magnetic loss
+# on a magnetic substrate, and the reference's magnetically lossy slab
+# (material_mu)
 ORCWA = {
+    "magnetic_pillars": magnetic_cases.PILLARS,
+    "magnetic_slab": magnetic_cases.slab("material = 1 4.0 0 1.0 0\nmaterial_mu = 2 4.0 0.5\n"),
     "pillars": """OpenRCWA 4 2
 title = drop-in check: pillar metasurface
 xmesh = -2.0e-07 20 2.0e-07
