@@ -53,9 +53,13 @@ constexpr long kWaitLimit = 1L << 22;
 // memory sums are added into D in FP64 and the accumulators restart.  The
 // tensor cores' FP32 accumulation is not round-to-nearest: its error grows
 // with the number of MMAs accumulated (six per 8-deep K step), so bounding
-// that number bounds the product's error independently of K.
+// that number bounds the product's error independently of K.  Measured on
+// the lossless 2D pillar stack (Nx = Ny = 10, n = 882, 148 points): the
+// largest |R + T - 1| of the mixed plan is 2.5e-5 / 4.8e-5 / 7.5e-5 / 1.04e-4
+// for K-blocks of 128 / 256 / 512 / the whole K, and the cascade products
+// take 417 / 289 / 198 / 150 ms per step; 256 keeps half of the 1e-4 budget.
 #ifndef RCWA_TC_KBLOCK
-#define RCWA_TC_KBLOCK 128
+#define RCWA_TC_KBLOCK 256
 #endif
 constexpr int kTcKBlock = RCWA_TC_KBLOCK;  // a build-time parameter
 
