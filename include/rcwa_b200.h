@@ -243,6 +243,27 @@ int rcwa_zgeev_batched(rcwa_engine* e, int n, int batch, const rcwa_cplx* A,
  * when it was captured.  Returns RCWA_ERR_INVALID for a negative cap. */
 int rcwa_set_qr_sweep_limit(int sweeps);
 
+/* CTAs per matrix of the Hessenberg reduction and the multishift Schur
+ * iteration (no reference counterpart: a scheduling choice of this engine).
+ * A batch of large matrices (order >= 1024) that would leave half of the SMs
+ * idle is given a thread-block cluster of up to 8 CTAs per matrix; every
+ * element is computed by the same operations whatever the team size, so the
+ * results are identical.  ctas = 0 restores the automatic choice, 1..8 forces
+ * a size for every later eigensolve (matrices of order >= 64).  Process-wide;
+ * a plan captured into a CUDA graph keeps the size chosen when it was
+ * captured.  Returns RCWA_ERR_INVALID outside 0..8. */
+int rcwa_set_eig_cluster(int ctas);
+/* The team size rcwa_set_eig_cluster's setting gives a batch of `batch`
+ * order-n matrices on the current device. */
+int rcwa_eig_cluster_size(int n, int batch);
+/* The same for the panel step of the LU factorisations (interface and tau
+ * factorisations, rcwa_zgetrf stages): a batch of large matrices (order >=
+ * 1024) that would leave half of the SMs idle factorises each 32-column
+ * panel on a cluster of up to 8 CTAs per matrix, with identical factors.
+ * ctas = 0: automatic, 1..8: forced; RCWA_ERR_INVALID outside 0..8. */
+int rcwa_set_lu_cluster(int ctas);
+int rcwa_lu_cluster_size(int n, int batch);
+
 /* Batched complex GEMM D = alpha*A*B + beta*C (row-major, host buffers
  * [batch][M*K], [batch][K*N], [batch][M*N]; C may be NULL when beta = 0), the
  * product kernel of the cascade: RCWA_PREC_FP64 on the FP64 tensor path,

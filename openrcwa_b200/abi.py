@@ -47,7 +47,8 @@ EXPORTS = [
     "rcwa_tuner_default", "rcwa_tuner_set", "rcwa_tuner_get", "rcwa_tuner_count", "rcwa_tuner_entry",
     "rcwa_tuner_save", "rcwa_tuner_load", "rcwa_engine_set_tuner", "rcwa_tuner_measure",
     "rcwa_set_qr_sweep_limit", "rcwa_plan_smatrix", "rcwa_mlp_nn_distance", "rcwa_engine_solve_tables",
-    "rcwa_plan_create_tables",
+    "rcwa_plan_create_tables", "rcwa_set_eig_cluster", "rcwa_eig_cluster_size",
+    "rcwa_set_lu_cluster", "rcwa_lu_cluster_size",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -173,6 +174,10 @@ def load() -> C.CDLL:
     lib.rcwa_engine_set_tuner.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
     lib.rcwa_tuner_measure.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, _IP, _DP]
     lib.rcwa_set_qr_sweep_limit.argtypes = [C.c_int]
+    lib.rcwa_set_eig_cluster.argtypes = [C.c_int]
+    lib.rcwa_eig_cluster_size.argtypes = [C.c_int, C.c_int]
+    lib.rcwa_set_lu_cluster.argtypes = [C.c_int]
+    lib.rcwa_lu_cluster_size.argtypes = [C.c_int, C.c_int]
     lib.rcwa_plan_smatrix.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     _lib = lib
     return lib
@@ -184,6 +189,31 @@ def set_qr_sweep_limit(sweeps: int) -> None:
     rc = load().rcwa_set_qr_sweep_limit(int(sweeps))
     if rc:
         raise RcwaError(rc, "set_qr_sweep_limit")
+
+
+def set_eig_cluster(ctas: int) -> None:
+    """CTAs per matrix of the eigensolver's Hessenberg and Schur kernels for
+    every later eigensolve (0: automatic, 1..8: forced)."""
+    rc = load().rcwa_set_eig_cluster(int(ctas))
+    if rc:
+        raise RcwaError(rc, "set_eig_cluster")
+
+
+def eig_cluster_size(n: int, batch: int) -> int:
+    """The team size the current setting gives a batch of order-n matrices."""
+    return int(load().rcwa_eig_cluster_size(int(n), int(batch)))
+
+
+def set_lu_cluster(ctas: int) -> None:
+    """CTAs per matrix of the LU panel step (0: automatic, 1..8: forced)."""
+    rc = load().rcwa_set_lu_cluster(int(ctas))
+    if rc:
+        raise RcwaError(rc, "set_lu_cluster")
+
+
+def lu_cluster_size(n: int, batch: int) -> int:
+    """The LU panel team size the current setting gives a batch of order-n matrices."""
+    return int(load().rcwa_lu_cluster_size(int(n), int(batch)))
 
 
 def _d(a):

@@ -10,7 +10,10 @@
 //      back-transformed with Z by the tile GEMM and normalised to unit 2-norm.
 // This replaces LAPACK zgeev('N','V') behind MKLEigenSolver
 // (rcwa/MKLEigenSolver.hpp:102-179).  Balancing is not applied.
+#include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 
 #include "eig.cuh"
 #include "linalg.cuh"
@@ -73,6 +76,30 @@ __device__ Scratch scratch_for(void* work, int n, int b) {
   return s;
 }
 
+// The CTAs that work on one matrix: a thread-block cluster of `size` CTAs
+// (size 1: the CTA alone).  sync() is the cluster barrier, whose release and
+// acquire make every CTA's global writes before it visible to all CTAs of the
+// cluster after it; a lone CTA uses __syncthreads.  Every thread of every
+// CTA of the team must reach each sync().
+struct Team {
+  int rank, size;
+  __device__ void sync() const {
+    if (size > 1) {
+      asm volatile("barrier.cluster.arrive.release.aligned;\n" ::: "memory");
+      asm volatile("barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+    } else {
+      __syncthreads();
+    }
+  }
+};
+
+__device__ __forceinline__ Team cluster_team() {
+  unsigned r, s;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(r));
+  asm volatile("mov.u32 %0, %%cluster_nctarank;\n" : "=r"(s));
+  return Team{(int)r, (int)s};
+}
+
 __device__ double block_sum(double v, double* red) {
   for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -98,28 +125,38 @@ __device__ int block_max_int(int v, int* red) {
 
 
 // In-CTA GEMM over 64x64 tiles: D = alpha*op(A)*op(B) + beta*C (C may alias D).
-template <bool TA, bool TB>
+// A CTA of a team takes the tiles t = rank, rank + size, ...; kL2 loads the
+// operands from L2 (they may come from other CTAs of the team).
+template <bool TA, bool TB, bool kL2 = false>
 __device__ void cta_gemm(TileSmem& sm, int M, int N, int K, const cplx* A, int lda, const cplx* B, int ldb,
-                         cplx* D, int ldd, const cplx* C, int ldc, cplx alpha, cplx beta) {
+                         cplx* D, int ldd, const cplx* C, int ldc, cplx alpha, cplx beta, int rank = 0,
+                         int size = 1) {
   if (M <= 0 || N <= 0) return;
   const int tm = (M + kTBM - 1) / kTBM, tn = (N + kTBN - 1) / kTBN;
-  for (int t = 0; t < tm * tn; ++t) {
+  for (int t = rank; t < tm * tn; t += size) {
     const int m0 = (t / tn) * kTBM, n0 = (t % tn) * kTBN;
     cplx acc[4][4];
     tile_zero(acc);
-    if (K > 0) tile_mma<TA, TB>(sm, acc, A, lda, B, ldb, nullptr, M, N, K, m0, n0);
+    if (K > 0) tile_mma<TA, TB, kL2>(sm, acc, A, lda, B, ldb, nullptr, M, N, K, m0, n0);
     tile_store(acc, D, ldd, C, ldc, alpha, beta, mkc(0.0, 0.0), M, N, m0, n0);
   }
   tile_barrier();
 }
 
-// cta_gemm by the first kTileThreads threads of a larger CTA, then a full
-// barrier (the Hessenberg kernel runs more warps than the tile routines use).
-template <bool TA, bool TB>
-__device__ void cta_gemm_part(TileSmem& sm, int M, int N, int K, const cplx* A, int lda, const cplx* B, int ldb,
-                              cplx* D, int ldd, const cplx* C, int ldc, cplx alpha, cplx beta) {
-  if (threadIdx.x < kTileThreads) cta_gemm<TA, TB>(sm, M, N, K, A, lda, B, ldb, D, ldd, C, ldc, alpha, beta);
-  __syncthreads();
+// cta_gemm by the first kTileThreads threads of every CTA of a team (the
+// Hessenberg kernel runs more warps than the tile routines use), the tiles
+// split over the team, then a barrier over the team.
+template <bool TA, bool TB, bool kTeam>
+__device__ void cta_gemm_part(const Team& tm, TileSmem& sm, int M, int N, int K, const cplx* A, int lda,
+                              const cplx* B, int ldb, cplx* D, int ldd, const cplx* C, int ldc, cplx alpha,
+                              cplx beta) {
+  if (threadIdx.x < kTileThreads) {
+    if (kTeam)
+      cta_gemm<TA, TB, true>(sm, M, N, K, A, lda, B, ldb, D, ldd, C, ldc, alpha, beta, tm.rank, tm.size);
+    else
+      cta_gemm<TA, TB>(sm, M, N, K, A, lda, B, ldb, D, ldd, C, ldc, alpha, beta);
+  }
+  tm.sync();
 }
 
 // Blocked Householder reduction to Hessenberg form in compact WY form, the
@@ -132,9 +169,21 @@ __device__ void cta_gemm_part(TileSmem& sm, int M, int N, int K, const cplx* A, 
 // is formed backwards with tile GEMMs.  Reflectors H = I - tau v v^H are
 // Hermitian with real tau; column j stores beta at (j+1, j) and the tail of
 // v_j below it, v_j(j+1) = v0[j].
-__device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, double* red, TileSmem& tsm) {
+// A team of several CTAs (a cluster) shares the work of one matrix: the
+// first CTA forms each reflector, every CTA then takes a slice of the rows of
+// A0 v_j and Y, and the tiles of every GEMM are split over the team.  Each
+// element is computed by the same operations as with one CTA, so the result
+// does not depend on the team size.  kTeam: compiled for teams of more than
+// one CTA (operands of the tile GEMMs then come from L2).
+template <bool kTeam>
+__device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, double* red, TileSmem& tsm,
+                                   const Team& tm) {
   const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
   const int nb = kHb;
+  const bool lead = tm.rank == 0;
+  // this CTA's rows of the matrix-vector products (an even split point)
+  const int per = ((n + tm.size - 1) / tm.size + 1) & ~1;
+  const int r0 = min(n, tm.rank * per), r1 = min(n, r0 + per);
   cplx* a = s.v;    // work column, then v_j
   __shared__ cplx z[2 * kHb];
   cplx* u = s.uv;   // n
@@ -151,80 +200,91 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
 #endif
     const int jb = min(nb, n - 2 - k);
     cplx* T = s.Tall + (size_t)(k / nb) * nb * nb;
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) T[idx] = mkc(0.0, 0.0);
+    if (lead)
+      for (int idx = tid; idx < nb * nb; idx += blockDim.x) T[idx] = mkc(0.0, 0.0);
     for (int jj = 0; jj < jb; ++jj) {
       const int j = k + jj;
 #ifdef RCWA_EIG_STATS
       long long h_t = clock64();
-#define HMARK(i) do { if (tid == 0) { const long long t_ = clock64(); atomicAdd(&g_eig_stats[i], (unsigned long long)(t_ - h_t)); h_t = t_; } } while (0)
+#define HMARK(i) do { if (tid == 0 && lead) { const long long t_ = clock64(); atomicAdd(&g_eig_stats[i], (unsigned long long)(t_ - h_t)); h_t = t_; } } while (0)
 #else
 #define HMARK(i) do {} while (0)
 #endif
-      // a = A0(:, j) - Y(:, :jj) conj(V(j, :jj))
-      for (int i = tid; i < n; i += blockDim.x) {
-        cplx acc = A[(size_t)i * lda + j];
-        for (int q = 0; q < jj; ++q) acc = cfma(cneg(Yc[(size_t)q * n + i]), cconj(Vc[(size_t)q * n + j]), acc);
-        a[i] = acc;
-      }
-      __syncthreads();
-      HMARK(16);
-      if (jj > 0) {
-        // a(k+1:) <- (I - V T^H V^H) a(k+1:):  z = V^H a, z = T^H z, a -= V z
-        for (int q = wid; q < jj; q += nw) {
-          cplx acc = mkc(0.0, 0.0);
-          for (int i = k + 1 + q + lane; i < n; i += 32) acc = cfmaconj(Vc[(size_t)q * n + i], a[i], acc);
-          for (int off = 16; off > 0; off >>= 1) {
-            acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
-            acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
-          }
-          if (lane == 0) z[q] = acc;
-        }
-        __syncthreads();
-        if (tid < jj) {
-          cplx acc = mkc(0.0, 0.0);
-          for (int q = 0; q <= tid; ++q) acc = cfmaconj(T[q * nb + tid], z[q], acc);  // (T^H z)_tid
-          z[nb + tid] = acc;
-        }
-        __syncthreads();
-        for (int i = k + 1 + tid; i < n; i += blockDim.x) {
-          cplx acc = a[i];
-          for (int q = 0; q < jj; ++q) acc = cfma(cneg(Vc[(size_t)q * n + i]), z[nb + q], acc);
+      double tau = 0.0;
+      if (lead) {
+        // a = A0(:, j) - Y(:, :jj) conj(V(j, :jj))
+        for (int i = tid; i < n; i += blockDim.x) {
+          cplx acc = A[(size_t)i * lda + j];
+          for (int q = 0; q < jj; ++q) acc = cfma(cneg(Yc[(size_t)q * n + i]), cconj(Vc[(size_t)q * n + j]), acc);
           a[i] = acc;
         }
         __syncthreads();
+        HMARK(16);
+        if (jj > 0) {
+          // a(k+1:) <- (I - V T^H V^H) a(k+1:):  z = V^H a, z = T^H z, a -= V z
+          for (int q = wid; q < jj; q += nw) {
+            cplx acc = mkc(0.0, 0.0);
+            for (int i = k + 1 + q + lane; i < n; i += 32) acc = cfmaconj(Vc[(size_t)q * n + i], a[i], acc);
+            for (int off = 16; off > 0; off >>= 1) {
+              acc.x += __shfl_xor_sync(0xffffffffu, acc.x, off);
+              acc.y += __shfl_xor_sync(0xffffffffu, acc.y, off);
+            }
+            if (lane == 0) z[q] = acc;
+          }
+          __syncthreads();
+          if (tid < jj) {
+            cplx acc = mkc(0.0, 0.0);
+            for (int q = 0; q <= tid; ++q) acc = cfmaconj(T[q * nb + tid], z[q], acc);  // (T^H z)_tid
+            z[nb + tid] = acc;
+          }
+          __syncthreads();
+          for (int i = k + 1 + tid; i < n; i += blockDim.x) {
+            cplx acc = a[i];
+            for (int q = 0; q < jj; ++q) acc = cfma(cneg(Vc[(size_t)q * n + i]), z[nb + q], acc);
+            a[i] = acc;
+          }
+          __syncthreads();
+        }
+        HMARK(17);
+        // reflector from a(j+1:)
+        double sig = 0.0;
+        for (int i = j + 2 + tid; i < n; i += blockDim.x) sig += cnorm2(a[i]);
+        sig = block_sum(sig, red);
+        const cplx alpha = a[j + 1];
+        cplx beta = alpha, v0 = mkc(1.0, 0.0);
+        if (sig != 0.0) {
+          const double aa = cabs(alpha);
+          const double xnorm = sqrt(aa * aa + sig);
+          const cplx ph = aa > 0.0 ? cscale(alpha, 1.0 / aa) : mkc(1.0, 0.0);
+          beta = cscale(ph, -xnorm);
+          v0 = cscale(ph, aa + xnorm);
+          tau = 2.0 / (cnorm2(v0) + sig);
+        }
+        // column j of the result; explicit v_j in V(:, jj) and V^H(jj, :),
+        // and in shared memory for the matrix-vector product (the tile
+        // buffer is free during the panel)
+        for (int i = tid; i < n; i += blockDim.x) {
+          cplx vi = mkc(0.0, 0.0);
+          if (i <= j) A[(size_t)i * lda + j] = a[i];
+          else if (i == j + 1) { A[(size_t)i * lda + j] = beta; vi = v0; }
+          else { A[(size_t)i * lda + j] = a[i]; vi = a[i]; }
+          if (tau == 0.0) vi = mkc(0.0, 0.0);
+          Vc[(size_t)jj * n + i] = vi;
+          s.VH[(size_t)jj * n + i] = cconj(vi);
+          a[i] = vi;
+          if (vs_ok) vs[i] = vi;
+        }
+        if (tid == 0) { s.tau[j] = tau; s.v0[j] = v0; }
       }
-      HMARK(17);
-      // reflector from a(j+1:)
-      double sig = 0.0;
-      for (int i = j + 2 + tid; i < n; i += blockDim.x) sig += cnorm2(a[i]);
-      sig = block_sum(sig, red);
-      const cplx alpha = a[j + 1];
-      double tau = 0.0;
-      cplx beta = alpha, v0 = mkc(1.0, 0.0);
-      if (sig != 0.0) {
-        const double aa = cabs(alpha);
-        const double xnorm = sqrt(aa * aa + sig);
-        const cplx ph = aa > 0.0 ? cscale(alpha, 1.0 / aa) : mkc(1.0, 0.0);
-        beta = cscale(ph, -xnorm);
-        v0 = cscale(ph, aa + xnorm);
-        tau = 2.0 / (cnorm2(v0) + sig);
+      tm.sync();
+      if (!lead) {
+        // the other CTAs of the team take v_j and tau from the first
+        tau = __ldcg(s.tau + j);
+        if (vs_ok) {
+          for (int i = tid; i < n; i += blockDim.x) vs[i] = __ldcg(a + i);
+          __syncthreads();
+        }
       }
-      // column j of the result; explicit v_j in V(:, jj) and V^H(jj, :),
-      // and in shared memory for the matrix-vector product (the tile
-      // buffer is free during the panel)
-      for (int i = tid; i < n; i += blockDim.x) {
-        cplx vi = mkc(0.0, 0.0);
-        if (i <= j) A[(size_t)i * lda + j] = a[i];
-        else if (i == j + 1) { A[(size_t)i * lda + j] = beta; vi = v0; }
-        else { A[(size_t)i * lda + j] = a[i]; vi = a[i]; }
-        if (tau == 0.0) vi = mkc(0.0, 0.0);
-        Vc[(size_t)jj * n + i] = vi;
-        s.VH[(size_t)jj * n + i] = cconj(vi);
-        a[i] = vi;
-        if (vs_ok) vs[i] = vi;
-      }
-      if (tid == 0) { s.tau[j] = tau; s.v0[j] = v0; }
-      __syncthreads();
       HMARK(18);
       // u = A0(:, j+1:) v_j (one pass over the trailing columns), z = V(:, :jj)^H v_j.
       // The pass is bound by the loads in flight (the trailing matrix mostly
@@ -232,25 +292,25 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       // loads of a 128-column step at once, predicated at the row end rather
       // than finished by a serial tail loop; v_j comes from shared memory.
       const cplx* vj = vs_ok ? vs : a;
-      for (int i0 = 2 * wid; i0 < n; i0 += 2 * nw) {
-        const bool two = i0 + 1 < n;
+      for (int i0 = r0 + 2 * wid; i0 < r1; i0 += 2 * nw) {
+        const bool two = i0 + 1 < r1;
         const cplx* row0 = A + (size_t)i0 * lda;
         const cplx* row1 = two ? row0 + lda : row0;
         cplx acc0 = mkc(0.0, 0.0), acc1 = mkc(0.0, 0.0);
         for (int c = j + 1 + lane; c < n; c += 128) {
-          cplx r0[4], r1[4], w[4];
+          cplx r0v[4], r1v[4], w[4];
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const int cc = c + 32 * q;
             const bool in = cc < n;
-            r0[q] = in ? row0[cc] : mkc(0.0, 0.0);
-            r1[q] = in ? row1[cc] : mkc(0.0, 0.0);
+            r0v[q] = in ? row0[cc] : mkc(0.0, 0.0);
+            r1v[q] = in ? row1[cc] : mkc(0.0, 0.0);
             w[q] = in ? vj[cc] : mkc(0.0, 0.0);
           }
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
-            acc0 = cfma(r0[q], w[q], acc0);
-            acc1 = cfma(r1[q], w[q], acc1);
+            acc0 = cfma(r0v[q], w[q], acc0);
+            acc1 = cfma(r1v[q], w[q], acc1);
           }
         }
         for (int off = 16; off > 0; off >>= 1) {
@@ -277,48 +337,52 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
       __syncthreads();
       HMARK(20);
       // Y(:, jj) = tau (u - Y(:, :jj) z); T(:jj, jj) = -tau T(:jj, :jj) z; T(jj, jj) = tau
-      for (int i = tid; i < n; i += blockDim.x) {
+      for (int i = r0 + tid; i < r1; i += blockDim.x) {
         cplx acc = u[i];
         for (int q = 0; q < jj; ++q) acc = cfma(cneg(Yc[(size_t)q * n + i]), z[q], acc);
         Yc[(size_t)jj * n + i] = cscale(acc, tau);
       }
-      if (tid < jj) {
-        cplx acc = mkc(0.0, 0.0);
-        for (int q = tid; q < jj; ++q) acc = cfma(T[tid * nb + q], z[q], acc);
-        T[tid * nb + jj] = cscale(acc, -tau);
+      if (lead) {
+        if (tid < jj) {
+          cplx acc = mkc(0.0, 0.0);
+          for (int q = tid; q < jj; ++q) acc = cfma(T[tid * nb + q], z[q], acc);
+          T[tid * nb + jj] = cscale(acc, -tau);
+        }
+        if (tid == 0) T[jj * nb + jj] = mkc(tau, 0.0);
       }
-      if (tid == 0) T[jj * nb + jj] = mkc(tau, 0.0);
-      __syncthreads();
+      tm.sync();
       HMARK(21);
 #undef HMARK
     }
 #ifdef RCWA_EIG_STATS
     const long long c_p1 = clock64();
-    STAT_ADD(13, c_p1 - c_p0);
+    if (lead) STAT_ADD(13, c_p1 - c_p0);
 #endif
     // trailing columns c0..n-1
     const int c0 = k + jb;
     const int m2 = n - c0;
     if (m2 > 0) {
       // A(:, c0:) -= Y V(c0:, :)^H
-      cta_gemm_part<true, false>(tsm, n, m2, jb, Yc, n, s.VH + c0, n, A + c0, lda, A + c0, lda, mkc(-1.0, 0.0),
-                            mkc(1.0, 0.0));
+      cta_gemm_part<true, false, kTeam>(tm, tsm, n, m2, jb, Yc, n, s.VH + c0, n, A + c0, lda, A + c0, lda,
+                                        mkc(-1.0, 0.0), mkc(1.0, 0.0));
       // W = V(k+1:, :)^H A(k+1:, c0:)  (jb x m2), W2 = T^H W, A(k+1:, c0:) -= V(k+1:, :) W2
-      cta_gemm_part<false, false>(tsm, jb, m2, n - k - 1, s.VH + k + 1, n, A + (size_t)(k + 1) * lda + c0, lda, s.Wb + c0, n,
-                             nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
-      for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-        const int r = idx / nb, c = idx % nb;
-        s.Vt[idx] = (r < jb && c < jb) ? cconj(T[c * nb + r]) : mkc(0.0, 0.0);  // T^H in Vt
-      }
-      __syncthreads();
-      cta_gemm_part<false, false>(tsm, jb, m2, jb, s.Vt, nb, s.Wb + c0, n, s.Yb + c0, n, nullptr, 0, mkc(1.0, 0.0),
-                             mkc(0.0, 0.0));
-      cta_gemm_part<true, false>(tsm, n - k - 1, m2, jb, Vc + k + 1, n, s.Yb + c0, n,
-                            A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
-                            mkc(-1.0, 0.0), mkc(1.0, 0.0));
+      cta_gemm_part<false, false, kTeam>(tm, tsm, jb, m2, n - k - 1, s.VH + k + 1, n,
+                                         A + (size_t)(k + 1) * lda + c0, lda, s.Wb + c0, n, nullptr, 0,
+                                         mkc(1.0, 0.0), mkc(0.0, 0.0));
+      if (lead)
+        for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+          const int r = idx / nb, c = idx % nb;
+          s.Vt[idx] = (r < jb && c < jb) ? cconj(T[c * nb + r]) : mkc(0.0, 0.0);  // T^H in Vt
+        }
+      tm.sync();
+      cta_gemm_part<false, false, kTeam>(tm, tsm, jb, m2, jb, s.Vt, nb, s.Wb + c0, n, s.Yb + c0, n, nullptr, 0,
+                                         mkc(1.0, 0.0), mkc(0.0, 0.0));
+      cta_gemm_part<true, false, kTeam>(tm, tsm, n - k - 1, m2, jb, Vc + k + 1, n, s.Yb + c0, n,
+                                        A + (size_t)(k + 1) * lda + c0, lda, A + (size_t)(k + 1) * lda + c0, lda,
+                                        mkc(-1.0, 0.0), mkc(1.0, 0.0));
     }
 #ifdef RCWA_EIG_STATS
-    STAT_ADD(14, clock64() - c_p1);
+    if (lead) STAT_ADD(14, clock64() - c_p1);
 #endif
   }
 #ifdef RCWA_EIG_STATS
@@ -326,16 +390,16 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
 #endif
   // Z (column-major, i.e. Zt = Z^T row-major) = Q, accumulated backwards:
   // Zt(k+1:, k+1:) -= (Zt conj(V)) T^T V^T
-  for (size_t idx = tid; idx < (size_t)n * n; idx += blockDim.x)
+  for (size_t idx = (size_t)r0 * n + tid; idx < (size_t)r1 * n; idx += blockDim.x)
     s.Z[idx] = mkc((idx / n) == (idx % n) ? 1.0 : 0.0, 0.0);
-  __syncthreads();
+  tm.sync();
   const int npan = (n >= 3) ? (n - 3) / nb + 1 : 0;
   for (int pnl = npan - 1; pnl >= 0; --pnl) {
     const int k = pnl * nb;
     const int jb = min(nb, n - 2 - k);
     const cplx* T = s.Tall + (size_t)pnl * nb * nb;
     // conj(V) (n x nb, in Wb) and V^T (nb x n, in VH) from the stored reflectors
-    for (int i = tid; i < n; i += blockDim.x) {
+    for (int i = r0 + tid; i < r1; i += blockDim.x) {
       for (int q = 0; q < nb; ++q) {
         const int j = k + q;
         cplx vi = mkc(0.0, 0.0);
@@ -347,25 +411,28 @@ __device__ void hessenberg_blocked(cplx* A, int n, int lda, const Scratch& s, do
         s.VH[(size_t)q * n + i] = vi;
       }
     }
-    for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
-      const int r = idx / nb, c = idx % nb;
-      s.Vt[idx] = T[c * nb + r];  // T^T
-    }
-    __syncthreads();
+    if (lead)
+      for (int idx = tid; idx < nb * nb; idx += blockDim.x) {
+        const int r = idx / nb, c = idx % nb;
+        s.Vt[idx] = T[c * nb + r];  // T^T
+      }
+    tm.sync();
     const int m = n - k - 1;
     cplx* Zs = s.Z + (size_t)(k + 1) * n + (k + 1);
-    cta_gemm_part<false, false>(tsm, m, jb, m, Zs, n, s.Wb + (size_t)(k + 1) * nb, nb, s.Yb, nb, nullptr, 0,
-                           mkc(1.0, 0.0), mkc(0.0, 0.0));
-    cta_gemm_part<false, false>(tsm, m, jb, jb, s.Yb, nb, s.Vt, nb, s.Vb, nb, nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
-    cta_gemm_part<false, false>(tsm, m, m, jb, s.Vb, nb, s.VH + k + 1, n, Zs, n, Zs, n, mkc(-1.0, 0.0), mkc(1.0, 0.0));
+    cta_gemm_part<false, false, kTeam>(tm, tsm, m, jb, m, Zs, n, s.Wb + (size_t)(k + 1) * nb, nb, s.Yb, nb,
+                                       nullptr, 0, mkc(1.0, 0.0), mkc(0.0, 0.0));
+    cta_gemm_part<false, false, kTeam>(tm, tsm, m, jb, jb, s.Yb, nb, s.Vt, nb, s.Vb, nb, nullptr, 0,
+                                       mkc(1.0, 0.0), mkc(0.0, 0.0));
+    cta_gemm_part<false, false, kTeam>(tm, tsm, m, m, jb, s.Vb, nb, s.VH + k + 1, n, Zs, n, Zs, n,
+                                       mkc(-1.0, 0.0), mkc(1.0, 0.0));
   }
-  for (size_t idx = tid; idx < (size_t)n * n; idx += blockDim.x) {
+  for (size_t idx = (size_t)r0 * n + tid; idx < (size_t)r1 * n; idx += blockDim.x) {
     const int i = (int)(idx / n), j = (int)(idx % n);
     if (i > j + 1) A[(size_t)i * lda + j] = mkc(0.0, 0.0);
   }
-  __syncthreads();
+  tm.sync();
 #ifdef RCWA_EIG_STATS
-  STAT_ADD(15, clock64() - c_q0);
+  if (lead) STAT_ADD(15, clock64() - c_q0);
 #endif
 }
 
@@ -847,8 +914,16 @@ __device__ void aed_right(cplx* M, const cplx* v, int len, cplx tau, int rows, i
 // did not converge and nothing was changed).  On return sm.shifts[0..cnt)
 // hold the bottom undeflated window eigenvalues, cnt <= kMsShifts, in
 // sm.aed[2].  Whole CTA.
-__device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem& sm) {
+// With a team of several CTAs every CTA computes the window's Schur form
+// (the same operations on the same data), the first CTA's outcome is taken
+// by all (ctrl[2..4]), the first CTA writes the window back and the
+// off-window updates are split over the team.  *shift_count receives the
+// number of shifts left in sm.shifts.
+__device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem& sm, const Team& tm, int* ctrl,
+                   int* shift_count) {
   const int tid = threadIdx.x, nthr = blockDim.x;
+  const bool lead = tm.rank == 0;
+  const int stride = nthr * tm.size, off0 = tid + nthr * tm.rank;
   const int nw = kAedW;
   const int kw = i - nw + 1;
   cplx* W = sm.work;
@@ -863,6 +938,8 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
   }
   const cplx s = T[(size_t)kw * ldt + kw - 1];
   __syncthreads();
+  // every CTA holds the window before the first one writes it back
+  if (tm.size > 1) tm.sync();
   if (tid < 32) {
     const int lane = tid;
 #ifdef RCWA_EIG_STATS
@@ -924,21 +1001,38 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
 #endif
   }
   __syncthreads();
-  const bool ok = sm.aed[0] != 0;
-  const int ns = sm.aed[1];
+  bool ok = sm.aed[0] != 0;
+  int ns = sm.aed[1];
+  bool spike = s.x != 0.0 || s.y != 0.0;
+  *shift_count = sm.aed[2];
+  if (tm.size > 1) {
+    if (lead && tid == 0) {
+      ctrl[2] = ok ? ns : -1;
+      ctrl[3] = sm.aed[2];
+      ctrl[4] = spike ? 1 : 0;
+    }
+    tm.sync();
+    const int c2 = __ldcg(ctrl + 2);
+    ok = c2 >= 0;
+    ns = ok ? c2 : ns;
+    *shift_count = __ldcg(ctrl + 3);
+    spike = __ldcg(ctrl + 4) != 0;
+  }
   if (!ok) return -1;
-  if (ns == nw && (s.x != 0.0 || s.y != 0.0)) return 0;
+  if (ns == nw && spike) return 0;
 #ifdef RCWA_EIG_STATS
   const long long c_off = clock64();
 #endif
   // window, spike and the off-window blocks
-  for (int idx = tid; idx < nw * nw; idx += nthr) {
-    const int r = idx / nw, c = idx % nw;
-    T[(size_t)(kw + r) * ldt + kw + c] = AW(r, c);
+  if (lead) {
+    for (int idx = tid; idx < nw * nw; idx += nthr) {
+      const int r = idx / nw, c = idx % nw;
+      T[(size_t)(kw + r) * ldt + kw + c] = AW(r, c);
+    }
+    if (tid == 0) T[(size_t)kw * ldt + kw - 1] = cmul(s, cconj(AV(0, 0)));
   }
-  if (tid == 0) T[(size_t)kw * ldt + kw - 1] = cmul(s, cconj(AV(0, 0)));
   // rows kw..i right of the window: Vh * T
-  for (int j = i + 1 + tid; j < n; j += nthr) {
+  for (int j = i + 1 + off0; j < n; j += stride) {
     cplx x[kAedW];
 #pragma unroll
     for (int r = 0; r < kAedW; ++r) x[r] = T[(size_t)(kw + r) * ldt + j];
@@ -951,7 +1045,7 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
     }
   }
   // columns kw..i above the window: T * V
-  for (int r = tid; r < kw; r += nthr) {
+  for (int r = off0; r < kw; r += stride) {
     cplx x[kAedW];
 #pragma unroll
     for (int c = 0; c < kAedW; ++c) x[c] = T[(size_t)r * ldt + kw + c];
@@ -964,7 +1058,7 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
     }
   }
   // Schur vectors (column-major): Z(:, kw..i) * V
-  for (int r = tid; r < n; r += nthr) {
+  for (int r = off0; r < n; r += stride) {
     cplx x[kAedW];
 #pragma unroll
     for (int c = 0; c < kAedW; ++c) x[c] = Z[(size_t)(kw + c) * n + r];
@@ -976,7 +1070,7 @@ __device__ int aed(cplx* T, int ldt, cplx* Z, int n, int l, int i, const MsSmem&
       Z[(size_t)(kw + c) * n + r] = acc;
     }
   }
-  __syncthreads();
+  tm.sync();
 #ifdef RCWA_EIG_STATS
   STAT_ADD(7, clock64() - c_off);
 #endif
@@ -1063,7 +1157,10 @@ __device__ __forceinline__ void replay_frame(cplx* base, size_t stride, int top0
 // One multishift sweep over the active block [l, i] with sm.shifts[0..s).
 // Bulge b sits at position p = l + t - 3b at chain step t; it is active while
 // l <= p <= i-1 and its rotation acts on rows/columns (p, p+1).
-__device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, const MsSmem& sm) {
+// With a team of several CTAs every CTA chases the bulges through its own
+// copy of the window (the same operations on the same data), the first CTA
+// writes the window back, and the off-window lines are split over the team.
+__device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, const MsSmem& sm, const Team& tm) {
   const int tid = threadIdx.x, nthr = blockDim.x, lane = tid & 31, warp = tid >> 5, nwarp = nthr >> 5;
   const int tend = (i - l) + 3 * (s - 1);
   int t = 0;
@@ -1090,6 +1187,8 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
       cp_async16(&MSW(idx / w, idx % w), &T[(size_t)(ws + idx / w) * ldt + ws + idx % w]);
     cp_async_wait_all();
     __syncthreads();
+    // every CTA holds its window before the first one writes it back
+    if (tm.size > 1) tm.sync();
     for (int tt = t; tt < t1; ++tt) {
       const int over = l + tt - (i - 1);
       const int bA = over > 0 ? (over + 2) / 3 : 0;
@@ -1147,7 +1246,8 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
     const long long c_mid = clock64();
     STAT_ADD(3, c_mid - c_start);
 #endif
-    for (int idx = tid; idx < w * w; idx += nthr) T[(size_t)(ws + idx / w) * ldt + ws + idx % w] = MSW(idx / w, idx % w);
+    if (tm.rank == 0)
+      for (int idx = tid; idx < w * w; idx += nthr) T[(size_t)(ws + idx / w) * ldt + ws + idx % w] = MSW(idx / w, idx % w);
     // rows/columns touched in this pass
     int rlo = i + 1, rhi = -1;
     for (int b = 0; b < s; ++b)
@@ -1168,7 +1268,7 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
     __syncthreads();
     const int top0 = l + t - 3 * (kMsShifts - 1);
     const int nR = (n - 1 - we + 31) / 32, nU = (ws + 31) / 32, nZ = (n + 31) / 32;
-    for (int task = warp; task < nR + nU + nZ; task += nwarp) {
+    for (int task = warp + nwarp * tm.rank; task < nR + nU + nZ; task += nwarp * tm.size) {
       if (task < nR) {
         // T(rlo..rhi, j), j right of the window: row rotations, lane = column
         const int j = we + 1 + 32 * task + lane;
@@ -1183,7 +1283,7 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
         if (r < n) replay_frame<false>(Z + r, (size_t)n, top0, nsteps, rlo, rhi, sm);
       }
     }
-    __syncthreads();
+    tm.sync();
 #ifdef RCWA_EIG_STATS
     STAT_ADD(4, clock64() - c_mid);
 #endif
@@ -1193,8 +1293,12 @@ __device__ void ms_sweep(cplx* T, int ldt, cplx* Z, int n, int l, int i, int s, 
 
 // Schur form by multishift sweeps on active blocks of at least ms_min rows
 // (ms_min >= kMsMin) and single-shift sweeps on smaller ones.  Returns 0 or
-// RCWA_ERR_NOCONV.
-__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSmem& sm, int sweep_cap) {
+// RCWA_ERR_NOCONV.  With a team of several CTAs the first CTA finds each
+// split point and runs the single-shift sweeps, and every decision that
+// steers the team's barriers comes from the first CTA through ctrl (global
+// scratch of at least 8 ints), so all CTAs take the same path.
+__device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSmem& sm, int sweep_cap,
+                        const Team& tm, int* ctrl) {
   const double ulp = 2.0 * RCWA_DBL_EPS;
   const double smlnum = RCWA_DBL_MIN * ((double)n / ulp);
   const int tid = threadIdx.x;
@@ -1202,13 +1306,21 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
   long long sweeps = 0;
   const long long budget = sweep_cap > 0 ? min(30LL * max(10, n), (long long)sweep_cap) : 30LL * max(10, n);
   int stall = 0, last_i = -1, last_l = -1;
+  const bool lead = tm.rank == 0;
+  int it = 0;
   while (i >= 0) {
-    int best = 0;
-    for (int k = 1 + tid; k <= i; k += blockDim.x)
-      if (negligible(T, ldt, k, 0, i, ulp, smlnum)) best = max(best, k);
-    const int l = block_max_int(best, sm.redi);
-    if (l > 0 && tid == 0) T[(size_t)l * ldt + l - 1] = mkc(0.0, 0.0);
-    __syncthreads();
+    int l = 0;
+    if (lead) {
+      int best = 0;
+      for (int k = 1 + tid; k <= i; k += blockDim.x)
+        if (negligible(T, ldt, k, 0, i, ulp, smlnum)) best = max(best, k);
+      l = block_max_int(best, sm.redi);
+      if (l > 0 && tid == 0) T[(size_t)l * ldt + l - 1] = mkc(0.0, 0.0);
+      if (tm.size > 1 && tid == 0) ctrl[it & 1] = l;
+    }
+    tm.sync();
+    if (tm.size > 1) l = __ldcg(ctrl + (it & 1));  // two slots: the first CTA may run one split ahead
+    ++it;
     if (l >= i) {
       --i;
       stall = 0;
@@ -1234,7 +1346,7 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
 #ifdef RCWA_EIG_STATS
       const long long c_ss = clock64();
 #endif
-      qr_sweep(T, ldt, Z, n, l, i, shift, reinterpret_cast<cplx(*)[kWin + 1]>(sm.Wt), sm.lc, sm.ls);
+      if (lead) qr_sweep(T, ldt, Z, n, l, i, shift, reinterpret_cast<cplx(*)[kWin + 1]>(sm.Wt), sm.lc, sm.ls);
 #ifdef RCWA_EIG_STATS
       STAT_ADD(9, clock64() - c_ss);
 #endif
@@ -1249,7 +1361,8 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
 #ifdef RCWA_EIG_STATS
       const long long c_aed = clock64();
 #endif
-      const int nd = aed(T, ldt, Z, n, l, i, sm);
+      int cnt = 0;
+      const int nd = aed(T, ldt, Z, n, l, i, sm, tm, ctrl, &cnt);
 #ifdef RCWA_EIG_STATS
       STAT_ADD(8, clock64() - c_aed);
       STAT_ADD(11, 1);
@@ -1263,8 +1376,8 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
         }
         ib = i - nd;
       }
-      if (nd >= 0 && sm.aed[2] >= kMsShifts / 2) {
-        s = sm.aed[2];
+      if (nd >= 0 && cnt >= kMsShifts / 2) {
+        s = cnt;
         have_shifts = true;
       }
     }
@@ -1287,7 +1400,7 @@ __device__ int schur_ms(cplx* T, int ldt, cplx* Z, int n, int ms_min, const MsSm
       }
     }
     __syncthreads();
-    ms_sweep(T, ldt, Z, n, l, ib, s, sm);
+    ms_sweep(T, ldt, Z, n, l, ib, s, sm, tm);
     if (++sweeps > budget) return RCWA_ERR_NOCONV;
   }
   return 0;
@@ -1318,19 +1431,35 @@ __global__ void __launch_bounds__(kMsThreads) schur_ms_kernel(cplx* const* Aarr,
     sm.ls[b * kMsLog + kMsW] = mkc(0.0, 0.0);
   }
   __syncthreads();
-  cplx* A = Aarr[blockIdx.x];
-  const Scratch s = scratch_for(work, n, blockIdx.x);
+  // one matrix per team (cluster) of CTAs
+  const Team tm = cluster_team();
+  const int mb = blockIdx.x / tm.size;
+  cplx* A = Aarr[mb];
+  const Scratch s = scratch_for(work, n, mb);
+  // the team's decisions go through the reflector scalars' storage, dead
+  // after the Hessenberg reduction (n >= 64 doubles)
+  int* ctrl = reinterpret_cast<int*>(s.tau);
 #ifdef RCWA_EIG_STATS
   const long long c_schur = clock64();
 #endif
-  const int status = hessenberg_finite(A, lda, n, sm.redi) ? schur_ms(A, lda, s.Z, n, ms_min, sm, sweep_cap)
-                                                          : RCWA_ERR_NONFINITE;
+  bool fin = false;
+  if (tm.rank == 0) {
+    fin = hessenberg_finite(A, lda, n, sm.redi);
+    if (tm.size > 1 && threadIdx.x == 0) ctrl[5] = fin ? 1 : 0;
+  }
+  if (tm.size > 1) {
+    tm.sync();
+    fin = __ldcg(ctrl + 5) != 0;
+  }
+  const int status = fin ? schur_ms(A, lda, s.Z, n, ms_min, sm, sweep_cap, tm, ctrl) : RCWA_ERR_NONFINITE;
 #ifdef RCWA_EIG_STATS
   STAT_ADD(10, clock64() - c_schur);
 #endif
-  cplx* w = w_all + (size_t)blockIdx.x * n;
-  for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = A[(size_t)k * lda + k];
-  if (threadIdx.x == 0) info_all[blockIdx.x] = status;
+  if (tm.rank == 0) {
+    cplx* w = w_all + (size_t)mb * n;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) w[k] = A[(size_t)k * lda + k];
+    if (threadIdx.x == 0) info_all[mb] = status;
+  }
 }
 
 // ---------------------------------------------------------------- eigenvectors
@@ -1417,11 +1546,15 @@ __device__ void trevc_blocked(const cplx* T, int ldt, cplx* X, int n, TileSmem& 
 // the first 256 threads also run the tile products.
 constexpr int kHessThreads = 512;
 
+template <bool kTeam>
 __global__ void __launch_bounds__(kHessThreads) hessenberg_kernel(cplx* const* Aarr, int n, int lda, void* work) {
   __shared__ double red[kHessThreads / 32];
   __shared__ TileSmem tsm;
-  const Scratch s = scratch_for(work, n, blockIdx.x);
-  hessenberg_blocked(Aarr[blockIdx.x], n, lda, s, red, tsm);
+  // one matrix per team (cluster) of CTAs
+  const Team tm = kTeam ? cluster_team() : Team{0, 1};
+  const int mb = blockIdx.x / tm.size;
+  const Scratch s = scratch_for(work, n, mb);
+  hessenberg_blocked<kTeam>(Aarr[mb], n, lda, s, red, tsm, tm);
 }
 
 __global__ void __launch_bounds__(kEigThreads) schur_kernel(cplx* const* Aarr, int n, int lda, cplx* w_all,
@@ -1467,12 +1600,101 @@ namespace {
 // QR sweep cap of every later eigensolve (0: the built-in budget), set by
 // rcwa_set_qr_sweep_limit; read when the Schur kernels are launched.
 std::atomic<int> g_qr_sweep_cap{0};
+// CTAs per matrix of the Hessenberg and multishift Schur kernels (0: the
+// automatic choice), set by rcwa_set_eig_cluster.
+std::atomic<int> g_eig_team{0};
+
+// Matrices of at least this order use a team of CTAs when the batch leaves
+// SMs idle.
+constexpr int kTeamMinN = 1024;
+
+// Clusters of `size` CTAs of `kernel` that fit on the device at once.
+template <class K>
+int active_clusters(K kernel, int threads, size_t smem, int size) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(size);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = size;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int nc = 0;
+  if (cudaOccupancyMaxActiveClusters(&nc, (void*)kernel, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nc;
+}
+
+// Team size for a batch of order-n matrices: the largest (up to 8) whose
+// clusters of both kernels all fit on the device in one wave, when the batch
+// alone would leave at least half of the SMs idle; 1 otherwise.
+int eig_team_size(int n, int batch, int ms_smem) {
+  const int forced = g_eig_team.load();
+  if (forced > 0) return forced;
+  if (n < kTeamMinN) return 1;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (2 * batch > sms) return 1;
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, int> cache;  // (device, batch) -> size
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find({dev, batch});
+  if (it != cache.end()) return it->second;
+  int pick = 1;
+  for (int c = std::min(8, sms / batch); c >= 2; --c)
+    if (active_clusters(hessenberg_kernel<true>, kHessThreads, 0, c) >= batch &&
+        active_clusters(schur_ms_kernel, kMsThreads, (size_t)ms_smem, c) >= batch) {
+      pick = c;
+      break;
+    }
+  cache[{dev, batch}] = pick;
+  return pick;
+}
+
+// launch of kernel over batch * team CTAs in clusters of `team`
+template <class K, class... Args>
+cudaError_t launch_team(K kernel, int batch, int team, int threads, size_t smem, cudaStream_t st, Args... args) {
+  if (team <= 1) {
+    kernel<<<batch, threads, smem, st>>>(args...);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(batch * team);
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = team;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
 }  // namespace
 
 extern "C" int rcwa_set_qr_sweep_limit(int sweeps) {
   if (sweeps < 0) return RCWA_ERR_INVALID;
   g_qr_sweep_cap.store(sweeps);
   return RCWA_OK;
+}
+
+extern "C" int rcwa_set_eig_cluster(int ctas) {
+  if (ctas < 0 || ctas > 8) return RCWA_ERR_INVALID;
+  g_eig_team.store(ctas);
+  return RCWA_OK;
+}
+
+extern "C" int rcwa_eig_cluster_size(int n, int batch) {
+  if (n < kMsMin || batch <= 0) return 1;
+  return eig_team_size(n, batch, (int)kMsSmemBytes);
 }
 
 cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* VR, int ldv, void* work,
@@ -1482,17 +1704,24 @@ cudaError_t zgeev_batched(cplx* const* A, int n, int lda, cplx* w, cplx* const* 
   const int sweep_cap = g_qr_sweep_cap.load();
   StageProf none;
   StageProf& P = prof ? *prof : none;
-  hessenberg_kernel<<<batch, kHessThreads, 0, st>>>(A, n, lda, work);
+  static SmemAttrOnce attr;
+  cudaError_t e = attr.ensure(schur_ms_kernel, (int)kMsSmemBytes);
+  if (e != cudaSuccess) return e;
+  // a team of CTAs per matrix where the batch is too small to fill the GPU
+  // (the single-shift kernel for small orders always runs one CTA)
+  const int team = n < ms_min ? 1 : eig_team_size(n, batch, (int)kMsSmemBytes);
+  e = team > 1 ? launch_team(hessenberg_kernel<true>, batch, team, kHessThreads, 0, st, A, n, lda, work)
+               : launch_team(hessenberg_kernel<false>, batch, 1, kHessThreads, 0, st, A, n, lda, work);
+  if (e != cudaSuccess) return e;
   ++launch_counter();
   P.mark(st, kStHessenberg);
   if (n < ms_min) {
     schur_kernel<<<batch, kEigThreads, 0, st>>>(A, n, lda, w, work, info, sweep_cap);
     ++launch_counter();
   } else {
-    static SmemAttrOnce attr;
-    cudaError_t e = attr.ensure(schur_ms_kernel, (int)kMsSmemBytes);
-    if (e != cudaSuccess) return e;
-    schur_ms_kernel<<<batch, kMsThreads, kMsSmemBytes, st>>>(A, n, lda, w, work, info, ms_min, sweep_cap);
+    if ((e = launch_team(schur_ms_kernel, batch, team, kMsThreads, kMsSmemBytes, st, A, n, lda, w, work, info,
+                         ms_min, sweep_cap)) != cudaSuccess)
+      return e;
     ++launch_counter();
   }
   P.mark(st, kStSchur);

@@ -5,6 +5,13 @@
 // (K-slab of 16).  The same tile routine drives the trailing updates of the
 // one-CTA-per-matrix blocked LU and of the blocked triangular solves, so the
 // O(n^3) part of every factorisation runs as register-blocked FP64 FMAs.
+#include <algorithm>
+#include <atomic>
+#include <map>
+#include <mutex>
+
+#include <cooperative_groups.h>
+
 #include "linalg.cuh"
 #include "tile.cuh"
 
@@ -220,6 +227,152 @@ __global__ void __launch_bounds__(kLuPanelThreads) getrf_panel_kernel(cplx* cons
   if (threadIdx.x == 0) info_all[b] = info;
 }
 
+// Panel step of the multi-launch LU for few large matrices: a thread-block
+// cluster of C CTAs per matrix shares the panel.  Rows kb..n-1 are split into
+// C slices; per column every CTA finds the largest |re|+|im| of its slice
+// (smallest row on ties), the CTAs read each other's candidates from shared
+// memory (distributed shared memory of the cluster) and take the same pivot,
+// swap their share of the columns of the two rows, and after a cluster
+// barrier scale and update their own rows.  Every element gets the same
+// operations as in lu_panel, so the factors are identical.
+__global__ void __launch_bounds__(kLuPanelThreads) getrf_panel_team_kernel(cplx* const* Aarr, int n, int lda,
+                                                                          int kb, int jb, int* ipiv_all,
+                                                                          int* info_all) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  __shared__ double red_v[kLuPanelThreads / 32];
+  __shared__ int red_i[kLuPanelThreads / 32];
+  __shared__ double s_bv;  // this CTA's pivot candidate
+  __shared__ int s_bi;
+  __shared__ int s_piv;
+  __shared__ cplx prow[kLuPanel];
+  const int C = (int)cl.num_blocks(), rank = (int)cl.block_rank();
+  const int b = blockIdx.x / C;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  constexpr int kU = 8;
+  cplx* A = Aarr[b];
+  int* ipiv = ipiv_all + (size_t)b * n;
+  int info = kb == 0 ? 0 : __ldcg(info_all + b);
+  const int per = (n - kb + C - 1) / C;
+  const int lo = kb + rank * per, hi = min(n, lo + per);
+  const int cper = (n + C - 1) / C;
+  const int clo = rank * cper, chi = min(n, clo + cper);
+  double best = -1.0;
+  int bi = n;
+  for (int i0 = max(lo, kb) + tid; i0 < hi; i0 += kU * nthr) {
+    double v[kU];
+#pragma unroll
+    for (int q = 0; q < kU; ++q) {
+      const int i = i0 + q * nthr;
+      v[q] = i < hi ? cabs1(A[(size_t)i * lda + kb]) : -1.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kU; ++q)
+      if (v[q] > best) { best = v[q]; bi = i0 + q * nthr; }
+  }
+  const int ce = kb + jb;
+  for (int j = kb; j < ce; ++j) {
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, best, off);
+      const int oi = __shfl_down_sync(0xffffffffu, bi, off);
+      if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+    }
+    if ((tid & 31) == 0) { red_v[tid >> 5] = best; red_i[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      double bv = red_v[0];
+      int bix = red_i[0];
+      for (int w = 1; w < nthr / 32; ++w)
+        if (red_v[w] > bv || (red_v[w] == bv && red_i[w] < bix)) { bv = red_v[w]; bix = red_i[w]; }
+      s_bv = bv;
+      s_bi = bix;
+    }
+    cl.sync();
+    if (tid == 0) {
+      double bv = -1.0;
+      int bix = n;
+      for (int r = 0; r < C; ++r) {
+        const double v = *cl.map_shared_rank(&s_bv, r);
+        const int ix = *cl.map_shared_rank(&s_bi, r);
+        if (v > bv || (v == bv && ix < bix)) { bv = v; bix = ix; }
+      }
+      // a column of zeros below the diagonal keeps its row (lu_panel's
+      // candidate is row j then)
+      s_piv = bix < n ? bix : j;
+      if (rank == 0) ipiv[j] = s_piv;
+    }
+    __syncthreads();
+    const int p = s_piv;
+    if (p != j) {
+      for (int c = clo + tid; c < chi; c += nthr) {
+        cplx t = A[(size_t)j * lda + c];
+        A[(size_t)j * lda + c] = A[(size_t)p * lda + c];
+        A[(size_t)p * lda + c] = t;
+      }
+    }
+    // the swap is complete everywhere, and every CTA has read the candidates
+    cl.sync();
+    for (int c = j + tid; c < ce; c += nthr) prow[c - kb] = __ldcg(A + (size_t)j * lda + c);
+    __syncthreads();
+    const cplx piv = prow[j - kb];
+    const int r0 = max(lo, j + 1);
+    if (piv.x == 0.0 && piv.y == 0.0) {
+      if (info == 0) info = j + 1;
+    } else {
+      const cplx inv = cdiv(mkc(1.0, 0.0), piv);
+      for (int i0 = r0 + tid; i0 < hi; i0 += kU * nthr) {
+        cplx v[kU];
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int i = i0 + q * nthr;
+          if (i < hi) v[q] = A[(size_t)i * lda + j];
+        }
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int i = i0 + q * nthr;
+          if (i < hi) A[(size_t)i * lda + j] = cmul(v[q], inv);
+        }
+      }
+    }
+    __syncthreads();
+    best = -1.0;
+    bi = n;
+    const int w = ce - j - 1;
+    if (w > 0 && r0 < hi) {
+      const int total = (hi - r0) * w;
+      for (int base = tid; base < total; base += kU * nthr) {
+        cplx l[kU], a[kU];
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int idx = base + q * nthr;
+          if (idx < total) {
+            const int i = r0 + idx / w, c = j + 1 + idx % w;
+            l[q] = A[(size_t)i * lda + j];
+            a[q] = A[(size_t)i * lda + c];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < kU; ++q) {
+          const int idx = base + q * nthr;
+          if (idx < total) {
+            const int i = r0 + idx / w, c = j + 1 + idx % w;
+            const cplx v = cfma(cneg(l[q]), prow[c - kb], a[q]);
+            A[(size_t)i * lda + c] = v;
+            if (c == j + 1) {
+              const double av = cabs1(v);
+              if (av > best || (av == best && i < bi)) { best = av; bi = i; }
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (rank == 0 && tid == 0) info_all[b] = info;
+  // no CTA leaves while another may still read its candidate
+  cl.sync();
+}
+
 // U12 of the multi-launch LU: one CTA per (matrix, 64 columns right of the
 // panel), a thread per column; the unit lower L11 (jb <= kLuPanel) is read
 // through the read-only path (every thread reads the same entry).
@@ -404,6 +557,80 @@ int sm_count() {
 }
 }  // namespace
 
+namespace {
+// CTAs per matrix of the multi-launch LU's panel step (0: automatic), set by
+// rcwa_set_lu_cluster.
+std::atomic<int> g_lu_team{0};
+constexpr int kLuTeamMinN = 1024;
+
+int lu_team_size(int n, int batch) {
+  const int forced = g_lu_team.load();
+  if (forced > 0) return forced;
+  const int sms = sm_count();
+  if (n < kLuTeamMinN || 2 * batch > sms) return 1;
+  static std::mutex mu;
+  static std::map<int, int> cache;  // batch -> size
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(batch);
+  if (it != cache.end()) return it->second;
+  int pick = 1;
+  for (int c = std::min(8, sms / batch); c >= 2; --c) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(c);
+    cfg.blockDim = dim3(kLuPanelThreads);
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = c;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, (void*)getrf_panel_team_kernel, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (nc >= batch) {
+      pick = c;
+      break;
+    }
+  }
+  cache[batch] = pick;
+  return pick;
+}
+
+cudaError_t launch_panel(cplx* const* A, int n, int lda, int kb, int jb, int* ipiv, int* info, int batch, int team,
+                         cudaStream_t st) {
+  if (team <= 1) {
+    getrf_panel_kernel<<<batch, kLuPanelThreads, 0, st>>>(A, n, lda, kb, jb, ipiv, info);
+    return cudaGetLastError();
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(batch * team);
+  cfg.blockDim = dim3(kLuPanelThreads);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = team;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, getrf_panel_team_kernel, A, n, lda, kb, jb, ipiv, info);
+}
+}  // namespace
+
+extern "C" int rcwa_set_lu_cluster(int ctas) {
+  if (ctas < 0 || ctas > 8) return RCWA_ERR_INVALID;
+  g_lu_team.store(ctas);
+  return RCWA_OK;
+}
+
+extern "C" int rcwa_lu_cluster_size(int n, int batch) {
+  if (batch <= 0 || n <= 0) return 1;
+  return lu_team_size(n, batch);
+}
+
 int zgetrf_default_schedule(int n, int batch, int sms) {
   if (sms <= 0) sms = sm_count();
   return (n <= 128 || batch >= 4 * sms) ? 0 : 1;
@@ -418,9 +645,12 @@ cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info,
     ++launch_counter();
     return cudaGetLastError();
   }
+  // a cluster of CTAs per matrix shares each panel when the batch leaves SMs idle
+  const int team = lu_team_size(n, batch);
   for (int kb = 0; kb < n; kb += kLuPanel) {
     const int jb = min(kLuPanel, n - kb);
-    getrf_panel_kernel<<<batch, kLuPanelThreads, 0, st>>>(A, n, lda, kb, jb, ipiv, info);
+    cudaError_t pe = launch_panel(A, n, lda, kb, jb, ipiv, info, batch, team, st);
+    if (pe != cudaSuccess) return pe;
     ++launch_counter();
     const int m2 = n - kb - jb;
     if (m2 <= 0) break;

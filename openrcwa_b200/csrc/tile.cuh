@@ -42,7 +42,9 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
                : "d"(a), "d"(b));
 }
 
-template <bool TA, bool TB>
+// kL2: every operand load goes to L2 (ld.global.cg), for operands written by
+// other CTAs of a cluster earlier in the same kernel.
+template <bool TA, bool TB, bool kL2 = false>
 __device__ __forceinline__ void tile_fetch(const cplx* __restrict__ A, int lda, const cplx* __restrict__ B, int ldb,
                                            const cplx* __restrict__ s, int M, int N, int K, int m0, int n0, int k0,
                                            cplx pa[4], cplx pb[4]) {
@@ -55,7 +57,10 @@ __device__ __forceinline__ void tile_fetch(const cplx* __restrict__ A, int lda, 
     else { mm = idx & 63; kk = idx >> 6; }
     const int gm = m0 + mm, gk = k0 + kk;
     cplx v = mkc(0.0, 0.0);
-    if (gm < M && gk < K) v = TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk];
+    if (gm < M && gk < K) {
+      const cplx* pa_ = TA ? A + (size_t)gk * lda + gm : A + (size_t)gm * lda + gk;
+      v = kL2 ? __ldcg(pa_) : *pa_;
+    }
     pa[r] = v;
   }
 #pragma unroll
@@ -67,8 +72,9 @@ __device__ __forceinline__ void tile_fetch(const cplx* __restrict__ A, int lda, 
     const int gn = n0 + nn, gk = k0 + kk;
     cplx v = mkc(0.0, 0.0);
     if (gn < N && gk < K) {
-      v = TB ? B[(size_t)gn * ldb + gk] : B[(size_t)gk * ldb + gn];
-      if (s) v = cmul(s[gk], v);
+      const cplx* pb_ = TB ? B + (size_t)gn * ldb + gk : B + (size_t)gk * ldb + gn;
+      v = kL2 ? __ldcg(pb_) : *pb_;
+      if (s) v = cmul(kL2 ? __ldcg(s + gk) : s[gk], v);
     }
     pb[r] = v;
   }
@@ -102,7 +108,7 @@ __device__ __forceinline__ void tile_stage(TileSmem& sm, const cplx pa[4], const
 // row-major operand.  Out-of-range elements read as zero.  The first
 // kTileThreads threads of the CTA must all call this (it contains
 // tile_barrier).
-template <bool TA, bool TB>
+template <bool TA, bool TB, bool kL2 = false>
 __device__ __forceinline__ void tile_mma(TileSmem& sm, cplx acc[4][4], const cplx* __restrict__ A, int lda,
                                          const cplx* __restrict__ B, int ldb, const cplx* __restrict__ s,
                                          int M, int N, int K, int m0, int n0) {
@@ -111,12 +117,12 @@ __device__ __forceinline__ void tile_mma(TileSmem& sm, cplx acc[4][4], const cpl
   const int g = lane >> 2, t = lane & 3;
   const int wm = 16 * (w & 3), wn = 32 * (w >> 2);
   cplx pa[4], pb[4];
-  tile_fetch<TA, TB>(A, lda, B, ldb, s, M, N, K, m0, n0, 0, pa, pb);
+  tile_fetch<TA, TB, kL2>(A, lda, B, ldb, s, M, N, K, m0, n0, 0, pa, pb);
   tile_stage<TA, TB>(sm, pa, pb);
   tile_barrier();
   for (int k0 = 0; k0 < K; k0 += kTBK) {
     const bool more = k0 + kTBK < K;
-    if (more) tile_fetch<TA, TB>(A, lda, B, ldb, s, M, N, K, m0, n0, k0 + kTBK, pa, pb);
+    if (more) tile_fetch<TA, TB, kL2>(A, lda, B, ldb, s, M, N, K, m0, n0, k0 + kTBK, pa, pb);
 #pragma unroll
     for (int k4 = 0; k4 < kTBK; k4 += 4) {
       double ar[2], ai[2], an[2], br[4], bi[4];
