@@ -76,6 +76,8 @@ def parse():
                          "Nx=Ny=25 (2601 orders, 5202 x 5202 layer matrices), POINTS of its 32 wavelengths at "
                          "normal incidence, TE+TM, one plan execution")
     ap.add_argument("--cfg5-nh", type=int, default=25, help="harmonics per axis of --cfg5 (25: the full order)")
+    ap.add_argument("--cfg5-lossless", action="store_true",
+                    help="--cfg5 with lossless layers on the FP64 plan (checks |R + T - 1|)")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
                     help="profiling aid: one batched eigensolve of BATCH random N x N matrices, no timing line")
     return ap.parse_args()
@@ -337,21 +339,28 @@ def run_cfg5(args):
     executed once after a small warm-up plan (module loading), with stage
     timing; solves/s from the device time (CUDA events on the launching
     stream), and two size-independent checks: TE = TM (a centred disk is C4
-    symmetric and the incidence is normal) and 0 <= R, T, R + T <= 1."""
+    symmetric and the incidence is normal) and 0 <= R, T, R + T <= 1.  With
+    --cfg5-lossless the layers are lossless and the plan FP64: |R + T - 1| is
+    then the check.  The roofline is the Schur stage (nominal 81.33 n^3 flops
+    per matrix) against the DGEMM rate measured in the same run."""
     import torch
     import openrcwa_b200 as o
     from openrcwa_b200 import workloads
     nh, npts = args.cfg5_nh, args.cfg5
-    stacks, pts, pxy = workloads.circular_pillars(seed=0, nH=nh)
+    lossless = args.cfg5_lossless
+    prec = o.RCWA_PREC_FP64 if lossless else o.RCWA_PREC_MIXED
+    stacks, pts, pxy = workloads.circular_pillars(seed=0, nH=nh, lossless=lossless)
     eng = o.Engine(0)
     stream = torch.cuda.Stream()
     ws, wp, wx = workloads.circular_pillars(seed=0, nH=3, n_lambda=2, n_layers=3)
-    w = eng.plan(ws, wp, wx, precision=o.RCWA_PREC_MIXED)
+    w = eng.plan(ws, wp, wx, precision=prec)
     w.execute(stream.cuda_stream)
     stream.synchronize()
     w.close()
+    fp64_peak = fp64_gemm_peak_tflops(torch)
+    torch.cuda.empty_cache()
     t0 = time.perf_counter()
-    plan = eng.plan(stacks, pts[:npts], pxy[:npts], precision=o.RCWA_PREC_MIXED)
+    plan = eng.plan(stacks, pts[:npts], pxy[:npts], precision=prec)
     t_create = time.perf_counter() - t0
     plan.set_profiling(True)
     e0 = torch.cuda.Event(enable_timing=True)
@@ -370,19 +379,33 @@ def run_cfg5(args):
     plan.close()
     eng.close()
     n = 2 * stacks[0].N
-    print(json.dumps({"cfg5": {
+    nj = int(npts * (stacks[0].thickness.size - 2))
+    schur_flops = 81.33 * float(n) ** 3 * nj
+    out = {
         "workload": "20 circular-pillar layers (closed-form disk Laurent tables, radius/period U(0.2, 0.45), "
-                    "thickness U(20, 100) nm, eps1 alternating 4.0 / 2.1+0.01i, eps2 1), substrate 2.25, period "
+                    "thickness U(20, 100) nm, eps1 alternating 4.0 / %s, eps2 1), substrate 2.25, period "
                     "400 nm, Nx=Ny=%d (%d orders, %d x %d layer matrices), first %d of 32 wavelengths 500-900 nm, "
-                    "normal incidence, TE+TM" % (nh, stacks[0].N, n, n, npts),
-        "precision": "mixed: cascade products 3xTF32 on tcgen05, eigensolve and solves FP64",
+                    "normal incidence, TE+TM" % ("2.1" if lossless else "2.1+0.01i", nh, stacks[0].N, n, n, npts),
+        "precision": ("fp64" if lossless else
+                      "mixed: cascade products 3xTF32 on tcgen05, eigensolve and solves FP64"),
         "solves_per_s": npts / (ms * 1e-3), "ms_per_execution": ms, "plan_create_s": t_create,
-        "chunks": len(chunks), "eigensolves": int(npts * (stacks[0].thickness.size - 2)),
+        "chunks": len(chunks), "eigensolves": nj,
+        "ctas_per_matrix": {"eigensolver": o.eig_cluster_size(n, nj // max(1, len(chunks))),
+                            "lu_panel_interfaces": o.lu_cluster_size(n, 2),
+                            "lu_panel_tau": o.lu_cluster_size(n, 1)},
         "stage_ms": {k: round(v, 1) for k, v in stages.items() if v > 1.0},
+        "roofline": {"kernel": "schur_qr", "bound": "tensor", "achieved": schur_flops / (stages["schur_qr"] * 1e9),
+                     "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": schur_flops / (stages["schur_qr"] * 1e9) / fp64_peak,
+                     "peak_source": "FP64 DGEMM measured in this run (cuBLAS via torch)",
+                     "note": "nominal 81.33 n^3 flops per matrix (LAPACK's count for the standard QR iteration)"},
         "status_max": int(status.max()),
         "max_abs_TE_minus_TM": float(np.max(np.abs(R[:, 0] - R[:, 1]))),
         "R_range": [float(R.min()), float(R.max())], "R_plus_T_max": float(np.max(R + T)),
-        "clocks": clk}}), flush=True)
+        "clocks": clk}
+    if lossless:
+        out["max_abs_R_plus_T_minus_1"] = float(np.max(np.abs(R + T - 1.0)))
+    print(json.dumps({"cfg5": out}), flush=True)
     return 0 if status.max() == 0 else 1
 
 

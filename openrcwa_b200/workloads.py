@@ -144,20 +144,20 @@ def disk_laurent_table(Lx, Ly, radius, center, eps1, eps2, nH):
     return F.astype(np.complex128)
 
 
-def circular_pillars(seed=0, nH=25, n_lambda=32, n_layers=20, period=4e-7):
+def circular_pillars(seed=0, nH=25, n_lambda=32, n_layers=20, period=4e-7, lossless=False):
     """Large-order single structure: n_layers circular-pillar layers (one disk
     per layer centred in the cell, radius/period ~U(0.2, 0.45), thickness
-    ~U(20, 100) nm, eps1 alternating 4.0 and 2.1+0.01i, eps2 = 1) between a
-    superstrate of eps 1 and a substrate of 2.25, period x period cells
-    (400 nm), 2nH+1 orders per axis; n_lambda wavelengths 500-900 nm at normal
-    incidence, TE and TM.  The layers' Laurent tables are the closed-form disk
-    transform.  Returns ([TableStack], points, pxy)."""
+    ~U(20, 100) nm, eps1 alternating 4.0 and 2.1+0.01i (2.1 when lossless),
+    eps2 = 1) between a superstrate of eps 1 and a substrate of 2.25, period x
+    period cells (400 nm), 2nH+1 orders per axis; n_lambda wavelengths
+    500-900 nm at normal incidence, TE and TM.  The layers' Laurent tables are
+    the closed-form disk transform.  Returns ([TableStack], points, pxy)."""
     rng = np.random.default_rng(seed)
     f2d, thick = [], [0.0]
     for k in range(n_layers):
         r = rng.uniform(0.2, 0.45) * period
         d = rng.uniform(20e-9, 100e-9)
-        e1 = 4.0 if k % 2 == 0 else complex(2.1, 0.01)
+        e1 = 4.0 if k % 2 == 0 else complex(2.1, 0.0 if lossless else 0.01)
         f2d.append(disk_laurent_table(period, period, r, (0.5 * period, 0.5 * period), e1, 1.0, nH))
         thick.append(d)
     thick.append(0.0)
