@@ -6,16 +6,21 @@
 // rcwa/RCWADriver.cpp:284-339).  solve() runs the whole layer / interface /
 // cascade computation on the device through the C ABI and keeps the
 // scattering matrices there; every scatterPlaneWave after it only re-evaluates
-// the efficiencies for the new incident vector.  The modal basis of the
-// uniform half-spaces is the identity here, so the amplitude vector c of
-// generateHorizontalPlaneWave is [px delta; py delta].
+// the efficiencies for the new incident vector.  generateHorizontalPlaneWave
+// returns the plane wave's tangential field [px delta; py delta] and
+// scatterPlaneWave takes it as such: the engine itself applies the
+// incidence layer's modal basis (the identity for a uniform half-space,
+// W_ref^-1 for a patterned one), so the efficiencies are the reference's
+// while c holds the field rather than the modal amplitudes of a patterned
+// incidence layer.
 //
 // Tdd() and Rud() copy the solved scattering matrices from the device on
 // first access after solve().
 //
 // Outside this engine (they report on std::cerr and leave outputs empty):
-// PML (enablePML), layer translations, non-uniform half-spaces, incident vectors other than generateHorizontalPlaneWave's and
-// the field images (saveFieldImage, saveDeviceImage).
+// PML (enablePML), layer translations, incident vectors other than
+// generateHorizontalPlaneWave's and the field images (saveFieldImage,
+// saveDeviceImage).
 #pragma once
 #include <algorithm>
 #include <cmath>

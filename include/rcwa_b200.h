@@ -56,8 +56,11 @@ typedef struct rcwa_plan rcwa_plan;
  * addLayer() of every layer (rcwa/RCWASolver.h:67-84, rcwa/Layer.h:29-31).
  * eps[l] is a (ncy-1) x (ncx-1) row-major grid, row = y strip, column = x
  * strip, exactly the Layer eps_ matrix.  Layer 0 is the incidence half-space,
- * layer n_layers-1 the transmission half-space; both must be uniform (every
- * cell equal), as sol/rcwa_bridge.cpp:255-259 assumes.  thickness[l] is used
+ * layer n_layers-1 the transmission half-space.  A uniform half-space (every
+ * cell equal) takes closed-form modes; one whose cells differ is solved like
+ * a patterned layer, as the reference solves every layer type
+ * (rcwa/RCWASolver.cpp:194-210), and its values at (0, 0) enter the
+ * efficiencies (rcwa/RCWASolver.cpp:1823-1830).  thickness[l] is used
  * for 0 < l < n_layers-1 only (rcwa/RCWASolver.cpp:415-431).  mu, when not
  * NULL, is the relative permeability on the same grid (Layer(coordX, coordY,
  * eps, mu), rcwa/Layer.cpp:41-72): a layer with a cell whose mu differs from 1

@@ -757,7 +757,11 @@ __device__ void small_eigs_warp(cplx* B, int ldb, int s, cplx* out) {
 // deflated, the others are moved to the top by adjacent swaps and serve as
 // shifts; the spike of the undeflated part is reflected onto its first entry
 // and that part is returned to Hessenberg form by Householder reflectors.
-constexpr int kAedW = 32;        // window order (one lane per column)
+#ifndef RCWA_AED_WINDOW
+#define RCWA_AED_WINDOW 32
+#endif
+constexpr int kAedW = RCWA_AED_WINDOW;  // window order (one lane per column; a build-time parameter)
+static_assert(kAedW <= 32 && kAedW >= kMsShifts + 2, "the early-deflation window is one warp wide");
 constexpr int kAedLd = kAedW + 1;
 constexpr int kAedNibble = 14;   // percent of the window deflated that skips the sweep
 static_assert(sizeof(cplx) * (2 * kAedW * kAedLd + kAedW) <= kMsRegion &&

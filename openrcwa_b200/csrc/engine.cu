@@ -103,6 +103,10 @@ struct StackInfo {
   std::vector<cplx> mu;
   std::vector<char> mag;
   std::vector<double> thick;
+  // a half-space whose cells differ (incidence side, transmission side): its
+  // modes come from the eigensolver like a patterned layer's, as in the
+  // reference, which solves every layer type (rcwa/RCWASolver.cpp:194-210)
+  char pat0 = 0, patL = 0;
   int ncx, ncy;
   // stacks given by Laurent tables: one (2nx-1) x (2ny-1) table per
   // patterned layer (layers 1..L-2); the cell grid is then one cell per layer
@@ -184,17 +188,7 @@ int validate_stack(const rcwa_stack& s, std::string& why) {
         if (!finite_c(z)) { why = "non-finite permeability"; return RCWA_ERR_NONFINITE; }
         if (z.re == 0.0 && z.im == 0.0) { why = "zero permeability"; return RCWA_ERR_INVALID; }
       }
-    if (l == 0 || l == s.n_layers - 1) {
-      const rcwa_cplx z0 = s.eps[(size_t)l * cells];
-      for (size_t c = 1; c < cells; ++c) {
-        const rcwa_cplx z = s.eps[(size_t)l * cells + c];
-        if (z.re != z0.re || z.im != z0.im) { why = "half-spaces must be uniform"; return RCWA_ERR_UNSUPPORTED; }
-        if (s.mu) {
-          const rcwa_cplx m0 = s.mu[(size_t)l * cells], m = s.mu[(size_t)l * cells + c];
-          if (m.re != m0.re || m.im != m0.im) { why = "half-spaces must be uniform"; return RCWA_ERR_UNSUPPORTED; }
-        }
-      }
-    } else if (!std::isfinite(s.thickness[l]) || s.thickness[l] < 0) {
+    if (l > 0 && l < s.n_layers - 1 && (!std::isfinite(s.thickness[l]) || s.thickness[l] < 0)) {
       why = "invalid thickness";
       return RCWA_ERR_INVALID;
     }
@@ -230,7 +224,47 @@ StackInfo make_stack_info(const rcwa_stack& s) {
     si.mu.resize(cells * s.n_layers);
     for (size_t i = 0; i < si.mu.size(); ++i) si.mu[i] = mkc(s.mu[i].re, s.mu[i].im);
   }
+  for (int side = 0; side < 2; ++side) {
+    const size_t l = side == 0 ? 0 : (size_t)s.n_layers - 1;
+    bool pat = false;
+    for (size_t c = 1; c < cells && !pat; ++c) {
+      const rcwa_cplx z = s.eps[l * cells + c], z0 = s.eps[l * cells];
+      pat = z.re != z0.re || z.im != z0.im;
+      if (s.mu) {
+        const rcwa_cplx m = s.mu[l * cells + c], m0 = s.mu[l * cells];
+        pat = pat || m.re != m0.re || m.im != m0.im;
+      }
+    }
+    (side == 0 ? si.pat0 : si.patL) = pat ? 1 : 0;
+  }
   return si;
+}
+
+// layers whose modes come from the eigensolver: the patterned layers, and a
+// half-space whose cells differ
+std::vector<int> eig_layers(const StackInfo& si) {
+  std::vector<int> ls;
+  if (si.pat0) ls.push_back(0);
+  for (int l = 1; l + 1 < si.L; ++l) ls.push_back(l);
+  if (si.patL && si.L > 1) ls.push_back(si.L - 1);
+  return ls;
+}
+
+// Layer::eps(x, y) / Layer::mu(x, y): the cell containing (x, y), x periodic,
+// y outside the grid gives 0 (rcwa/Layer.cpp:383-450); used for the
+// efficiencies of a patterned half-space (scatterPlaneWave takes its values
+// at (0, 0), rcwa/RCWASolver.cpp:1823-1827)
+cplx cell_value(const StackInfo& si, const std::vector<cplx>& f, int l, double x, double y) {
+  const double Lx = si.cx.back() - si.cx.front();
+  while (x < si.cx.front()) x += Lx;
+  while (x > si.cx.back()) x -= Lx;
+  if (y < si.cy.front() || y > si.cy.back()) return mkc(0.0, 0.0);
+  int ix = 0, iy = 0;
+  for (int i = 0; i + 1 < si.ncx; ++i)
+    if (x <= si.cx[i + 1]) { ix = i; break; }
+  for (int j = 0; j + 1 < si.ncy; ++j)
+    if (y <= si.cy[j + 1]) { iy = j; break; }
+  return f[(size_t)l * (si.ncx - 1) * (si.ncy - 1) + (size_t)iy * (si.ncx - 1) + ix];
 }
 
 bool is_mag(const StackInfo& si, int l) { return !si.mag.empty() && si.mag[l]; }
@@ -642,7 +676,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
     for (int p : g.second) {
       const StackInfo& sp = si[pts[p].stack];
       const int Lm = (int)std::count(sp.mag.begin(), sp.mag.end(), (char)1);
-      const size_t need = chunk_bytes_per_point(N, sp.L, Lm, precision == RCWA_PREC_MIXED);
+      const size_t need = chunk_bytes_per_point(N, sp.L + sp.pat0 + sp.patL, Lm, precision == RCWA_PREC_MIXED);
       if (!cur.points.empty() && (used + need > budget || cur.points.size() >= 1024)) flush();
       cur.points.push_back(p);
       used += need;
@@ -656,7 +690,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       const int s = pts[p].stack;
       c.max_ncx = std::max(c.max_ncx, si[s].ncx);
       c.max_ncy = std::max(c.max_ncy, si[s].ncy);
-      for (int l = 1; l + 1 < si[s].L; ++l) {
+      for (int l : eig_layers(si[s])) {
         for (int k = 0; k < (is_mag(si[s], l) ? 2 : 1); ++k) {
           auto key = std::make_pair(s, l + k * kMuJob);
           if (!c.conv_index.count(key)) {
@@ -778,7 +812,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         pf.mark(st, kStConvGather);
         return err;
       });
-      // E = fe33^-1: LU in place, then solve against the identity
+      // E = fe33^-1: LU in place, then the inverse in the getri order
       std::vector<cplx*> f33(nconv), einv(nconv);
       for (int j = 0; j < nconv; ++j) { f33[j] = W_(c.fe33) + NN * j; einv[j] = W_(c.Einv) + NN * j; }
       const size_t o33 = meta.add_vec(f33), oE = meta.add_vec(einv);
@@ -789,8 +823,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         cplx* const* b = (cplx* const*)((char*)plan->meta.p + oE);
         cudaError_t err;
         if ((err = zgetrf_batched(a, N, N, cipiv, cinfo, nconv, st)) != cudaSuccess) return err;
-        if ((err = zset_identity_batched(b, N, N, nconv, st)) != cudaSuccess) return err;
-        err = zgetrs_batched(a, N, N, cipiv, b, N, N, nconv, st);
+        err = zgetri_batched(a, N, N, cipiv, b, N, nconv, st);
         pf.mark(st, kStConvInverse);
         return err;
       });
@@ -1008,18 +1041,18 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       // layer buffers of point lp, layer l
       auto layerW = [&](int lp, int l) -> cplx* {
         const int p = c.points[lp];
-        const int L = si[pts[p].stack].L;
-        if (l == 0) return W_(c.hW0) + nn * lp;
-        if (l == L - 1) return W_(c.hWL) + nn * lp;
+        const StackInfo& sl = si[pts[p].stack];
+        if (l == 0 && !sl.pat0) return W_(c.hW0) + nn * lp;
+        if (l == sl.L - 1 && !sl.patL) return W_(c.hWL) + nn * lp;
         for (size_t j = 0; j < c.job_point.size(); ++j)
           if (c.job_point[j] == lp && c.job_layer[j] == l) return W_(c.W) + nn * j;
         return nullptr;
       };
       auto layerV = [&](int lp, int l) -> cplx* {
         const int p = c.points[lp];
-        const int L = si[pts[p].stack].L;
-        if (l == 0) return W_(c.hV0) + nn * lp;
-        if (l == L - 1) return W_(c.hVL) + nn * lp;
+        const StackInfo& sl = si[pts[p].stack];
+        if (l == 0 && !sl.pat0) return W_(c.hV0) + nn * lp;
+        if (l == sl.L - 1 && !sl.patL) return W_(c.hVL) + nn * lp;
         for (size_t j = 0; j < c.job_point.size(); ++j)
           if (c.job_point[j] == lp && c.job_layer[j] == l) return W_(c.V) + nn * j;
         return nullptr;
@@ -1062,7 +1095,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           cplx* VLU = W_(c.VLU) + nn * lp;
           csrc.push_back(layerW(lp, b)); cdst.push_back(IE);
           csrc.push_back(layerV(lp, b)); cdst.push_back(IH);
-          if (a == 0) {
+          if (a == 0 && !si[pts[p].stack].pat0) {
             HalfSolveItem h;
             h.X = IH;
             h.V0 = layerV(lp, 0);
@@ -1182,8 +1215,8 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           if ((err = fold_info(pinfo, (const int*)(m + osp), k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStTauLU);
-          if ((err = zset_identity_batched(pa(otau), n, n, k, st)) != cudaSuccess) return err;
-          if ((err = zgetrs_batched(cpa(oSp), n, n, pipiv, pa(otau), n, n, k, st)) != cudaSuccess) return err;
+          // tau = (F + G)^-1 in the getri order (PartialPivLU::inverse, :451-453)
+          if ((err = zgetri_batched(cpa(oSp), n, n, pipiv, pa(otau), n, k, st)) != cudaSuccess) return err;
           pf.mark(st, kStTau);
           // Rud = I - 2 G tau ; Tdd = 2 waveTdd tau  (:457-460)
           g.A = cpa(otG); g.B = cpa(otTau); g.C = nullptr; g.D = pa(orD);
@@ -1196,6 +1229,79 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           return err;
         });
       }
+      // ---------------- responses of points with a patterned half-space
+      // C = W_ref^-1 [e_inc, e_N+inc] (LU of a copy of W_ref), then
+      // Rc = W_ref (Rud C), Tc = W_trn (Tdd C): the harmonics of
+      // generateHorizontalPlaneWave's plane wave (rcwa/Layer.cpp:453-480)
+      // scattered into both half-spaces (rcwa/RCWASolver.cpp:1806-1811).
+      // Buffers of the finished cascade hold them: the W_ref copy in WLU, C
+      // in F, Rud C in IE, Tdd C in IH, Rc in tau, Tc in VLU (n x 2 each).
+      std::vector<int> qpts;
+      for (int lp = 0; lp < np; ++lp) {
+        const StackInfo& sl = si[pts[c.points[lp]].stack];
+        if (sl.pat0 || sl.patL) qpts.push_back(lp);
+      }
+      std::vector<cplx*> rc_of(np, nullptr), tc_of(np, nullptr);
+      if (!qpts.empty()) {
+        const int nq = (int)qpts.size();
+        const int inc = ny * ((nx - 1) / 2) + (ny - 1) / 2;
+        std::vector<const cplx*> w0(nq), rA(nq), tA(nq), wt(nq);
+        std::vector<cplx*> wlu(nq), cb(nq), r1(nq), t1(nq), rcp(nq), tcp(nq);
+        std::vector<int> qpoint(nq);
+        for (int q = 0; q < nq; ++q) {
+          const int lp = qpts[q];
+          const int L = si[pts[c.points[lp]].stack].L;
+          w0[q] = layerW(lp, 0);
+          wt[q] = layerW(lp, L - 1);
+          wlu[q] = W_(c.WLU) + nn * lp;
+          cb[q] = W_(c.F) + nn * lp;
+          r1[q] = W_(c.IE) + nn * lp;
+          t1[q] = W_(c.IH) + nn * lp;
+          rcp[q] = W_(c.tau) + nn * lp;
+          tcp[q] = W_(c.VLU) + nn * lp;
+          rA[q] = rud[lp];
+          tA[q] = tdd[lp];
+          qpoint[q] = c.points[lp];
+          rc_of[lp] = rcp[q];
+          tc_of[lp] = tcp[q];
+        }
+        const size_t ow0 = meta.add_vec(w0), owt = meta.add_vec(wt), owlu = meta.add_vec(wlu);
+        const size_t ocb = meta.add_vec(cb), or1 = meta.add_vec(r1), ot1 = meta.add_vec(t1);
+        const size_t orc = meta.add_vec(rcp), otc = meta.add_vec(tcp), orA = meta.add_vec(rA), otA = meta.add_vec(tA);
+        const size_t oqp = meta.add_vec(qpoint);
+        int* pipiv = (int*)(wb + c.pipiv);
+        int* pinfo = (int*)(wb + c.pinfo);
+        int* status = P->dStatus;
+        P->steps.push_back([=](cudaStream_t st, StageProf& pf) {
+          char* m = (char*)plan->meta.p;
+          auto cpa = [m](size_t o) { return (const cplx* const*)(m + o); };
+          auto pa = [m](size_t o) { return (cplx* const*)(m + o); };
+          cudaError_t err;
+          if ((err = zcopy_batched(cpa(ow0), n, pa(owlu), n, n, n, nq, st)) != cudaSuccess) return err;
+          if ((err = zgetrf_batched(pa(owlu), n, n, pipiv, pinfo, nq, st)) != cudaSuccess) return err;
+          if ((err = fold_info(pinfo, (const int*)(m + oqp), nq, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
+            return err;
+          // C = [e_inc, e_N+inc], then C = W_ref^-1 C
+          if ((err = unit_columns(pa(ocb), n, inc, N + inc, nq, st)) != cudaSuccess) return err;
+          if ((err = zgetrs_batched(cpa(owlu), n, n, pipiv, pa(ocb), 2, 2, nq, st)) != cudaSuccess) return err;
+          GemmArgs g{};
+          g.M = n; g.N = 2; g.K = n;
+          g.lda = n; g.ldb = 2; g.ldc = 2; g.ldd = 2;
+          g.alpha = mkc(1, 0); g.beta = mkc(0, 0); g.gammaI = mkc(0, 0);
+          g.batch = nq;
+          g.A = cpa(orA); g.B = cpa(ocb); g.D = pa(or1);
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          g.A = cpa(otA); g.B = cpa(ocb); g.D = pa(ot1);
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          g.A = cpa(ow0); g.B = cpa(or1); g.D = pa(orc);
+          if ((err = zgemm_batched(g, st)) != cudaSuccess) return err;
+          g.A = cpa(owt); g.B = cpa(ot1); g.D = pa(otc);
+          err = zgemm_batched(g, st);
+          pf.mark(st, kStScatter);
+          return err;
+        });
+      }
+
       // ---------------- scatter
       std::vector<ScatterItem> sc;
       for (int lp = 0; lp < np; ++lp) {
@@ -1208,9 +1314,18 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           it.ab = (const cplx*)(inb + ab_off[p]);
           // k^2 = k0^2 eps mu of the half-spaces, and the transmitted flux
           // ratio |mu_ref / mu_trn| (rcwa/RCWASolver.cpp:1826-1830, 1905-1907)
-          const cplx mr = layer_mu0(si[s], 0), mt = layer_mu0(si[s], si[s].L - 1);
-          it.n2_ref = cmul(si[s].eps[0], mr);
-          it.n2_trn = cmul(si[s].eps[(size_t)(si[s].L - 1) * cells], mt);
+          // (a patterned half-space: its values at (0, 0), Layer::eps(0, 0)
+          // and Layer::mu(0, 0), rcwa/RCWASolver.cpp:1823-1827)
+          const StackInfo& sk = si[s];
+          const int Lt = sk.L - 1;
+          const cplx mr = sk.pat0 && !sk.mu.empty() ? cell_value(sk, sk.mu, 0, 0.0, 0.0) : layer_mu0(sk, 0);
+          const cplx mt = sk.patL && !sk.mu.empty() ? cell_value(sk, sk.mu, Lt, 0.0, 0.0) : layer_mu0(sk, Lt);
+          const cplx er = sk.pat0 ? cell_value(sk, sk.eps, 0, 0.0, 0.0) : sk.eps[0];
+          const cplx et = sk.patL ? cell_value(sk, sk.eps, Lt, 0.0, 0.0) : sk.eps[(size_t)Lt * cells];
+          it.n2_ref = cmul(er, mr);
+          it.n2_trn = cmul(et, mt);
+          it.Rc = rc_of[lp];
+          it.Tc = tc_of[lp];
           it.trn_scale = (mr.x == mt.x && mr.y == mt.y)
                              ? 1.0
                              : std::abs(std::complex<double>(mr.x, mr.y) / std::complex<double>(mt.x, mt.y));

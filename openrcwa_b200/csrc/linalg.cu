@@ -400,6 +400,12 @@ __device__ __forceinline__ void load_block32(cplx (*Tsm)[33], const cplx* LU, in
   }
 }
 
+// kInv (the inverse, LAPACK getri order): B starts as the identity without
+// the row interchanges, so column c of L^-1 is zero above row c and the
+// forward pass of the slab starting at column c0 begins at row c0 with its
+// long-K products cut to K = c0 .. rb; the column interchanges follow in
+// zcolperm_kernel.  This saves a third of the flops of solving against P.
+template <bool kInv>
 __global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const* LUarr, int n, int lda,
                                                              const int* ipiv_all, cplx* const* Barr,
                                                              int nrhs, int ldb) {
@@ -413,7 +419,12 @@ __global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const*
   const cplx* LU = LUarr[b];
   const int* ipiv = ipiv_all + (size_t)b * n;
   cplx* B = Barr[b] + c0;
-  if (tid < cw) {
+  if (kInv) {
+    for (int idx = tid; idx < n * cw; idx += blockDim.x) {
+      const int r = idx / cw, c = idx % cw;
+      B[(size_t)r * ldb + c] = mkc(r == c0 + c ? 1.0 : 0.0, 0.0);
+    }
+  } else if (tid < cw) {
     for (int j = 0; j < n; ++j) {
       const int p = ipiv[j];
       if (p != j) {
@@ -424,13 +435,16 @@ __global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const*
     }
   }
   __syncthreads();
-  // forward substitution with the unit lower factor
-  for (int rb = 0; rb < n; rb += 64) {
+  // forward substitution with the unit lower factor (rows below k0 of the
+  // slab are zero for the inverse)
+  const int k0 = kInv ? c0 : 0;
+  for (int rb = k0; rb < n; rb += 64) {
     const int rw = min(64, n - rb);
-    if (rb > 0) {
+    if (rb > k0) {
       cplx acc[4][4];
       tile_zero(acc);
-      tile_mma<false, false>(sm, acc, LU + (size_t)rb * lda, lda, B, ldb, nullptr, rw, cw, rb, 0, 0);
+      tile_mma<false, false>(sm, acc, LU + (size_t)rb * lda + k0, lda, B + (size_t)k0 * ldb, ldb, nullptr, rw, cw,
+                             rb - k0, 0, 0);
       tile_store(acc, B + (size_t)rb * ldb, ldb, B + (size_t)rb * ldb, ldb, mkc(-1.0, 0.0), mkc(1.0, 0.0),
                  mkc(0.0, 0.0), rw, cw, 0, 0);
       __syncthreads();
@@ -510,6 +524,33 @@ __global__ void __launch_bounds__(kTileThreads) zgetrs_kernel(const cplx* const*
       }
       __syncthreads();
     }
+  }
+}
+
+// X <- X P for the column interchanges of getrf (ipiv, applied from the
+// last to the first as LAPACK getri does): rows of X pass through shared
+// memory, `rows` per CTA; the permutation is rebuilt per CTA from ipiv.
+__global__ void zcolperm_kernel(cplx* const* Xarr, int n, int ldx, const int* ipiv_all, int rows) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  int* perm = reinterpret_cast<int*>(dsm);
+  cplx* buf = reinterpret_cast<cplx*>(dsm + (((size_t)n * sizeof(int) + 15) & ~(size_t)15));
+  const int b = blockIdx.y, r0 = blockIdx.x * rows;
+  const int* ipiv = ipiv_all + (size_t)b * n;
+  cplx* X = Xarr[b];
+  const int rw = min(rows, n - r0);
+  for (int c = threadIdx.x; c < n; c += blockDim.x) perm[c] = c;
+  for (int idx = threadIdx.x; idx < rw * n; idx += blockDim.x)
+    buf[idx] = X[(size_t)(r0 + idx / n) * ldx + idx % n];
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int j = n - 1; j >= 0; --j) {
+      const int p = ipiv[j];
+      if (p != j) { const int t = perm[j]; perm[j] = perm[p]; perm[p] = t; }
+    }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < rw * n; idx += blockDim.x) {
+    const int r = idx / n, c = idx % n;
+    X[(size_t)(r0 + r) * ldx + c] = buf[(size_t)r * n + perm[c]];
   }
 }
 
@@ -676,7 +717,27 @@ cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipi
                            int nrhs, int ldb, int batch, cudaStream_t st) {
   if (batch <= 0 || n <= 0 || nrhs <= 0) return cudaSuccess;
   dim3 grid((nrhs + 63) / 64, batch);
-  zgetrs_kernel<<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, B, nrhs, ldb);
+  zgetrs_kernel<false><<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, B, nrhs, ldb);
+  ++launch_counter();
+  return cudaGetLastError();
+}
+
+cudaError_t zgetri_batched(const cplx* const* LU, int n, int lda, const int* ipiv, cplx* const* X, int ldx,
+                           int batch, cudaStream_t st) {
+  if (batch <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid((n + 63) / 64, batch);
+  zgetrs_kernel<true><<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, X, n, ldx);
+  ++launch_counter();
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // rows per CTA: as many as fit in 64 KB next to the permutation
+  const size_t perm_bytes = ((size_t)n * sizeof(int) + 15) & ~(size_t)15;
+  const int rows = (int)std::max<size_t>(1, std::min<size_t>(8, (64u << 10) / ((size_t)n * sizeof(cplx))));
+  const size_t smem = perm_bytes + (size_t)rows * n * sizeof(cplx);
+  if (smem > (size_t)(227u << 10)) return cudaErrorInvalidValue;
+  static SmemAttrOnce attr;
+  if ((e = attr.ensure(zcolperm_kernel, (int)(227u << 10))) != cudaSuccess) return e;
+  zcolperm_kernel<<<dim3((n + rows - 1) / rows, batch), 256, smem, st>>>(X, n, ldx, ipiv, rows);
   ++launch_counter();
   return cudaGetLastError();
 }

@@ -46,6 +46,13 @@ cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info,
 cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipiv,
                            cplx* const* B, int nrhs, int ldb, int batch, cudaStream_t st);
 
+// X = A^-1 (n x n, into X, not in place) from the factors of zgetrf_batched:
+// the LAPACK getri order (L^-1 and U^-1 on the identity without the row
+// interchanges, then the column interchanges), a third fewer flops than
+// zgetrs_batched on the identity.
+cudaError_t zgetri_batched(const cplx* const* LU, int n, int lda, const int* ipiv, cplx* const* X, int ldx,
+                           int batch, cudaStream_t st);
+
 // B = I (n x n) for every batch item.
 cudaError_t zset_identity_batched(cplx* const* B, int n, int ldb, int batch, cudaStream_t st);
 

@@ -106,6 +106,15 @@ __global__ void assemble_pq_kernel(const MagItem* items, int N, int with_p) {
   }
 }
 
+// C (n x 2, row-major) = [e_r0, e_r1] for every item.
+__global__ void unit_columns_kernel(cplx* const* C, int n, int r0, int r1) {
+  cplx* c = C[blockIdx.y];
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < (size_t)2 * n; e += (size_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e / 2), k = (int)(e % 2);
+    c[e] = mkc(r == (k == 0 ? r0 : r1) ? 1.0 : 0.0, 0.0);
+  }
+}
+
 // Modes of a magnetic layer: V = (Q W) diag(1/keff) (rcwa/WaveEquationSolver.cpp:36).
 __global__ void finish_modes_scaled_kernel(const LayerItem* items, int N, int* status) {
   const LayerItem it = items[blockIdx.y];
@@ -236,7 +245,10 @@ __global__ void cascade_init_kernel(cplx* const* Rud, cplx* const* Tdd, int n) {
 // generateHorizontalPlaneWave + scatterPlaneWave + sums
 // (rcwa/RCWASolver.cpp:1778-1908, sol/rcwa_bridge.cpp:311-312).  With the
 // analytic half-space modes W_ref = W_trn = I, c = [px delta; py delta], so
-// cref = px Rud(:,inc) + py Rud(:,N+inc) and the harmonics are cref itself.
+// cref = px Rud(:,inc) + py Rud(:,N+inc) and the harmonics are cref itself;
+// with a patterned half-space c = W_ref^-1 [px delta; py delta] and the
+// harmonics W_ref Rud c, W_trn Tdd c come from the precomputed responses
+// Rc, Tc.
 __global__ void scatter_kernel(const ScatterItem* items, int N, int nx, int ny, int* status) {
   const ScatterItem it = items[blockIdx.x];
   const int inc = ny * ((nx - 1) / 2) + (ny - 1) / 2;
@@ -253,12 +265,22 @@ __global__ void scatter_kernel(const ScatterItem* items, int N, int nx, int ny, 
   const double kzinc = fabs(kzinc_c.x);
   double sr = 0.0, st = 0.0;
   for (int h = threadIdx.x; h < N; h += blockDim.x) {
-    const cplx* Rr = it.Rud;
-    const cplx* Tt = it.Tdd;
-    const cplx rx = cfma(it.px, Rr[(size_t)h * n + inc], cmul(it.py, Rr[(size_t)h * n + N + inc]));
-    const cplx ry = cfma(it.px, Rr[(size_t)(N + h) * n + inc], cmul(it.py, Rr[(size_t)(N + h) * n + N + inc]));
-    const cplx tx = cfma(it.px, Tt[(size_t)h * n + inc], cmul(it.py, Tt[(size_t)h * n + N + inc]));
-    const cplx ty = cfma(it.px, Tt[(size_t)(N + h) * n + inc], cmul(it.py, Tt[(size_t)(N + h) * n + N + inc]));
+    cplx rx, ry, tx, ty;
+    if (it.Rc) {
+      const cplx* Rr = it.Rc;
+      const cplx* Tt = it.Tc;
+      rx = cfma(it.px, Rr[(size_t)h * 2], cmul(it.py, Rr[(size_t)h * 2 + 1]));
+      ry = cfma(it.px, Rr[(size_t)(N + h) * 2], cmul(it.py, Rr[(size_t)(N + h) * 2 + 1]));
+      tx = cfma(it.px, Tt[(size_t)h * 2], cmul(it.py, Tt[(size_t)h * 2 + 1]));
+      ty = cfma(it.px, Tt[(size_t)(N + h) * 2], cmul(it.py, Tt[(size_t)(N + h) * 2 + 1]));
+    } else {
+      const cplx* Rr = it.Rud;
+      const cplx* Tt = it.Tdd;
+      rx = cfma(it.px, Rr[(size_t)h * n + inc], cmul(it.py, Rr[(size_t)h * n + N + inc]));
+      ry = cfma(it.px, Rr[(size_t)(N + h) * n + inc], cmul(it.py, Rr[(size_t)(N + h) * n + N + inc]));
+      tx = cfma(it.px, Tt[(size_t)h * n + inc], cmul(it.py, Tt[(size_t)h * n + N + inc]));
+      ty = cfma(it.px, Tt[(size_t)(N + h) * n + inc], cmul(it.py, Tt[(size_t)(N + h) * n + N + inc]));
+    }
     const cplx a = it.ab[h], b = it.ab[N + h];
     const cplx kt = cadd(cmul(a, a), cmul(b, b));
     const cplx kzr = cneg(csqrt_principal(csub(kr2, kt)));
@@ -321,6 +343,13 @@ cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st
 cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st) {
   if (count <= 0) return cudaSuccess;
   finish_modes_kernel<<<ew_grid((size_t)4 * N * N, count), 256, 0, st>>>(items, N, status);
+  ++launch_counter();
+  return cudaGetLastError();
+}
+
+cudaError_t unit_columns(cplx* const* C, int n, int r0, int r1, int count, cudaStream_t st) {
+  if (count <= 0) return cudaSuccess;
+  unit_columns_kernel<<<ew_grid((size_t)2 * n, count), 256, 0, st>>>(C, n, r0, r1);
   ++launch_counter();
   return cudaGetLastError();
 }

@@ -66,6 +66,12 @@ struct PhaseItem {
 struct ScatterItem {
   const cplx* Rud;
   const cplx* Tdd;
+  // a point with a patterned half-space: the responses to the two unit
+  // plane-wave inputs, n x 2 row-major, W_ref Rud W_ref^-1 [e_inc, e_N+inc]
+  // and W_trn Tdd W_ref^-1 [e_inc, e_N+inc] (nullptr: W_ref = W_trn = I and
+  // the Rud, Tdd columns inc and N+inc are these responses)
+  const cplx* Rc = nullptr;
+  const cplx* Tc = nullptr;
   const cplx* ab;
   cplx n2_ref, n2_trn;  // eps * mu of the half-spaces: k^2 = k0^2 eps mu
   double trn_scale;     // |mu_ref / mu_trn|, the flux ratio of the transmitted orders
@@ -81,6 +87,8 @@ struct ScatterItem {
 cudaError_t assemble_m(const LayerItem* items, int count, int N, cudaStream_t st);
 cudaError_t finish_modes(const LayerItem* items, int count, int N, int* status, cudaStream_t st);
 cudaError_t halfspace_modes(const HalfItem* items, int count, int N, int* status, cudaStream_t st);
+// C (n x 2, row-major) = [e_r0, e_r1] for every item
+cudaError_t unit_columns(cplx* const* C, int n, int r0, int r1, int count, cudaStream_t st);
 // P / k0^2 (with_p) and Q of magnetic layers, n x n each
 cudaError_t assemble_pq(const MagItem* items, int count, int N, bool with_p, cudaStream_t st);
 // V <- V diag(1/keff), gamma = GammaSqrtOp(mu): the modes of a layer whose

@@ -136,7 +136,7 @@ def test_bad_permeability_is_rejected(eng):
         eng.solve_batch([o.Stack(2, 2, g, g, np.array(eps), thick, mu=m)], pts, pxy)
     assert ex.value.code == o.abi.RCWA_ERR_NONFINITE
     m = np.array(mu)
-    m[0, 0, 0] = 2.0
+    m[1, 0, 0] = 0.0
     with pytest.raises(o.RcwaError) as ex:
         eng.solve_batch([o.Stack(2, 2, g, g, np.array(eps), thick, mu=m)], pts, pxy)
-    assert ex.value.code == o.abi.RCWA_ERR_UNSUPPORTED
+    assert ex.value.code == o.abi.RCWA_ERR_INVALID
