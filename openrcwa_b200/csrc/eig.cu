@@ -647,7 +647,10 @@ __device__ int schur(cplx* T, int ldt, cplx* Z, int n, cplx (*Wt)[kWin + 1], dou
 #define RCWA_MS_WINDOW 64
 #endif
 constexpr int kMsW = RCWA_MS_WINDOW;  // window order (a build-time parameter)
-constexpr int kMsShifts = 10;      // bulges per sweep
+#ifndef RCWA_MS_SHIFTS
+#define RCWA_MS_SHIFTS 10
+#endif
+constexpr int kMsShifts = RCWA_MS_SHIFTS;  // bulges per sweep (a build-time parameter)
 constexpr int kMsMin = kSchurCrossover;  // smallest crossover: the chase window needs 64 rows
 constexpr int kMsThreads = 256;    // eight warps
 constexpr int kMsLog = kMsW + 1;         // rotation log per bulge; slot kMsW holds the identity
@@ -757,8 +760,12 @@ __device__ void small_eigs_warp(cplx* B, int ldb, int s, cplx* out) {
 // deflated, the others are moved to the top by adjacent swaps and serve as
 // shifts; the spike of the undeflated part is reflected onto its first entry
 // and that part is returned to Hessenberg form by Householder reflectors.
+// Measured on the cfg2 FP64 step (740 matrices of 882): Schur 2488 / 2286 /
+// 2251 / 2228 / 2260 / 2251 ms with windows of 32 / 20 / 18 / 16 / 14 / 12
+// (a smaller window's cheaper one-warp Schur against its fewer deflations);
+// with 16, 8 and 12 shifts per sweep gave 2271 and 2231 ms against 2228.
 #ifndef RCWA_AED_WINDOW
-#define RCWA_AED_WINDOW 32
+#define RCWA_AED_WINDOW 16
 #endif
 constexpr int kAedW = RCWA_AED_WINDOW;  // window order (one lane per column; a build-time parameter)
 static_assert(kAedW <= 32 && kAedW >= kMsShifts + 2, "the early-deflation window is one warp wide");
