@@ -76,6 +76,8 @@ def parse():
                          "Nx=Ny=25 (2601 orders, 5202 x 5202 layer matrices), POINTS of its 32 wavelengths at "
                          "normal incidence, TE+TM, one plan execution")
     ap.add_argument("--cfg5-nh", type=int, default=25, help="harmonics per axis of --cfg5 (25: the full order)")
+    ap.add_argument("--field", action="store_true",
+                    help="time a field slice inside one solved point of the cfg2 stack (rcwa_plan_field)")
     ap.add_argument("--cfg5-lossless", action="store_true",
                     help="--cfg5 with lossless layers on the FP64 plan (checks |R + T - 1|)")
     ap.add_argument("--eig-only", default=None, metavar="N,BATCH",
@@ -409,6 +411,50 @@ def run_cfg5(args):
     return 0 if status.max() == 0 else 1
 
 
+def run_field(args):
+    """Field slices inside one solved point of the cfg2 stack (rcwa_plan_field:
+    the intermediate mode amplitudes and saveFieldImage's XZ slice of Ex at
+    500 columns), timed end to end per call (the call synchronises), beside
+    the oracle's restatement of the same slice on the host cores."""
+    import openrcwa_b200 as o
+    import oracle.rcwa_oracle as orc
+    from openrcwa_b200 import workloads
+    nh = args.nh
+    stacks, pts, pxy = workloads.pillars_2d(seed=0, nH=nh)
+    eng = o.Engine(0)
+    plan = eng.plan(stacks, pts[:1], pxy[:1])
+    plan.execute()
+    px, py = pxy[0, 0]
+    f = plan.field(0, px, py, 1, 0.0, 0, nres1=500)  # warm-up (module loading, allocations)
+    reps = 5
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        f = plan.field(0, px, py, 1, 0.0, 0, nres1=500)
+    t_gpu = (time.perf_counter() - t0) / reps
+    plan.close()
+    eng.close()
+    st = stacks[0]
+    s = orc.RCWASolver(st.nHx, st.nHy)
+    for l in range(st.eps.shape[0]):
+        s.addLayer(orc.OracleLayer(st.cx, st.cy, st.eps[l]))
+    s.setBlochWavevector(pts[0, 2], pts[0, 3])
+    t0 = time.perf_counter()
+    s.solve(pts[0, 1], list(range(st.eps.shape[0])), list(st.thickness))
+    c = s.generateHorizontalPlaneWave(px, py, 0)
+    t_solve = time.perf_counter() - t0
+    inp = [(i, v) for i, v in enumerate(c) if abs(v) > 1e-14]
+    t0 = time.perf_counter()
+    fo = s.fieldSlice(1, 0.0, 0, inp, list(range(st.eps.shape[0])), list(st.thickness), nRes1=500)
+    t_cpu = time.perf_counter() - t0
+    print(json.dumps({"field": {
+        "workload": "XZ slice of Ex (500 x %d samples) inside one point of the cfg2 stack (Nx=Ny=%d, n = %d, "
+                    "5 interior layers)" % (f.shape[0], nh, 2 * st.N),
+        "gpu_s_per_slice": t_gpu, "cpu_oracle_s_per_slice": t_cpu, "cpu_oracle_solve_s": t_solve,
+        "max_abs_vs_oracle": float(np.max(np.abs(f - fo))), "max_abs_field": float(np.max(np.abs(fo)))}}),
+          flush=True)
+    return 0
+
+
 def run_eig_only(spec):
     """One rcwa_zgeev_batched call on seeded random matrices (the kernels of the
     per-layer eigenproblem alone), for counter captures of those kernels."""
@@ -600,6 +646,8 @@ def main():
         return run_conv_only(args.conv_only)
     if args.cfg5:
         return run_cfg5(args)
+    if args.field:
+        return run_field(args)
     if args.gemm_only:
         return run_gemm_only(args.gemm_only)
     if args.smatrix:

@@ -19,13 +19,15 @@
 //
 // Outside this engine (they report on std::cerr and leave outputs empty):
 // PML (enablePML), layer translations, incident vectors other than
-// generateHorizontalPlaneWave's and the field images (saveFieldImage,
-// saveDeviceImage).
+// generateHorizontalPlaneWave's and the device image (saveDeviceImage).
 #pragma once
 #include <algorithm>
 #include <cmath>
+#include <fstream>
+#include <iomanip>
 #include <iostream>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "Layer.h"
@@ -166,8 +168,55 @@ class RCWASolver {
   const Eigen::MatrixXcs& Tdd() const { fetch(); return tdd_; }
   const Eigen::MatrixXcs& Rud() const { fetch(); return rud_; }
 
-  template <class... A>
-  void saveFieldImage(A&&...) { std::cerr << "[rcwa_b200] saveFieldImage is not provided by this engine\n"; }
+  // saveFieldImage (rcwa/RCWASolver.cpp:707-1012): one field component on a
+  // slice of the solved stack, 500 samples along the first slice axis, the
+  // CSV of writeFieldCSV (8 significant digits, ", " between columns; the
+  // modulus, real or imaginary part).  The input is the plane wave of
+  // generateHorizontalPlaneWave (the zero-order entries of inputCoeffs);
+  // layer translations are not provided.
+  void saveFieldImage(const std::string& filename, SliceType sliceType, scalar sliceCoord,
+                      FieldComponent fieldComponent, SaveOption opt,
+                      const std::vector<std::pair<int, scalex>>& inputCoeffs, const std::vector<int>& layerStack,
+                      const std::vector<scalar>& /*thickness*/, const std::vector<scalar>* translation = nullptr) {
+    const int N = nx_ * ny_;
+    const int k0i = ny_ * ((nx_ - 1) / 2) + (ny_ - 1) / 2;
+    if (!plan_ || translation || layerStack != stack_) {
+      std::cerr << "[rcwa_b200] saveFieldImage: solve() this stack first (no translations)\n";
+      return;
+    }
+    rcwa_cplx px{0.0, 0.0}, py{0.0, 0.0};
+    for (const auto& ic : inputCoeffs) {
+      if (ic.first == k0i) px = rcwa_cplx{ic.second.real(), ic.second.imag()};
+      else if (ic.first == N + k0i) py = rcwa_cplx{ic.second.real(), ic.second.imag()};
+      else if (std::abs(ic.second) != 0.0) {
+        std::cerr << "[rcwa_b200] saveFieldImage: only the zero-order plane wave of generateHorizontalPlaneWave\n";
+        return;
+      }
+    }
+    const int nres1 = 500;
+    int rows = 0;
+    if (rcwa_plan_field_rows(plan_, 0, (int)sliceType, nres1, &rows) != RCWA_OK) return;
+    std::vector<rcwa_cplx> f((size_t)rows * nres1);
+    const int rc = rcwa_plan_field(plan_, 0, px, py, (int)sliceType, sliceCoord, (int)fieldComponent, nres1, f.data());
+    if (rc != RCWA_OK) {
+      std::cerr << "[rcwa_b200] saveFieldImage: " << rcwa_status_string(rc) << "\n";
+      return;
+    }
+    std::ofstream fout(filename);
+    if (!fout) {
+      std::cerr << "Cannot open field output file: " << filename << "\n";
+      return;
+    }
+    fout << std::setprecision(8);
+    for (int i = 0; i < rows; ++i) {
+      for (int j = 0; j < nres1; ++j) {
+        const rcwa_cplx v = f[(size_t)i * nres1 + j];
+        fout << (opt == realpart ? v.re : opt == imagpart ? v.im : std::hypot(v.re, v.im));
+        if (j + 1 < nres1) fout << ", ";
+      }
+      fout << "\n";
+    }
+  }
   template <class... A>
   void saveDeviceImage(A&&...) { std::cerr << "[rcwa_b200] saveDeviceImage is not provided by this engine\n"; }
 

@@ -265,6 +265,24 @@ int rcwa_eig_cluster_size(int n, int batch);
  * panel on a cluster of up to 8 CTAs per matrix, with identical factors.
  * ctas = 0: automatic, 1..8: forced; RCWA_ERR_INVALID outside 0..8. */
 int rcwa_set_lu_cluster(int ctas);
+
+/* Fields inside a solved stack, for one point of an executed single-chunk
+ * plan: the mode amplitudes of every interior layer for the plane wave
+ * (px, py) of generateHorizontalPlaneWave (RCWASolver::evaluateIntermediateField,
+ * rcwa/RCWASolver.cpp:1505-1644), then one field component on a slice as
+ * RCWASolver::saveFieldImage evaluates it before writing its CSV
+ * (rcwa/RCWASolver.cpp:707-1012, no layer translation).  slice: 0 = XY at
+ * depth coord, 1 = XZ at y = coord, 2 = YZ at x = coord, the depth measured
+ * from the top of the first interior layer (the slice covers the interior
+ * layers); component 0..5 = Ex, Ey, Ez, Hx, Hy, Hz; nres1 samples along x
+ * (XY, XZ) or y (YZ), at cell centres from the grid's origin; field:
+ * rows x nres1 complex, rows from rcwa_plan_field_rows (saveFieldImage's
+ * nRes2 = max(1, (int)(nres1 L2 / L1))).  The stack needs an interior layer.
+ * Allocates device scratch for the call (about 7 n^2 complex per interface)
+ * and waits for it to finish. */
+int rcwa_plan_field_rows(const rcwa_plan* plan, int point, int slice, int nres1, int* rows);
+int rcwa_plan_field(rcwa_plan* plan, int point, rcwa_cplx px, rcwa_cplx py, int slice, double coord,
+                    int component, int nres1, rcwa_cplx* field);
 int rcwa_lu_cluster_size(int n, int batch);
 
 /* Batched complex GEMM D = alpha*A*B + beta*C (row-major, host buffers

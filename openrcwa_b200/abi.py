@@ -48,7 +48,7 @@ EXPORTS = [
     "rcwa_tuner_save", "rcwa_tuner_load", "rcwa_engine_set_tuner", "rcwa_tuner_measure",
     "rcwa_set_qr_sweep_limit", "rcwa_plan_smatrix", "rcwa_mlp_nn_distance", "rcwa_engine_solve_tables",
     "rcwa_plan_create_tables", "rcwa_set_eig_cluster", "rcwa_eig_cluster_size",
-    "rcwa_set_lu_cluster", "rcwa_lu_cluster_size",
+    "rcwa_set_lu_cluster", "rcwa_lu_cluster_size", "rcwa_plan_field_rows", "rcwa_plan_field",
 ]
 
 _DP = C.POINTER(C.c_double)
@@ -177,6 +177,9 @@ def load() -> C.CDLL:
     lib.rcwa_set_eig_cluster.argtypes = [C.c_int]
     lib.rcwa_eig_cluster_size.argtypes = [C.c_int, C.c_int]
     lib.rcwa_set_lu_cluster.argtypes = [C.c_int]
+    lib.rcwa_plan_field_rows.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, _IP]
+    lib.rcwa_plan_field.argtypes = [C.c_void_p, C.c_int, rcwa_cplx, rcwa_cplx, C.c_int, C.c_double, C.c_int, C.c_int,
+                                    C.c_void_p]
     lib.rcwa_lu_cluster_size.argtypes = [C.c_int, C.c_int]
     lib.rcwa_plan_smatrix.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
     _lib = lib
@@ -517,6 +520,20 @@ class Plan:
         for c in range(max(count, 0)):
             self.eng.lib.rcwa_plan_schedule(self.h, c, C.cast(v, _IP))
             out.append(dict(zip(keys, list(v))))
+        return out
+
+    def field(self, point, px, py, slice, coord, component, nres1=500):
+        """One field component inside the stack (rcwa_plan_field): slice 0 XY
+        at depth coord, 1 XZ at y = coord, 2 YZ at x = coord; component 0..5 =
+        Ex, Ey, Ez, Hx, Hy, Hz.  Returns a (rows, nres1) complex array."""
+        rows = np.zeros(1, dtype=np.int32)
+        self.eng._check(self.eng.lib.rcwa_plan_field_rows(self.h, int(point), int(slice), int(nres1), _i(rows)),
+                        "plan_field_rows")
+        out = np.zeros((int(rows[0]), int(nres1)), dtype=np.complex128)
+        px, py = complex(px), complex(py)
+        self.eng._check(self.eng.lib.rcwa_plan_field(self.h, int(point), rcwa_cplx(px.real, px.imag),
+                                                     rcwa_cplx(py.real, py.imag), int(slice), float(coord),
+                                                     int(component), int(nres1), _v(out)), "plan_field")
         return out
 
     def rescatter(self, pxy):

@@ -33,6 +33,7 @@
 
 #include "eig.cuh"
 #include "engine_internal.cuh"
+#include "field.cuh"
 #include "fourier.cuh"
 #include "linalg.cuh"
 #include "gemm_tc.cuh"
@@ -148,6 +149,9 @@ struct rcwa_plan {
   bool graph_prof = false;   // the graph holds the stage-timing event records
   long long graph_launches = 0;
   long long executions = 0;
+  // per point: the device data the fields inside the stack need (valid for
+  // single-chunk plans, whose workspace holds every point after execution)
+  std::vector<FieldPoint> field_pts;
   ~rcwa_plan() {
     // kernels of this plan may still run on a caller's stream; its pooled
     // blocks and the borrowed workspace go back to the engine only after them
@@ -1229,6 +1233,35 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           return err;
         });
       }
+      // ---------------- what rcwa_plan_field needs of every point
+      if (P->field_pts.size() != (size_t)n_pts) P->field_pts.resize(n_pts);
+      for (int lp = 0; lp < np; ++lp) {
+        const int p = c.points[lp], s = pts[p].stack;
+        const StackInfo& sk = si[s];
+        FieldPoint& fp = P->field_pts[p];
+        fp.N = N; fp.nx = nx; fp.ny = ny; fp.L = sk.L;
+        fp.W.assign(sk.L, nullptr); fp.V.assign(sk.L, nullptr); fp.gamma.assign(sk.L, nullptr);
+        fp.Einv.assign(sk.L, nullptr);
+        for (int l = 0; l < sk.L; ++l) {
+          fp.W[l] = layerW(lp, l);
+          fp.V[l] = layerV(lp, l);
+          fp.gamma[l] = layerG(lp, l);
+          if (l > 0 && l + 1 < sk.L) fp.Einv[l] = W_(c.Einv) + NN * c.conv_index.at({s, l});
+        }
+        fp.thick = sk.thick;
+        fp.Rud = rud[lp];
+        fp.Tdd = tdd[lp];
+        fp.ab = (const cplx*)(inb + ab_off[p]);
+        fp.pat0 = sk.pat0 != 0;
+        fp.k0 = 2 * kPi / pts[p].lambda;
+        fp.kx0 = pts[p].kx0;
+        fp.ky0 = pts[p].ky0;
+        fp.x0 = sk.cx.front();
+        fp.y0 = sk.cy.front();
+        fp.Lx = sk.Lx;
+        fp.Ly = sk.Ly;
+      }
+
       // ---------------- responses of points with a patterned half-space
       // C = W_ref^-1 [e_inc, e_N+inc] (LU of a copy of W_ref), then
       // Rc = W_ref (Rud C), Tc = W_trn (Tdd C): the harmonics of
@@ -1427,6 +1460,29 @@ extern "C" int rcwa_plan_execute(rcwa_plan* p, void* stream) {
   }
   ++p->executions;
   if (err != cudaSuccess) return fail(p->e, RCWA_ERR_CUDA, std::string("launch failed: ") + cudaGetErrorString(err));
+  return RCWA_OK;
+}
+
+extern "C" int rcwa_plan_field_rows(const rcwa_plan* p, int point, int slice, int nres1, int* rows) {
+  if (!p || !rows || point < 0 || point >= p->n_pts || slice < 0 || slice > 2 || nres1 < 1) return RCWA_ERR_INVALID;
+  if (p->field_pts.size() != (size_t)p->n_pts) return RCWA_ERR_INVALID;
+  *rows = field_rows(p->field_pts[point], slice, nres1);
+  return RCWA_OK;
+}
+
+extern "C" int rcwa_plan_field(rcwa_plan* p, int point, rcwa_cplx px, rcwa_cplx py, int slice, double coord,
+                               int component, int nres1, rcwa_cplx* field) {
+  if (!p || !field || point < 0 || point >= p->n_pts) return RCWA_ERR_INVALID;
+  if (p->chunks != 1) return fail(p->e, RCWA_ERR_UNSUPPORTED, "fields need a single-chunk plan");
+  if (p->executions == 0) return fail(p->e, RCWA_ERR_INVALID, "execute the plan before asking for its fields");
+  if (p->field_pts.size() != (size_t)p->n_pts || p->field_pts[point].L < 3)
+    return fail(p->e, RCWA_ERR_INVALID, "fields need at least one interior layer");
+  if (cudaSetDevice(p->e->device) != cudaSuccess) return RCWA_ERR_CUDA;
+  // the plan's last execution may still run on another stream
+  if (cudaDeviceSynchronize() != cudaSuccess) return RCWA_ERR_CUDA;
+  const int rc = field_slice(p->field_pts[point], mkc(px.re, px.im), mkc(py.re, py.im), slice, coord, component,
+                             nres1, reinterpret_cast<cplx*>(field), p->e->stream);
+  if (rc != RCWA_OK) return fail(p->e, rc, "field evaluation failed");
   return RCWA_OK;
 }
 

@@ -252,9 +252,11 @@ def has_magnetic(p: Problem) -> bool:
     return any(abs(m - 1.0) > 1e-12 for m in p.mu) or any(s != 0.0 for s in p.msigma)
 
 
-def run(text: str):
-    """runRCWA (rcwa/RCWADriver.cpp:196-378) without field output: per
-    wavelength (micrometres) R, T, A and the per-order REF/TRN vectors."""
+def run(text: str, field=None):
+    """runRCWA (rcwa/RCWADriver.cpp:196-378): per wavelength (micrometres) R,
+    T, A and the per-order REF/TRN vectors.  field = (component, slice,
+    coord, opt) adds, for the first wavelength, the values saveFieldImage
+    writes (:336-356; opt 0 modulus, 1 real, 2 imaginary part) as "field"."""
     p = parse(text)
     magnetic = has_magnetic(p)
     ze = z_edges(p)
@@ -290,6 +292,12 @@ def run(text: str):
         sol.solve(lam, stack, thick)
         c = sol.generateHorizontalPlaneWave(px, py, 0)
         ref, trn = sol.scatterPlaneWave(c, 0, len(centers) - 1, k0)
+        fval = None
+        if field is not None and not out:
+            comp, sl, coord, opt = field
+            inp = [(i, v) for i, v in enumerate(c) if abs(v) > 1e-14]
+            f = sol.fieldSlice(sl, coord, comp, inp, stack, thick)
+            fval = np.abs(f) if opt == 0 else (f.real if opt == 1 else f.imag)
         out.append({"lambda": lam, "R": ref.sum(), "T": trn.sum(), "A": 1 - ref.sum() - trn.sum(), "REF": ref,
-                    "TRN": trn})
+                    "TRN": trn, "field": fval})
     return out

@@ -403,6 +403,7 @@ class RCWASolver:
         nL = len(stack)
         Tdd = np.eye(n, dtype=np.complex128)
         Rud = np.zeros((n, n), dtype=np.complex128)
+        self.taus = []  # taus_ (rcwa/RCWASolver.cpp:454), kept for the intermediate fields
         for i in range(nL - 1):
             index = nL - i - 1
             li = stack[index]
@@ -416,9 +417,140 @@ class RCWASolver:
             F = self.iE[k] + self.iE[k] @ wRud        # :440-441
             G = self.iH[k] - self.iH[k] @ wRud        # :442-443
             tau = np.linalg.inv(F + G)                # PartialPivLU inverse :451-453
+            self.taus.append(tau)
             Rud = -2.0 * G @ tau + np.eye(n)          # :457-458
             Tdd = 2.0 * wTdd @ tau                    # :460
         self.Rud, self.Tdd = Rud, Tdd
+
+    def evaluateIntermediateField(self, inputCoeffs, stack, thickness):
+        """evaluateIntermediateField, input given as (index, value) pairs
+        (rcwa/RCWASolver.cpp:1505-1644): the mode amplitudes c_m (backward)
+        and c_p (forward) of every interior layer, top to bottom
+        (c_m[k], c_p[k] belong to stack[k + 1]).  Eigen's PartialPivLU and
+        CompleteOrthogonalDecomposition solves are LU solves here."""
+        n = 2 * self.nx * self.ny
+        nL = len(stack)
+        if nL < 3:
+            return [], []
+        I = np.eye(n, dtype=np.complex128)
+        S11, S12, S21, S22, phases = [], [], [], [], []
+        Rud = np.zeros((n, n), dtype=np.complex128)
+        REF = [Rud]
+        for i in range(nL - 1):
+            index = nL - i - 1
+            li = stack[index]
+            phase = np.ones(n, dtype=np.complex128) if i == 0 else np.exp(1j * self.sol[li].gamma * thickness[index])
+            phases.append(phase)
+            k = self.imap[index - 1]
+            IE, IH = self.iE[k], self.iH[k]
+            t11 = 0.5 * (IE + IH)
+            t12 = 0.5 * (IE - IH)
+            inv_t22 = np.linalg.inv(t11)
+            inv_t22_t12 = np.linalg.solve(t11, t12)
+            S11.append(t11 - t12 @ inv_t22_t12)
+            S12.append(t12 @ inv_t22)
+            S21.append(-inv_t22_t12)
+            S22.append(inv_t22)
+            if i == 0:
+                for_inv_s22 = t11
+            wRud = phase[:, None] * Rud * phase[None, :]
+            G = IH - IH @ wRud
+            Rud = -2.0 * G @ self.taus[i] + I
+            REF.append(Rud)
+        inp = np.zeros(n, dtype=np.complex128)
+        for idx, v in inputCoeffs:
+            inp[idx] = v
+        R = self.Rud @ inp
+        T = self.Tdd @ inp
+        nI = nL - 2
+        c_m, c_p, d = [None] * nI, [None] * nI, [None] * nI
+        c_m[nI - 1] = S12[0] @ (for_inv_s22 @ T)
+        temp = np.linalg.solve(S11[nL - 2], R - S12[nL - 2] @ inp)
+        c_p[0] = S21[nL - 2] @ temp + S22[nL - 2] @ inp
+        d[nI - 1] = phases[nL - 2] * c_p[0]
+        for i in range(nI - 2, -1, -1):
+            c_m[nI - i - 2] = REF[i + 2] @ d[i + 1]
+            tempi = np.linalg.solve(S11[i + 1], c_m[nI - i - 2] - S12[i + 1] @ d[i + 1])
+            c_p[nI - i - 1] = S21[i + 1] @ tempi + S22[i + 1] @ d[i + 1]
+            d[i] = phases[i + 1] * c_p[nI - i - 1]
+        return c_m, c_p
+
+    def fieldSlice(self, sliceType, sliceCoord, component, inputCoeffs, stack, thickness, nRes1=500):
+        """The field that saveFieldImage writes, before the CSV formatting
+        (rcwa/RCWASolver.cpp:707-1012, no layer translation): sliceType 0 = XY
+        at depth sliceCoord, 1 = XZ at y = sliceCoord, 2 = YZ at x =
+        sliceCoord (z from the top of the first interior layer); component
+        0..5 = Ex, Ey, Ez, Hx, Hy, Hz.  Returns the (nRes2 x nRes1) complex
+        field."""
+        c_m, c_p = self.evaluateIntermediateField(inputCoeffs, stack, thickness)
+        if not c_m:
+            return None
+        L0 = self.layers[0]
+        nx, ny = self.nx, self.ny
+        Lx = L0.cx[-1] - L0.cx[0]
+        Ly = L0.cy[-1] - L0.cy[0]
+        if sliceType == 1:
+            s1, L1, s2, L2 = L0.cx[0], Lx, 0.0, float(sum(thickness[1:len(stack) - 1]))
+        elif sliceType == 2:
+            s1, L1, s2, L2 = L0.cy[0], Ly, 0.0, float(sum(thickness[1:len(stack) - 1]))
+        else:
+            s1, L1, s2, L2 = L0.cx[0], Lx, L0.cy[0], Ly
+        nRes2 = max(int(nRes1 * L2 / L1), 1)
+        x1 = s1 + (L1 / nRes1) * (np.arange(nRes1) + 0.5)
+        x2 = s2 + (L2 / nRes2) * (np.arange(nRes2) + 0.5)
+        N = nx * ny
+        k0 = 2 * PI / self.lam
+        a = self.alpha.astype(np.complex128)
+        b = self.beta.astype(np.complex128)
+
+        def harmonics(z):
+            z0, layer0 = 0.0, -1
+            for j in range(1, len(stack) - 1):
+                z1 = z0 + thickness[j]
+                if z0 <= z <= z1:
+                    layer0 = j - 1
+                    break
+                z0 = z1
+            lt = stack[layer0 + 1]
+            g = self.sol[lt].gamma
+            u_p = c_p[layer0] * np.exp(1j * (z - z0) * g)
+            d_m = c_m[layer0] * np.exp(-1j * (z - z1) * g)
+            W, V = self.sol[lt].W, self.sol[lt].V
+            if component in (0, 1):
+                h = (W @ (u_p + d_m))[N * component:N * (component + 1)]
+            elif component in (3, 4):
+                h = (V @ (u_p - d_m))[N * (component - 3):N * (component - 2)]
+            elif component == 5:
+                E = W @ (u_p + d_m)
+                h = 1j / (k0 * k0) * (a * E[N:] - b * E[:N])
+            else:
+                H = V @ (u_p - d_m)
+                Ly_ = self.layers[lt]
+                fe33 = fourier2d(Ly_.cx, Ly_.cy, Ly_.eps, nx, ny, ContinuousXY) if Ly_.f2d is None else \
+                    block_toeplitz_dense(np.asarray(Ly_.f2d, dtype=np.complex128))
+                h = 1j * np.linalg.solve(fe33, a * H[N:] - b * H[:N])
+            return h.reshape(nx, ny)  # harmonics2d(i, j) = h[j + i * ny]
+
+        mx, my = (nx - 1) // 2, (ny - 1) // 2
+        m = np.arange(-mx, mx + 1)
+        q = np.arange(-my, my + 1)
+        field = np.zeros((nRes2, nRes1), dtype=np.complex128)
+        if sliceType in (1, 2):
+            for i, z in enumerate(x2):
+                H2 = harmonics(z)
+                if sliceType == 1:
+                    one = H2 @ np.exp(1j * (2 * PI * q / Ly + self.ky0) * sliceCoord)
+                    wav = np.exp(1j * np.outer(x1, 2 * PI * m / Lx + self.kx0))
+                else:
+                    one = H2.T @ np.exp(1j * (2 * PI * m / Lx + self.kx0) * sliceCoord)
+                    wav = np.exp(1j * np.outer(x1, 2 * PI * q / Ly + self.ky0))
+                field[i] = wav @ one
+        else:
+            H2 = harmonics(sliceCoord)
+            wx = np.exp(1j * np.outer(x1, 2 * PI * m / L1 + self.kx0))   # (nRes1, nx)
+            wy = np.exp(1j * np.outer(x2, 2 * PI * q / L2 + self.ky0))   # (nRes2, ny)
+            field = wy @ H2.T @ wx.T
+        return field
 
     def generateHorizontalPlaneWave(self, px, py, layerType):
         """generateHorizontalPlaneWave + Layer::generatePlaneWave
