@@ -18,8 +18,8 @@
 // first access after solve().
 //
 // Outside this engine (they report on std::cerr and leave outputs empty):
-// PML (enablePML), layer translations, incident vectors other than
-// generateHorizontalPlaneWave's and the device image (saveDeviceImage).
+// PML (enablePML), layer translations in solve and saveFieldImage, and
+// incident vectors other than generateHorizontalPlaneWave's.
 #pragma once
 #include <algorithm>
 #include <cmath>
@@ -217,8 +217,74 @@ class RCWASolver {
       fout << "\n";
     }
   }
-  template <class... A>
-  void saveDeviceImage(A&&...) { std::cerr << "[rcwa_b200] saveDeviceImage is not provided by this engine\n"; }
+  // saveDeviceImage (rcwa/RCWASolver.cpp:1322-1487): the real part of the
+  // permittivity of the interior layers on a slice, 2000 samples along the
+  // first slice axis, in writeFieldCSV's format; host code on the layers'
+  // cell grids (a depth z belongs to the layer with z0 <= z < z1).
+  void saveDeviceImage(const std::string& filename, SliceType sliceType, scalar sliceCoord,
+                       const std::vector<int>& layerStack, const std::vector<scalar>& thickness,
+                       const std::vector<scalar>* translation = nullptr) {
+    if (layers_.empty() || layerStack.size() < 3 || thickness.size() != layerStack.size()) {
+      std::cerr << "Device image requires at least one finite-thickness interior layer!\n";
+      return;
+    }
+    const Layer& L0 = layers_.front();
+    scalar s1 = L0.l0(), L1 = L0.Lx(), s2 = 0.0, L2 = 0.0;
+    if (sliceType == sliceYZ) { s1 = L0.b0(); L1 = L0.Ly(); }
+    if (sliceType == sliceXY) { s2 = L0.b0(); L2 = L0.Ly(); }
+    else
+      for (size_t i = 1; i + 1 < layerStack.size(); ++i) L2 += thickness[i];
+    const int n1 = 2000;
+    int n2 = (int)(n1 * L2 / L1);
+    if (n2 < 1) n2 = 1;
+    const scalar st1 = L1 / n1, st2 = L2 / n2;
+    auto layer_at = [&](scalar z) -> int {
+      scalar z0 = 0.0;
+      for (size_t j = 1; j + 1 < layerStack.size(); ++j) {
+        const scalar z1 = z0 + thickness[j];
+        if (z0 <= z && z < z1) return (int)j;
+        z0 = z1;
+      }
+      return -1;
+    };
+    std::vector<double> dev((size_t)n1 * n2);
+    int lfix = sliceType == sliceXY ? layer_at(sliceCoord) : -1;
+    if (sliceType == sliceXY && lfix < 0) {
+      std::cerr << "Device image requires at least one finite-thickness interior layer!\n";
+      return;
+    }
+    for (int i = 0; i < n2; ++i) {
+      const scalar c2 = s2 + st2 * (i + 0.5);
+      const int l = sliceType == sliceXY ? lfix : layer_at(c2);
+      if (l < 0) {
+        std::cerr << "Device image requires at least one finite-thickness interior layer!\n";
+        return;
+      }
+      const Layer& Ly = layers_[(size_t)layerStack[(size_t)l]];
+      const scalar tx = translation ? (*translation)[(size_t)l] : 0.0;
+      for (int j = 0; j < n1; ++j) {
+        const scalar c1 = s1 + st1 * (j + 0.5);
+        scalex v;
+        if (sliceType == sliceXZ) v = Ly.eps(c1 - tx, sliceCoord);
+        else if (sliceType == sliceYZ) v = Ly.eps(sliceCoord - tx, c1);
+        else v = Ly.eps(c1 - tx, c2);
+        dev[(size_t)i * n1 + j] = v.real();
+      }
+    }
+    std::ofstream fout(filename);
+    if (!fout) {
+      std::cerr << "Cannot open field output file: " << filename << "\n";
+      return;
+    }
+    fout << std::setprecision(8);
+    for (int i = 0; i < n2; ++i) {
+      for (int j = 0; j < n1; ++j) {
+        fout << dev[(size_t)i * n1 + j];
+        if (j + 1 < n1) fout << ", ";
+      }
+      fout << "\n";
+    }
+  }
 
  private:
   std::vector<double> merged(bool xaxis, const std::vector<int>& stack) const {

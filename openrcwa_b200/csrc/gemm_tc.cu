@@ -386,7 +386,10 @@ __global__ void __launch_bounds__(kTcThreads, N == 128 ? 2 : 1) zgemm_tf32x3_ker
 // slab into shared memory with plain bulk copies (cp.async.bulk, the TMA
 // engine, from this GPU's memory; no tensor map, no multicast) and its
 // threads do no conversion at all.
-constexpr int kV2Stages = 3;
+#ifndef RCWA_TC_STAGES
+#define RCWA_TC_STAGES 3
+#endif
+constexpr int kV2Stages = RCWA_TC_STAGES;  // a build-time parameter
 constexpr size_t kV2StageBytes = 8 * 4096;  // 4 A planes + 4 B planes
 constexpr size_t kV2Smem = kV2Stages * kV2StageBytes + 64;
 
@@ -487,13 +490,16 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_split_kernel(GemmA
   int epending[kV2Stages] = {};  // a commit on empty[s] not yet waited for (thread 0)
   int fpending[kV2Stages] = {};  // bulk copies into stage s not yet waited for (thread 0)
   const int slabs_per_block = kTcKBlock / kTcK;
+  int issued = 0;  // slabs whose copies thread 0 has issued (they run across K-blocks)
   for (int kb0 = 0; kb0 < KS; kb0 += slabs_per_block) {
     const int kb1 = min(KS, kb0 + slabs_per_block);
     if (tid == 0 && !*s_fail) {
       bool fail = false;
-      // pipeline over the block's slabs: copies run kV2Stages - 1 slabs ahead
-      for (int i = kb0; i < kb1 + kV2Stages - 1 && !fail; ++i) {
-        if (i < kb1) {
+      // pipeline over the block's slabs: copies run kV2Stages - 1 slabs ahead,
+      // into the next K-block too, so its first slabs arrive during the drain
+      for (int j = kb0; j < kb1 && !fail; ++j) {
+        while (issued < KS && issued <= j + kV2Stages - 1) {
+          const int i = issued;
           const int stg = i % kV2Stages;
           if (epending[stg]) {
             if (!mbar_wait(smem_u32(empty + stg), ephase[stg])) { fail = true; break; }
@@ -508,9 +514,10 @@ __global__ void __launch_bounds__(kTcThreads, 2) zgemm_tf32x3_split_kernel(GemmA
             bulk_g2s(dst + (4 + p) * 4096, PB + (size_t)p * nblkB * 1024 + (size_t)i * 1024, 4096, fb);
           }
           fpending[stg] = 1;
+          ++issued;
         }
-        const int j = i - (kV2Stages - 1);
-        if (j >= kb0 && j < kb1) {
+        if (fail) break;
+        {
           const int stg = j % kV2Stages;
           if (!mbar_wait(smem_u32(full + stg), fphase[stg])) { fail = true; break; }
           fphase[stg] ^= 1u;

@@ -252,7 +252,47 @@ def has_magnetic(p: Problem) -> bool:
     return any(abs(m - 1.0) > 1e-12 for m in p.mu) or any(s != 0.0 for s in p.msigma)
 
 
-def run(text: str, field=None):
+def device_image(sol, slice_, coord, stack, thickness, n1=2000):
+    """saveDeviceImage (rcwa/RCWASolver.cpp:1322-1487) without translations:
+    the real part of the interior layers' permittivity on the slice, a depth
+    z belonging to the layer with z0 <= z < z1."""
+    L0 = sol.layers[0]
+    Lx, Ly = L0.cx[-1] - L0.cx[0], L0.cy[-1] - L0.cy[0]
+    if slice_ == 1:
+        s1, L1, s2, L2 = L0.cx[0], Lx, 0.0, float(sum(thickness[1:len(stack) - 1]))
+    elif slice_ == 2:
+        s1, L1, s2, L2 = L0.cy[0], Ly, 0.0, float(sum(thickness[1:len(stack) - 1]))
+    else:
+        s1, L1, s2, L2 = L0.cx[0], Lx, L0.cy[0], Ly
+    n2 = max(int(n1 * L2 / L1), 1)
+
+    def layer_at(z):
+        z0 = 0.0
+        for j in range(1, len(stack) - 1):
+            z1 = z0 + thickness[j]
+            if z0 <= z < z1:
+                return j
+            z0 = z1
+        raise ValueError("depth outside the interior layers")
+
+    def cells(edges, v):
+        # the first cell whose upper edge is >= v (Layer::eps, rcwa/Layer.cpp:383-429)
+        return np.searchsorted(np.asarray(edges)[1:], v, side="left")
+
+    out = np.zeros((n2, n1))
+    c1 = s1 + (L1 / n1) * (np.arange(n1) + 0.5)
+    for i in range(n2):
+        c2 = s2 + (L2 / n2) * (i + 0.5)
+        lay = sol.layers[stack[layer_at(coord if slice_ == 0 else c2)]]
+        x, y = (c1, np.full(n1, coord)) if slice_ == 1 else \
+            ((np.full(n1, coord), c1) if slice_ == 2 else (c1, np.full(n1, c2)))
+        per = lay.cx[-1] - lay.cx[0]
+        x = np.where(x < lay.cx[0], x + per, np.where(x > lay.cx[-1], x - per, x))
+        out[i] = np.asarray(lay.eps)[cells(lay.cy, y), cells(lay.cx, x)].real
+    return out
+
+
+def run(text: str, field=None, device=None):
     """runRCWA (rcwa/RCWADriver.cpp:196-378): per wavelength (micrometres) R,
     T, A and the per-order REF/TRN vectors.  field = (component, slice,
     coord, opt) adds, for the first wavelength, the values saveFieldImage
@@ -292,12 +332,14 @@ def run(text: str, field=None):
         sol.solve(lam, stack, thick)
         c = sol.generateHorizontalPlaneWave(px, py, 0)
         ref, trn = sol.scatterPlaneWave(c, 0, len(centers) - 1, k0)
-        fval = None
+        fval = dval = None
+        if device is not None and not out:
+            dval = device_image(sol, device[0], device[1], stack, thick)
         if field is not None and not out:
             comp, sl, coord, opt = field
             inp = [(i, v) for i, v in enumerate(c) if abs(v) > 1e-14]
             f = sol.fieldSlice(sl, coord, comp, inp, stack, thick)
             fval = np.abs(f) if opt == 0 else (f.real if opt == 1 else f.imag)
         out.append({"lambda": lam, "R": ref.sum(), "T": trn.sum(), "A": 1 - ref.sum() - trn.sum(), "REF": ref,
-                    "TRN": trn, "field": fval})
+                    "TRN": trn, "field": fval, "device": dval})
     return out

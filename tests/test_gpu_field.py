@@ -138,3 +138,20 @@ def test_driver_field_csv(tmp_path, component, slice_, coord, opt):
     assert got.shape == want.shape
     # 8 significant digits in the CSV
     assert np.max(np.abs(got - want)) <= 2e-8 * max(1.0, 5 * np.max(np.abs(want)))
+
+
+@pytest.mark.skipif(not os.path.exists(DRIVER), reason="oracle/_ref not built (oracle/build_ref.sh)")
+@pytest.mark.parametrize("slice_,coord", [("xz", "0.05"), ("xy", "0.07")])
+def test_driver_device_csv(tmp_path, slice_, coord):
+    # saveDeviceImage through the adapter: the permittivity of the interior
+    # layers on the slice, against the driver oracle's restatement
+    from oracle import driver_oracle
+    (tmp_path / "in.orcwa").write_text(ORCWA_FIELD)
+    out = subprocess.run([DRIVER, "-o", "out.csv", "-device", "-slice", slice_, "-scoord", coord, "-deviceout",
+                          "d.csv", "in.orcwa"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout + out.stderr
+    got = np.array([[float(v) for v in ln.split(",")] for ln in open(tmp_path / "d.csv") if ln.strip()])
+    sl = {"xy": 0, "xz": 1, "yz": 2}[slice_]
+    want = driver_oracle.run(ORCWA_FIELD, device=(sl, float(coord)))[0]["device"]
+    assert got.shape == want.shape
+    assert np.max(np.abs(got - want)) <= 1e-7 * np.max(np.abs(want))
