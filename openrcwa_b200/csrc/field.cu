@@ -166,7 +166,8 @@ int field_slice(const FieldPoint& fp, cplx px, cplx py, int slice, double coord,
   const size_t vecs = (size_t)2 * nI + nI + 16;
   const size_t bytes = mats * ((sizeof(cplx) * nn + 255) & ~(size_t)255) + vecs * ((sizeof(cplx) * n + 255) & ~(size_t)255) +
                        3 * ((sizeof(cplx) * n * nz + 255) & ~(size_t)255) +
-                       ((sizeof(int) * n * (3 * ns + 3) + 255) & ~(size_t)255) + 256 * 4 + sizeof(void*) * 4096 +
+                       ((sizeof(int) * n * (3 * ns + 3) + 255) & ~(size_t)255) + sizeof(int) * (3 * ns + 264) +
+                       sizeof(void*) * 4096 +
                        ((sizeof(cplx) * (size_t)nres1 * nres2 + 255) & ~(size_t)255) + 4096;
   if (cudaMalloc(&S.base, bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -198,7 +199,7 @@ int field_slice(const FieldPoint& fp, cplx px, cplx py, int slice, double coord,
   cplx* Hm = S.take<cplx>((size_t)n * nz);
   cplx* h = S.take<cplx>((size_t)n * nz);
   int* ipiv = S.take<int>((size_t)n * (3 * ns + 3));
-  int* info = S.take<int>(256);
+  int* info = S.take<int>((size_t)3 * ns + 8);
   cplx* dfield = S.take<cplx>((size_t)nres1 * nres2);
   void** pool = S.take<void*>(4096);
   std::vector<void*> hp;
@@ -208,15 +209,35 @@ int field_slice(const FieldPoint& fp, cplx px, cplx py, int slice, double coord,
     return (cplx* const*)(pool + o);
   };
   // all pointer arrays first (their device addresses are known), one upload
-  std::vector<cplx* const*> pIEH(ns), pLUab(ns), pLIEH(ns), pLT(ns), pFG(ns), pS(ns), pTau(ns);
+  std::vector<cplx* const*> pIEH(ns), pLT(ns);
   cplx* const* pLU0 = nullptr;
   cplx* const* pInp = nullptr;
   for (int i = 0; i < ns; ++i) {
-    pLUab[i] = P({WLU, VLU});
     pIEH[i] = P({IE[i], IH[i]});
-    pLIEH[i] = P({LIE[i], LIH[i]});
     pLT[i] = P({LT[i]});
   }
+  // the interfaces' independent work as batches: copies of Wa, Va (into the
+  // LIE, LIH buffers, free until the amplitude factors), Wb, Vb (into IE,
+  // IH); LU of every Wa, Va; the solves; later the LU of every IE, IH, t11
+  std::vector<const void*> csrc, cdst, luA, rhsA, luC;
+  for (int i = 0; i < ns; ++i) {
+    const int index = L - 1 - i, a = index - 1, b = index;
+    csrc.insert(csrc.end(), {fp.W[a], fp.V[a], fp.W[b], fp.V[b]});
+    cdst.insert(cdst.end(), {LIE[i], LIH[i], IE[i], IH[i]});
+    luA.insert(luA.end(), {LIE[i], LIH[i]});
+    rhsA.insert(rhsA.end(), {IE[i], IH[i]});
+    luC.insert(luC.end(), {LIE[i], LIH[i], LT[i]});
+  }
+  auto Pv = [&](const std::vector<const void*>& v) {
+    const size_t o = hp.size();
+    for (const void* q : v) hp.push_back(const_cast<void*>(q));
+    return (cplx* const*)(pool + o);
+  };
+  cplx* const* pCs = Pv(csrc);
+  cplx* const* pCd = Pv(cdst);
+  cplx* const* pLA = Pv(luA);
+  cplx* const* pRA = Pv(rhsA);
+  cplx* const* pLC = Pv(luC);
   cplx* const* pW = P({WLU});
   cplx* const* pF = P({F});
   cplx* const* pTauD = P({tau});
@@ -269,19 +290,16 @@ int field_slice(const FieldPoint& fp, cplx px, cplx py, int slice, double coord,
   auto copy = [&](const cplx* s, cplx* d) { return cudaMemcpyAsync(d, s, sizeof(cplx) * nn, cudaMemcpyDeviceToDevice, st); };
   const cplx one = mkc(1, 0), zero = mkc(0, 0), half = mkc(0.5, 0);
   cudaError_t e = cudaSuccess;
-  int* ip_ab = ipiv;                          // 2 n: LU of Wa, Va
   int* ip_run = ipiv + (size_t)2 * n;         // n: LU of F + G, W_ref
-  int* ip_st = ipiv + (size_t)3 * n;          // 3 n per step: IE, IH, t11
-  // ---- interfaces, recursion, and the factors the amplitudes need
+  int* ip_st = ipiv + (size_t)3 * n;          // 3 n per step: IE, IH, t11 (first Wa, Va)
+  // ---- interfaces IE = Wa^-1 Wb, IH = Va^-1 Vb of every step at once
+  // (rcwa/RCWASolver.cpp:537-543)
+  e = zcopy_batched((const cplx* const*)pCs, n, pCd, n, n, n, 4 * ns, st);
+  if (ok(e)) e = zgetrf_batched(pLA, n, n, ip_st, info, 2 * ns, st);
+  if (ok(e)) e = zgetrs_batched((const cplx* const*)pLA, n, n, ip_st, pRA, n, n, 2 * ns, st);
+  // ---- the recursion, step by step
   for (int i = 0; i < ns && ok(e); ++i) {
-    const int index = L - 1 - i, a = index - 1, b = index;
-    // IE = Wa^-1 Wb, IH = Va^-1 Vb  (rcwa/RCWASolver.cpp:537-543)
-    if (ok(e)) e = copy(fp.W[a], WLU);
-    if (ok(e)) e = copy(fp.V[a], VLU);
-    if (ok(e)) e = copy(fp.W[b], IE[i]);
-    if (ok(e)) e = copy(fp.V[b], IH[i]);
-    if (ok(e)) e = zgetrf_batched(pLUab[i], n, n, ip_ab, info, 2, st);
-    if (ok(e)) e = zgetrs_batched((const cplx* const*)pLUab[i], n, n, ip_ab, pIEH[i], n, n, 2, st);
+    const int index = L - 1 - i, b = index;
     // waveRud, F = IE + IE waveRud, G = IH - IH waveRud, tau = (F + G)^-1,
     // Rud = I - 2 G tau  (:423-460)
     const cplx* Rprev = i == 0 ? nullptr : REF[i - 1];
@@ -305,7 +323,10 @@ int field_slice(const FieldPoint& fp, cplx px, cplx py, int slice, double coord,
     if (ok(e)) e = zgetrf_batched(pF, n, n, ip_run, info, 1, st);
     if (ok(e)) e = zgetri_batched((const cplx* const*)pF, n, n, ip_run, pTauD, n, 1, st);
     if (ok(e)) e = gemm(G, n, tau, n, REF[i], n, n, n, n, mkc(-2, 0), one);
-    // factors for the amplitudes: LU of IE, IH and t11 = (IE + IH)/2
+  }
+  // ---- factors for the amplitudes, every step at once: LU of IE, IH and
+  // t11 = (IE + IH)/2 (item 3i + k's pivots at ip_st + (3i + k) n)
+  for (int i = 0; i < ns && ok(e); ++i) {
     if (ok(e)) e = copy(IE[i], LIE[i]);
     if (ok(e)) e = copy(IH[i], LIH[i]);
     if (ok(e)) {
@@ -313,9 +334,8 @@ int field_slice(const FieldPoint& fp, cplx px, cplx py, int slice, double coord,
       ++launch_counter();
       e = cudaGetLastError();
     }
-    if (ok(e)) e = zgetrf_batched(pLIEH[i], n, n, ip_st + (size_t)3 * n * i, info, 2, st);
-    if (ok(e)) e = zgetrf_batched(pLT[i], n, n, ip_st + (size_t)3 * n * i + 2 * n, info, 1, st);
   }
+  if (ok(e)) e = zgetrf_batched(pLC, n, n, ip_st, info, 3 * ns, st);
   if (!ok(e)) return RCWA_ERR_CUDA;
   // ---- the input: modal amplitudes of the incidence layer for the plane
   // wave (px, py) (generateHorizontalPlaneWave, rcwa/Layer.cpp:453-480)
