@@ -298,7 +298,9 @@ int rcwa_zgemm_batched(rcwa_engine* e, int M, int N, int K, int batch, const rcw
  * blocking).  A tuner is a table of schedule choices keyed by decision, matrix
  * order n and batch class (waves of one-CTA-per-matrix work: 1, 2, 3, 4 for
  * 4-7, 8 for 8 and more).  Decisions and their choices:
- *   RCWA_TUNE_LU       0: one CTA factors each matrix, 1: panel by panel
+ *   RCWA_TUNE_LU       0: one CTA factors each matrix, 1: panel by panel,
+ *                      2: 128-column blocks (1 inside each block, then one
+ *                      K = 128 trailing update per block; n >= 256)
  *   RCWA_TUNE_SCHUR    active-block size below which the Schur iteration uses
  *                      single-shift sweeps (64, 96, 128, 192; only 64 for
  *                      n < 64 and n >= 512; default 128 for 64 <= n < 128,

@@ -14,9 +14,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "librcwa_b200.so")
-SOURCES = ["linalg.cu", "eig.cu", "fourier.cu", "rcwa_kernels.cu", "engine.cu", "stages.cu", "bridge.cu", "noalloc.cu", "smatrix.cu", "gemm_tc.cu", "mlp.cu", "tuner.cu", "field.cu"]
+SOURCES = ["linalg.cu", "eig.cu", "fourier.cu", "rcwa_kernels.cu", "engine.cu", "stages.cu", "bridge.cu", "noalloc.cu", "smatrix.cu", "gemm_tc.cu", "mlp.cu", "tuner.cu", "field.cu", "lu_blocked.cu"]
 HEADERS = ["common.cuh", "tile.cuh", "linalg.cuh", "eig.cuh", "fourier.cuh", "rcwa_kernels.cuh",
-           "engine_internal.cuh", "gemm_tc.cuh", "tuner.cuh", "field.cuh"]
+           "engine_internal.cuh", "gemm_tc.cuh", "tuner.cuh", "field.cuh", "lu_blocked.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
               "--expt-relaxed-constexpr", "-I", os.path.join(ROOT, "include")]

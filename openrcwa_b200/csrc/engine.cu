@@ -38,6 +38,7 @@
 #include "linalg.cuh"
 #include "gemm_tc.cuh"
 #include "rcwa_kernels.cuh"
+#include "lu_blocked.cuh"
 #include "tuner.cuh"
 
 
@@ -130,7 +131,7 @@ struct rcwa_plan {
   double* dTrn = nullptr;
   int* dStatus = nullptr;
   int* dTcErr = nullptr;   // set when a tensor-core completion wait ran out
-  int* dTcScale = nullptr; // operand scale exponents of the tensor-core products (2 x 1024)
+  int* dTcScale = nullptr; // operand scale exponents of the tensor-core products (2 x 2048)
   // per chunk: n, points, interface LU schedule, tau LU schedule, Schur
   // crossover, product path (0: 3xTF32 on 128 x 128 tiles, 1: FP64 tensor
   // path, 2: 3xTF32 on 128 x 256 tiles)
@@ -628,7 +629,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
     size_t oRef = ol.take(sizeof(double) * std::max<size_t>(acc, 1)), oTrn = ol.take(sizeof(double) * std::max<size_t>(acc, 1));
     size_t oS = ol.take(sizeof(int) * n_pts);
     size_t oE = ol.take(sizeof(int));
-    size_t oSc = ol.take(sizeof(int) * 2 * 1024);
+    size_t oSc = ol.take(sizeof(int) * 2 * 2048);
     if (!P->outputs.take(e, ol.off)) return fail(e, RCWA_ERR_NOMEM, "output allocation failed");
     char* b = (char*)P->outputs.p;
     P->dR = (double*)(b + oR);
@@ -1089,6 +1090,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
         std::vector<const cplx*> fA(k), fB(k), fC(k), gA(k), gB(k), gC(k), sF(k), sG(k), tG(k), tT(k), tTau(k);
         std::vector<cplx*> fD(k), gD(k), sD(k), tauD(k), rD(k), tD(k), Sp(k);
         std::vector<int> ipoint, spoint(k);
+        int kdt = 0;  // dense-route points with 3xTF32 solves
         for (int q = 0; q < k; ++q) {
           const int lp = part[q], p = c.points[lp];
           const int L = si[pts[p].stack].L;
@@ -1111,6 +1113,7 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
             lu.push_back(WLU); luV.push_back(VLU);
             rhs.push_back(IE); rhsV.push_back(IH);
             ipoint.push_back(p);
+            if (tc_plan && !c.fp64_pt[lp]) ++kdt;  // the dense list keeps part's order: 3xTF32 points first
           }
           spoint[q] = p;
           if (step > 0) {
@@ -1132,14 +1135,24 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           tT[q] = tdd[lp]; tD[q] = gbuf[lp];
           std::swap(tdd[lp], gbuf[lp]);
         }
-        // LU batch: the W's of the dense-route points, then their V's
+        // LU batch: the W's and then the V's of the dense-route points whose
+        // solves run with 3xTF32 updates, then those of the FP64 points
         const int kd = (int)lu.size(), kh = (int)hs.size();
         csrc.insert(csrc.end(), csrcV.begin(), csrcV.end());
         cdst.insert(cdst.end(), cdstV.begin(), cdstV.end());
-        lu.insert(lu.end(), luV.begin(), luV.end());
-        rhs.insert(rhs.end(), rhsV.begin(), rhsV.end());
-        const std::vector<int> ipointW = ipoint;
-        ipoint.insert(ipoint.end(), ipointW.begin(), ipointW.end());
+        {
+          std::vector<cplx*> l2, r2;
+          std::vector<int> i2;
+          auto put = [&](int q0, int q1) {
+            for (int q = q0; q < q1; ++q) { l2.push_back(lu[q]); r2.push_back(rhs[q]); i2.push_back(ipoint[q]); }
+            for (int q = q0; q < q1; ++q) { l2.push_back(luV[q]); r2.push_back(rhsV[q]); i2.push_back(ipoint[q]); }
+          };
+          put(0, kdt);
+          put(kdt, kd);
+          lu = l2;
+          rhs = r2;
+          ipoint = i2;
+        }
         const int ncopy = (int)csrc.size();
         const size_t ocs = meta.add_vec(csrc), ocd = meta.add_vec(cdst), olu = meta.add_vec(lu), orhs = meta.add_vec(rhs);
         const size_t oip = meta.add_vec(ipoint), osp = meta.add_vec(spoint), ohs = meta.add_vec(hs);
@@ -1187,11 +1200,23 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           // interface matrices IE = Wa^-1 Wb, IH = Va^-1 Vb (rcwa/RCWASolver.cpp:537-543)
           if ((err = zcopy_batched(cpa(ocs), n, pa(ocd), n, n, n, ncopy, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
-          if ((err = zgetrf_batched(pa(olu), n, n, pipiv, pinfo, 2 * kd, st, lu_if)) != cudaSuccess) return err;
+          // factorisations and solves: the first 2 kdt with 3xTF32 updates
+          // between 128-wide blocks, the rest in FP64
+          const TcProducts tcx{tcscale, tcerr, planes, planes_bytes};
+          if (kdt > 0 && (err = zgetrf_blocked_batched(pa(olu), n, n, pipiv, pinfo, 2 * kdt, &tcx, st)) != cudaSuccess)
+            return err;
+          if (kd > kdt && (err = zgetrf_batched(pa(olu) + 2 * kdt, n, n, pipiv + (size_t)2 * kdt * n, pinfo + 2 * kdt,
+                                                2 * (kd - kdt), st, lu_if)) != cudaSuccess)
+            return err;
           if ((err = fold_info(pinfo, (const int*)(m + oip), 2 * kd, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStInterfaceLU);
-          if ((err = zgetrs_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * kd, st)) != cudaSuccess) return err;
+          if (kdt > 0 && (err = zgetrs_blocked_batched(cpa(olu), n, n, pipiv, pa(orhs), n, n, 2 * kdt, false, &tcx,
+                                                       st)) != cudaSuccess)
+            return err;
+          if (kd > kdt && (err = zgetrs_batched(cpa(olu) + 2 * kdt, n, n, pipiv + (size_t)2 * kdt * n,
+                                                pa(orhs) + 2 * kdt, n, n, 2 * (kd - kdt), st)) != cudaSuccess)
+            return err;
           if ((err = halfspace_solve((const HalfSolveItem*)(m + ohs), kh, N, status, st)) != cudaSuccess) return err;
           pf.mark(st, kStInterface);
           if (nph > 0) {
@@ -1215,12 +1240,21 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           if ((err = zaxpby_batched(cpa(osF), cpa(osG), pa(osD), mkc(1, 0), mkc(1, 0), n, k, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStTau);
-          if ((err = zgetrf_batched(pa(oSp), n, n, pipiv, pinfo, k, st, lu_tau)) != cudaSuccess) return err;
+          if (kt > 0 && (err = zgetrf_blocked_batched(pa(oSp), n, n, pipiv, pinfo, kt, &tcx, st)) != cudaSuccess)
+            return err;
+          if (k > kt && (err = zgetrf_batched(pa(oSp) + kt, n, n, pipiv + (size_t)kt * n, pinfo + kt, k - kt, st,
+                                              lu_tau)) != cudaSuccess)
+            return err;
           if ((err = fold_info(pinfo, (const int*)(m + osp), k, RCWA_ERR_SINGULAR, status, st)) != cudaSuccess)
             return err;
           pf.mark(st, kStTauLU);
           // tau = (F + G)^-1 in the getri order (PartialPivLU::inverse, :451-453)
-          if ((err = zgetri_batched(cpa(oSp), n, n, pipiv, pa(otau), n, k, st)) != cudaSuccess) return err;
+          if (kt > 0 && (err = zgetrs_blocked_batched(cpa(oSp), n, n, pipiv, pa(otau), n, n, kt, true, &tcx, st)) !=
+                            cudaSuccess)
+            return err;
+          if (k > kt && (err = zgetri_batched(cpa(oSp) + kt, n, n, pipiv + (size_t)kt * n, pa(otau) + kt, n, k - kt,
+                                              st)) != cudaSuccess)
+            return err;
           pf.mark(st, kStTau);
           // Rud = I - 2 G tau ; Tdd = 2 waveTdd tau  (:457-460)
           g.A = cpa(otG); g.B = cpa(otTau); g.C = nullptr; g.D = pa(orD);

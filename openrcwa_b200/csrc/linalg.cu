@@ -13,6 +13,7 @@
 #include <cooperative_groups.h>
 
 #include "linalg.cuh"
+#include "lu_blocked.cuh"
 #include "tile.cuh"
 
 namespace {
@@ -374,12 +375,13 @@ __global__ void __launch_bounds__(kLuPanelThreads) getrf_panel_team_kernel(cplx*
 }
 
 // U12 of the multi-launch LU: one CTA per (matrix, 64 columns right of the
-// panel), a thread per column; the unit lower L11 (jb <= kLuPanel) is read
-// through the read-only path (every thread reads the same entry).
-__global__ void __launch_bounds__(64) getrf_trsm_kernel(cplx* const* Aarr, int n, int lda, int kb, int jb) {
+// panel, up to column ce), a thread per column; the unit lower L11 (jb <=
+// kLuPanel) is read through the read-only path (every thread reads the same
+// entry).
+__global__ void __launch_bounds__(64) getrf_trsm_kernel(cplx* const* Aarr, int lda, int kb, int jb, int ce) {
   cplx* A = Aarr[blockIdx.y];
   const int c = kb + jb + blockIdx.x * 64 + threadIdx.x;
-  if (c >= n) return;
+  if (c >= ce) return;
   for (int r = 1; r < jb; ++r) {
     cplx x = A[(size_t)(kb + r) * lda + c];
     const cplx* Lr = A + (size_t)(kb + r) * lda + kb;
@@ -686,24 +688,31 @@ cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info,
     ++launch_counter();
     return cudaGetLastError();
   }
+  if (schedule == 2) return zgetrf_blocked_batched(A, n, lda, ipiv, info, batch, nullptr, st);
+  return zgetrf_columns(A, n, lda, 0, n, ipiv, info, batch, st);
+}
+
+cudaError_t zgetrf_columns(cplx* const* A, int n, int lda, int k0, int ce, int* ipiv, int* info, int batch,
+                           cudaStream_t st) {
+  if (batch <= 0 || k0 < 0 || ce > n || k0 >= ce) return cudaErrorInvalidValue;
   // a cluster of CTAs per matrix shares each panel when the batch leaves SMs idle
   const int team = lu_team_size(n, batch);
-  for (int kb = 0; kb < n; kb += kLuPanel) {
-    const int jb = min(kLuPanel, n - kb);
+  for (int kb = k0; kb < ce; kb += kLuPanel) {
+    const int jb = min(kLuPanel, ce - kb);
     cudaError_t pe = launch_panel(A, n, lda, kb, jb, ipiv, info, batch, team, st);
     if (pe != cudaSuccess) return pe;
     ++launch_counter();
-    const int m2 = n - kb - jb;
-    if (m2 <= 0) break;
-    getrf_trsm_kernel<<<dim3((m2 + 63) / 64, batch), 64, 0, st>>>(A, n, lda, kb, jb);
+    const int m2 = n - kb - jb, w = ce - kb - jb;
+    if (m2 <= 0 || w <= 0) break;
+    getrf_trsm_kernel<<<dim3((w + 63) / 64, batch), 64, 0, st>>>(A, lda, kb, jb, ce);
     ++launch_counter();
-    // A22 -= L21 U12
+    // A22 -= L21 U12 (the block's columns)
     GemmArgs g{};
     g.A = A; g.B = A; g.C = A; g.D = A;
     g.offA = (size_t)(kb + jb) * lda + kb;
     g.offB = (size_t)kb * lda + kb + jb;
     g.offC = g.offD = (size_t)(kb + jb) * lda + kb + jb;
-    g.M = m2; g.N = m2; g.K = jb;
+    g.M = m2; g.N = w; g.K = jb;
     g.lda = g.ldb = g.ldc = g.ldd = lda;
     g.alpha = mkc(-1.0, 0.0); g.beta = mkc(1.0, 0.0); g.gammaI = mkc(0.0, 0.0);
     g.batch = batch;
@@ -713,9 +722,19 @@ cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info,
   return cudaGetLastError();
 }
 
+// From this order on, solves with at least 64 right-hand sides run blocked
+// (lu_blocked.cu: 128-row triangles plus batched GEMM updates over the whole
+// grid) instead of one CTA per 64-column slab; a build parameter.
+#ifndef RCWA_BLOCKED_SOLVE_MIN_N
+#define RCWA_BLOCKED_SOLVE_MIN_N 256
+#endif
+constexpr int kBlockedSolveMinN = RCWA_BLOCKED_SOLVE_MIN_N;
+
 cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipiv, cplx* const* B,
                            int nrhs, int ldb, int batch, cudaStream_t st) {
   if (batch <= 0 || n <= 0 || nrhs <= 0) return cudaSuccess;
+  if (n >= kBlockedSolveMinN && nrhs >= 64)
+    return zgetrs_blocked_batched(LU, n, lda, ipiv, B, nrhs, ldb, batch, false, nullptr, st);
   dim3 grid((nrhs + 63) / 64, batch);
   zgetrs_kernel<false><<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, B, nrhs, ldb);
   ++launch_counter();
@@ -725,11 +744,17 @@ cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipi
 cudaError_t zgetri_batched(const cplx* const* LU, int n, int lda, const int* ipiv, cplx* const* X, int ldx,
                            int batch, cudaStream_t st) {
   if (batch <= 0 || n <= 0) return cudaSuccess;
+  if (n >= kBlockedSolveMinN) return zgetrs_blocked_batched(LU, n, lda, ipiv, X, n, ldx, batch, true, nullptr, st);
   dim3 grid((n + 63) / 64, batch);
   zgetrs_kernel<true><<<grid, kTileThreads, 0, st>>>(LU, n, lda, ipiv, X, n, ldx);
   ++launch_counter();
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  return zcolperm_batched(X, n, ldx, ipiv, batch, st);
+}
+
+cudaError_t zcolperm_batched(cplx* const* X, int n, int ldx, const int* ipiv, int batch, cudaStream_t st) {
+  cudaError_t e;
   // rows per CTA: as many as fit in 64 KB next to the permutation
   const size_t perm_bytes = ((size_t)n * sizeof(int) + 15) & ~(size_t)15;
   const int rows = (int)std::max<size_t>(1, std::min<size_t>(8, (64u << 10) / ((size_t)n * sizeof(cplx))));

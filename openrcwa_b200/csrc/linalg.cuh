@@ -36,11 +36,20 @@ cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st);
 // schedule 1: panel by panel, the panel factorisation one CTA per matrix and
 // the triangular solve and trailing update spread over all SMs; -1: the
 // default rule (zgetrf_default_schedule: schedule 0 for n <= 128 or batches of
-// at least four waves of CTAs, else 1).  Both pivot by the same rule; their
-// rounding differs in the trailing updates.
+// at least four waves of CTAs, else 1); schedule 2: 128-column blocks, each
+// factorised as in schedule 1 and followed by one K = 128 trailing update
+// (zgetrf_blocked_batched in lu_blocked.cuh).  All pivot by the same rule;
+// their rounding differs in the trailing updates.
 int zgetrf_default_schedule(int n, int batch, int sms = 0);  // sms <= 0: this device's SM count
 cudaError_t zgetrf_batched(cplx* const* A, int n, int lda, int* ipiv, int* info, int batch,
                            cudaStream_t st, int schedule = -1);
+// Columns k0 .. ce-1 of the panel-by-panel LU, whose columns before k0 are
+// factorised and whose columns from k0 on have taken every update of them:
+// 32-column panels (row interchanges across whole rows) with the U12 solves
+// and FP64 trailing updates confined to columns < ce.  The columns from ce on
+// are left to the caller (a blocked LU's trailing update).  k0 = 0 clears info.
+cudaError_t zgetrf_columns(cplx* const* A, int n, int lda, int k0, int ce, int* ipiv, int* info, int batch,
+                           cudaStream_t st);
 
 // Solve A X = B in place of B (n x nrhs) from the factors of zgetrf_batched.
 cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipiv,
@@ -52,6 +61,10 @@ cudaError_t zgetrs_batched(const cplx* const* LU, int n, int lda, const int* ipi
 // zgetrs_batched on the identity.
 cudaError_t zgetri_batched(const cplx* const* LU, int n, int lda, const int* ipiv, cplx* const* X, int ldx,
                            int batch, cudaStream_t st);
+
+// X <- X P for the column interchanges of zgetrf_batched (LAPACK getri's
+// last step), every batch item.
+cudaError_t zcolperm_batched(cplx* const* X, int n, int ldx, const int* ipiv, int batch, cudaStream_t st);
 
 // B = I (n x n) for every batch item.
 cudaError_t zset_identity_batched(cplx* const* B, int n, int ldb, int batch, cudaStream_t st);

@@ -100,7 +100,12 @@ int tune_batch_class(int batch, int sms) {
 
 int tune_candidates(int op, int n, int* out) {
   switch (op) {
-    case kTuneLU: out[0] = 0; out[1] = 1; return 2;
+    case kTuneLU:
+      // 128-column blocks need room for a block and a trailing matrix
+      out[0] = 0; out[1] = 1;
+      if (n < 256) return 2;
+      out[2] = 2;
+      return 3;
     case kTuneSchur:
       // the crossover only matters while small active blocks are a large part
       // of the iteration; from 512 rows on the multishift phase dominates

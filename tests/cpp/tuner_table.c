@@ -20,7 +20,8 @@ int main(int argc, char** argv) {
   CHECK(rcwa_tuner_create(&t) == RCWA_OK && t);
   CHECK(rcwa_tuner_set_sms(t, 148) == RCWA_OK);
   int c[4];
-  CHECK(rcwa_tuner_candidates(RCWA_TUNE_LU, 882, c) == 2 && c[0] == 0 && c[1] == 1);
+  CHECK(rcwa_tuner_candidates(RCWA_TUNE_LU, 882, c) == 3 && c[0] == 0 && c[1] == 1 && c[2] == 2);
+  CHECK(rcwa_tuner_candidates(RCWA_TUNE_LU, 200, c) == 2);
   CHECK(rcwa_tuner_candidates(RCWA_TUNE_SCHUR, 300, c) == 4 && c[3] == 192);
   CHECK(rcwa_tuner_candidates(7, 300, c) == -1);
   CHECK(rcwa_tuner_default(t, RCWA_TUNE_LU, 882, 148) == 1);
@@ -35,7 +36,7 @@ int main(int argc, char** argv) {
   int op, n, cls, ch, nc, cand[4];
   double ms[4];
   CHECK(rcwa_tuner_entry(t, 0, &op, &n, &cls, &ch, &nc, cand, ms) == RCWA_OK);
-  CHECK(op == RCWA_TUNE_LU && n == 882 && cls == 2 && ch == 0 && nc == 2);
+  CHECK(op == RCWA_TUNE_LU && n == 882 && cls == 2 && ch == 0 && nc == 3);
   CHECK(rcwa_tuner_entry(t, 2, &op, &n, &cls, &ch, &nc, cand, ms) == RCWA_ERR_INVALID);
   CHECK(rcwa_tuner_save(t, path) == RCWA_OK);
   rcwa_tuner* u = NULL;

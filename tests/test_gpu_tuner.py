@@ -71,6 +71,28 @@ def test_every_schedule_matches_oracle(eng, case, lu, cross):
     _check_oracle(R, T, REF, TRN, ref)
 
 
+def test_blocked_lu_schedule_matches_oracle(eng):
+    # LU choice 2 (128-column blocks, K = 128 trailing updates) at n = 338:
+    # three blocks, the last one ragged
+    st, pts, pxy, ref = _stack_points(_setup(12, 6))
+    n = 2 * st.N
+    t = o.Tuner()
+    for b in (len(pts), 2 * len(pts)):
+        t.set("lu", n, b, 2)
+    eng.set_tuner(t, o.RCWA_TUNING_TABLE)
+    try:
+        plan = eng.plan([st], pts, pxy)
+        sched = plan.schedule()[0]
+        assert sched["lu_interface"] == 2 and sched["lu_tau"] == 2
+        plan.execute()
+        R, T, ref_o, trn_o, status = plan.results(orders=True)
+        plan.close()
+    finally:
+        eng.set_tuner(None, o.RCWA_TUNING_OFF)
+    assert not np.any(status)
+    _check_oracle(R, T, ref_o.reshape(len(pts), pxy.shape[1], st.N), trn_o.reshape(len(pts), pxy.shape[1], st.N), ref)
+
+
 def test_mixed_plan_with_fp64_products_equals_fp64_plan(eng, case):
     st, pts, pxy, _ = case
     n = 2 * st.N

@@ -19,7 +19,8 @@ def tuner():
 
 def test_candidates(tuner):
     o, t = tuner
-    assert t.candidates("lu", 882) == [0, 1]
+    assert t.candidates("lu", 882) == [0, 1, 2]
+    assert t.candidates("lu", 200) == [0, 1]
     assert t.candidates("product", 98) == [0, 1, 2]
     assert t.candidates("schur", 242) == [64, 96, 128, 192]
     assert t.candidates("schur", 882) == [64]  # large matrices: multishift phase dominates
@@ -64,7 +65,9 @@ def test_invalid_choices_rejected(tuner):
     with pytest.raises(o.RcwaError):
         t.set("schur", 450, 10, 80)
     with pytest.raises(o.RcwaError):
-        t.set("lu", 882, 10, 2)
+        t.set("lu", 882, 10, 3)
+    with pytest.raises(o.RcwaError):
+        t.set("lu", 200, 10, 2)   # 128-column blocks need n >= 256
     with pytest.raises(o.RcwaError):
         t.set("schur", 40, 10, 96)
     with pytest.raises(o.RcwaError):
