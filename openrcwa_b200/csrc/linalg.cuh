@@ -36,7 +36,7 @@ cudaError_t zgemm_batched(const GemmArgs& g, cudaStream_t st);
 // schedule 1: panel by panel, the panel factorisation one CTA per matrix and
 // the triangular solve and trailing update spread over all SMs; -1: the
 // default rule (zgetrf_default_schedule: schedule 0 for n <= 128 or batches of
-// at least four waves of CTAs, else 1); schedule 2: 128-column blocks, each
+// at least four waves of CTAs, else 2 from n = 256 on, else 1); schedule 2: 128-column blocks, each
 // factorised as in schedule 1 and followed by one K = 128 trailing update
 // (zgetrf_blocked_batched in lu_blocked.cuh).  All pivot by the same rule;
 // their rounding differs in the trailing updates.

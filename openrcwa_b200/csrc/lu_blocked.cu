@@ -56,6 +56,7 @@ template <bool kUpper>
 __global__ void __launch_bounds__(64) trsm_diag_kernel(const cplx* const* LUarr, int lda, cplx* const* Barr, int ldb,
                                                       int nrhs, int r0, int rows, int c_lo) {
   __shared__ cplx Tsm[32][33];
+  __shared__ cplx dinv[32];  // backward: reciprocals of the quarter's diagonal
   const int b = blockIdx.y;
   const int c = c_lo + blockIdx.x * 64 + threadIdx.x;
   const bool col = c < nrhs;
@@ -68,41 +69,51 @@ __global__ void __launch_bounds__(64) trsm_diag_kernel(const cplx* const* LUarr,
     cplx x[32];
 #pragma unroll
     for (int r = 0; r < 32; ++r) x[r] = (col && r < hw) ? B[(size_t)(h0 + r) * ldb + c] : mkc(0.0, 0.0);
-    // the quarters already solved: above (forward) or below (backward)
+    // the quarters already solved: above (forward) or below (backward); their
+    // values come back four at a time so the loads overlap
     for (int s2 = 0; s2 < step; ++s2) {
       const int pj = kUpper ? nq - 1 - s2 : s2;
       const int p0 = r0 + 32 * pj, pw = min(32, r0 + rows - p0);
       __syncthreads();
       load_tile32(Tsm, LU, lda, h0, p0, hw, pw);
       __syncthreads();
-      if (col)
-        for (int q = 0; q < pw; ++q) {
-          const cplx y = B[(size_t)(p0 + q) * ldb + c];
+      if (col) {
 #pragma unroll
-          for (int r = 0; r < 32; ++r) x[r] = cfma(cneg(Tsm[r][q]), y, x[r]);
+        for (int q0 = 0; q0 < 32; q0 += 4) {
+          cplx y[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) y[u] = q0 + u < pw ? B[(size_t)(p0 + q0 + u) * ldb + c] : mkc(0.0, 0.0);
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int r = 0; r < 32; ++r) x[r] = cfma(cneg(Tsm[r][q0 + u]), y[u], x[r]);
         }
+      }
     }
     __syncthreads();
     load_tile32(Tsm, LU, lda, h0, h0, hw, hw);
+    if (kUpper) {
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        const int q = threadIdx.x;
+        dinv[q] = q < hw ? cdiv(mkc(1.0, 0.0), Tsm[q][q]) : mkc(0.0, 0.0);
+      }
+    }
     __syncthreads();
+    // the quarter's own triangle, column by column: each finished entry
+    // updates the rows still open, all independent of one another
     if (col) {
       if (!kUpper) {
 #pragma unroll
-        for (int r = 1; r < 32; ++r) {
-          cplx acc = x[r];
+        for (int q = 0; q < 31; ++q)
 #pragma unroll
-          for (int q = 0; q < r; ++q) acc = cfma(cneg(Tsm[r][q]), x[q], acc);
-          x[r] = acc;
-        }
+          for (int r = q + 1; r < 32; ++r) x[r] = cfma(cneg(Tsm[r][q]), x[q], x[r]);
       } else {
 #pragma unroll
-        for (int r = 31; r >= 0; --r) {
-          if (r < hw) {
-            cplx acc = x[r];
+        for (int q = 31; q >= 0; --q) {
+          x[q] = cmul(x[q], dinv[q]);
 #pragma unroll
-            for (int q = r + 1; q < 32; ++q) acc = cfma(cneg(Tsm[r][q]), x[q], acc);
-            x[r] = cdiv(acc, Tsm[r][r]);
-          }
+          for (int r = 0; r < q; ++r) x[r] = cfma(cneg(Tsm[r][q]), x[q], x[r]);
         }
       }
 #pragma unroll

@@ -24,7 +24,8 @@ int main(int argc, char** argv) {
   CHECK(rcwa_tuner_candidates(RCWA_TUNE_LU, 200, c) == 2);
   CHECK(rcwa_tuner_candidates(RCWA_TUNE_SCHUR, 300, c) == 4 && c[3] == 192);
   CHECK(rcwa_tuner_candidates(7, 300, c) == -1);
-  CHECK(rcwa_tuner_default(t, RCWA_TUNE_LU, 882, 148) == 1);
+  CHECK(rcwa_tuner_default(t, RCWA_TUNE_LU, 882, 148) == 2);
+  CHECK(rcwa_tuner_default(t, RCWA_TUNE_LU, 200, 148) == 1);
   CHECK(rcwa_tuner_default(t, RCWA_TUNE_LU, 882, 600) == 0);
   CHECK(rcwa_tuner_set(t, RCWA_TUNE_SCHUR, 300, 20, 96) == RCWA_OK);
   CHECK(rcwa_tuner_set(t, RCWA_TUNE_LU, 882, 296, 0) == RCWA_OK);  /* 2 waves */

@@ -31,9 +31,11 @@ def test_candidates(tuner):
 
 def test_default_rules(tuner):
     _, t = tuner
-    # LU: one CTA per matrix for n <= 128 or >= 4 waves of matrices, else panels
-    assert t.default("lu", 882, 148) == 1
-    assert t.default("lu", 882, 591) == 1
+    # LU: one CTA per matrix for n <= 128 or >= 4 waves of matrices, else
+    # 128-column blocks from n = 256 on, panels below
+    assert t.default("lu", 882, 148) == 2
+    assert t.default("lu", 882, 591) == 2
+    assert t.default("lu", 200, 148) == 1
     assert t.default("lu", 882, 592) == 0
     assert t.default("lu", 128, 10) == 0
     assert t.default("schur", 882, 740) == 64
