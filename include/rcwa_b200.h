@@ -402,6 +402,27 @@ int rcwa_star_product_batched(rcwa_engine* e, int n, int batch,
                               const rcwa_cplx* rud, const rcwa_cplx* rdu,
                               const rcwa_cplx* tdd, const rcwa_cplx* tuu, int* status);
 
+/* RCWAIntegrator::compute(N) (core/RCWAIntegrator.cpp:21-86) over the
+ * sampler's matrices: P, Q [nslab + 2][n*n] row-major as LayerSampler::sample
+ * (core/LayerSampler.h:51-53) gives them at depth z0 (sample 0), at the
+ * midpoints z0 + (i + 1/2)(z1 - z0)/nslab of the nslab slabs (samples
+ * 1 .. nslab) and at z1 (sample nslab + 1).  Every sample's modes come from
+ * WaveEquationSolver::solve (eigenvectors W of P Q, keff = GammaSqrtOp of the
+ * eigenvalues, V = Q W keff^-1); the slabs' S-matrices are taken against the
+ * modes at z1 and cascaded with the star product, pairwise in ceil(log2
+ * nslab) batched levels (the product is associative; the reference folds
+ * them from the top down), and the last step brings the top side into the
+ * modes at z0.  Outputs (any may be NULL) as the integrator's accessors:
+ * Rud, Rdu, Tdd, Tuu [n*n]; W0, V0 [n*n], gam0 [n] (z0); W1, V1, gam1 (z1).
+ * nslab = 0 is the region without slabs (the identity S-matrix brought into
+ * the modes at z0).  Returns RCWA_ERR_NOCONV / RCWA_ERR_NONFINITE from an
+ * eigensolve, RCWA_ERR_SINGULAR from an LU, else RCWA_OK. */
+int rcwa_rcwa_integrate(rcwa_engine* e, int n, int nslab, double lambda, double z0, double z1,
+                        const rcwa_cplx* P, const rcwa_cplx* Q,
+                        rcwa_cplx* Rud, rcwa_cplx* Rdu, rcwa_cplx* Tdd, rcwa_cplx* Tuu,
+                        rcwa_cplx* W0, rcwa_cplx* V0, rcwa_cplx* gam0,
+                        rcwa_cplx* W1, rcwa_cplx* V1, rcwa_cplx* gam1);
+
 /* ---- eigensolver without device allocation ---------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (code running inside another framework's memory pool, real-time loops where

@@ -40,7 +40,7 @@ EXPORTS = [
     "rcwa_plan_launch_count", "rcwa_plan_rescatter", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
-    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_zgemm_batched",
+    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_rcwa_integrate", "rcwa_zgemm_batched",
     "rcwa_mlp_create", "rcwa_mlp_destroy", "rcwa_mlp_param_count", "rcwa_mlp_get_params", "rcwa_mlp_set_params",
     "rcwa_mlp_set_data", "rcwa_mlp_train", "rcwa_mlp_loss_grad", "rcwa_mlp_predict_fp32", "rcwa_mlp_predict",
     "rcwa_plan_schedule", "rcwa_tuner_create", "rcwa_tuner_destroy", "rcwa_tuner_set_sms", "rcwa_tuner_candidates",
@@ -141,6 +141,8 @@ def load() -> C.CDLL:
     lib.rcwa_slab_smatrix_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 5 + [_DP, _DP] + \
         [C.c_void_p, C.c_void_p, _IP]
     lib.rcwa_star_product_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 8 + [_IP]
+    lib.rcwa_rcwa_integrate.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double] + \
+        [C.c_void_p] * 12
     lib.rcwa_zgemm_batched.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, rcwa_cplx, rcwa_cplx, C.c_int, C.c_void_p]
     _FP = C.POINTER(C.c_float)
@@ -459,6 +461,24 @@ class Engine:
         if rc and not np.any(st):
             self._check(rc, "star_product")
         return {"Rud": Rud, "Rdu": Rdu, "Tdd": Tdd, "Tuu": Tuu}, st
+
+    def rcwa_integrate(self, P, Q, lam, z0, z1):
+        """RCWAIntegrator::compute (core/RCWAIntegrator.cpp:21-86) over sampled
+        matrices: P, Q (nslab + 2, n, n) at z0, the slab midpoints and z1.
+        Returns a dict with Rud, Rdu, Tdd, Tuu, W0, V0, gam0, W1, V1, gam1."""
+        P = np.ascontiguousarray(P, dtype=np.complex128)
+        Q = np.ascontiguousarray(Q, dtype=np.complex128)
+        if P.ndim != 3 or P.shape != Q.shape or P.shape[1] != P.shape[2] or P.shape[0] < 2:
+            raise ValueError("P, Q must be (nslab + 2, n, n)")
+        ns, n = P.shape[0], P.shape[1]
+        out = {k: np.zeros((n, n), dtype=np.complex128) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "W1", "V1")}
+        out["gam0"] = np.zeros(n, dtype=np.complex128)
+        out["gam1"] = np.zeros(n, dtype=np.complex128)
+        rc = self.lib.rcwa_rcwa_integrate(self.h, n, ns - 2, float(lam), float(z0), float(z1), _v(P), _v(Q),
+                                          *[_v(out[k]) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "gam0",
+                                                                 "W1", "V1", "gam1")])
+        self._check(rc, "rcwa_integrate")
+        return out
 
     def ofd_solve(self, setup, orders=True):
         """The rcwa_run computation for a setup object with the

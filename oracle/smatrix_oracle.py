@@ -12,6 +12,8 @@ Restates, in NumPy:
   (rcwa/RCWAScatterMatrix.h:40-47).
 * the Redheffer star product of the z-integrators
   (core/RCWAIntegrator.cpp:57-67, core/RedhefferIntegrator.cpp:136-146).
+* RCWAIntegrator::compute (core/RCWAIntegrator.cpp:21-86) over sampled P, Q.
+* DifferentialIntegrator::compute (core/DifferentialIntegrator.cpp:21-133).
 
 Eigen's ``PartialPivLU::solve`` / ``inverse`` map to ``numpy.linalg.solve`` /
 ``numpy.linalg.inv`` (LAPACK getrf/getrs/getri).
@@ -73,3 +75,119 @@ def identity_smatrix(n):
     I = np.eye(n, dtype=complex)
     Z = np.zeros((n, n), dtype=complex)
     return {"Tdd": I.copy(), "Tuu": I.copy(), "Rud": Z.copy(), "Rdu": Z.copy()}
+
+
+def wave_equation_modes(P, Q):
+    """WaveEquationSolver::solve (rcwa/WaveEquationSolver.cpp:24-37) with
+    LAPACK's zgeev: W = eigenvectors of P Q, keff = GammaSqrtOp(eigenvalues),
+    V = Q W keff^-1."""
+    from oracle.rcwa_oracle import gamma_sqrt
+    lam, W = np.linalg.eig(P @ Q)
+    keff = gamma_sqrt(lam)
+    V = (Q @ W) / keff[None, :]
+    return W, V, keff
+
+
+def rcwa_integrate(P, Q, lam, z0, z1):
+    """RCWAIntegrator::compute (core/RCWAIntegrator.cpp:21-86) over given samples.
+
+    ``P[k], Q[k]`` are the sampler's matrices (LayerSampler::sample) at the
+    depths z0 (k = 0), the midpoints z0 + (i + 1/2) dz of the N = len(P) - 2
+    slabs (k = 1 .. N, dz = (z1 - z0) / N) and z1 (k = N + 1).  Every slab's
+    S-matrix is taken against the modes at z1 (:28-34, :49-50), the slabs are
+    cascaded from the top down with the star product (:36-68), and the last
+    step brings the top side into the modes at z0 (:70-85).  Returns a dict
+    with Tdd, Tuu, Rud, Rdu, W0, V0, gam0, W1, V1, gam1.
+    """
+    N = len(P) - 2
+    W1, V1, g1 = wave_equation_modes(P[N + 1], Q[N + 1])
+    n = W1.shape[0]
+    S = identity_smatrix(n)
+    dz = (z1 - z0) / N if N > 0 else 0.0
+    for i in range(N):
+        W, V, g = wave_equation_modes(P[1 + i], Q[1 + i])
+        rud, tuu = slab_smatrix(W, V, g, W1, V1, lam, dz)
+        S = star_product(S, {"rud": rud, "rdu": rud, "tdd": tuu, "tuu": tuu})
+    W0, V0, g0 = wave_equation_modes(P[0], Q[0])
+    F = np.linalg.solve(W1, W0)
+    G = np.linalg.solve(V1, V0)
+    A = 0.5 * (F + G)
+    B = 0.5 * (F - G)
+    M = A - S["Rdu"] @ B
+    Rdu = np.linalg.solve(M, S["Rdu"] @ A - B)
+    Tdd = np.linalg.solve(M, S["Tdd"])
+    Rud = S["Tuu"] @ B @ Tdd + S["Rud"]
+    Tuu = S["Tuu"] @ (B @ Rdu + A)
+    return {"Tdd": Tdd, "Tuu": Tuu, "Rud": Rud, "Rdu": Rdu, "W0": W0, "V0": V0, "gam0": g0,
+            "W1": W1, "V1": V1, "gam1": g1}
+
+
+def field_space(out):
+    """The integrator's S-blocks as operators on tangential fields, free of the
+    eigenvectors' order, scale and phase: W0 Tdd W1^-1, W1 Tuu W0^-1,
+    W1 Rud W1^-1, W0 Rdu W0^-1 (Tdd and Rdu act on the z0 side on the left,
+    Tuu and Rud on the z1 side)."""
+    W0, W1 = out["W0"], out["W1"]
+    i0, i1 = np.linalg.inv(W0), np.linalg.inv(W1)
+    return {"Tdd": W0 @ out["Tdd"] @ i1, "Tuu": W1 @ out["Tuu"] @ i0,
+            "Rud": W1 @ out["Rud"] @ i1, "Rdu": W0 @ out["Rdu"] @ i0}
+
+
+def _top_projection(S, W1, V1, W0, V0):
+    """The last step of RCWAIntegrator / DifferentialIntegrator::compute
+    (core/RCWAIntegrator.cpp:73-85, core/DifferentialIntegrator.cpp:116-133):
+    the cascade, built in the modes at z1, brought into the modes at z0."""
+    F = np.linalg.solve(W1, W0)
+    G = np.linalg.solve(V1, V0)
+    A = 0.5 * (F + G)
+    B = 0.5 * (F - G)
+    M = A - S["Rdu"] @ B
+    Rdu = np.linalg.solve(M, S["Rdu"] @ A - B)
+    Tdd = np.linalg.solve(M, S["Tdd"])
+    Rud = S["Tuu"] @ B @ Tdd + S["Rud"]
+    Tuu = S["Tuu"] @ (B @ Rdu + A)
+    return {"Tdd": Tdd, "Tuu": Tuu, "Rud": Rud, "Rdu": Rdu}
+
+
+def differential_integrate(P, Q, lam, z0, z1):
+    """DifferentialIntegrator::compute (core/DifferentialIntegrator.cpp:21-133).
+
+    ``P[k], Q[k]`` are the sampler's matrices at z0 + k dz/2, k = 0 .. 2N
+    (dz = (z1 - z0) / N): every slab i takes its left end (2i), midpoint
+    (2i + 1) and right end (2i + 2).  The modes at z0 and z1 are those of
+    samples 0 and 2N.  Per slab the fourth-order transfer blocks L11, L12,
+    L21, L22 (:55-66) are taken into the modes at z1 (:73-86), turned into an
+    S-matrix (:93-97) and cascaded with the star product (:104-114).
+    """
+    N = (len(P) - 1) // 2
+    W1, V1, g1 = wave_equation_modes(P[2 * N], Q[2 * N])
+    W0, V0, g0 = wave_equation_modes(P[0], Q[0])
+    n = W1.shape[0]
+    k0 = 2 * math.pi / lam
+    dz = (z1 - z0) / N
+    I = np.eye(n)
+    S = identity_smatrix(n)
+    c = dz * dz / (k0 * k0)
+    for i in range(N):
+        P0, P1, P2 = P[2 * i], P[2 * i + 1], P[2 * i + 2]
+        Q0, Q1, Q2 = Q[2 * i], Q[2 * i + 1], Q[2 * i + 2]
+        L11 = I - c / 6 * (P1 @ Q0 + P1 @ Q1 + P2 @ Q1 - c / 4 * P2 @ Q1 @ P1 @ Q0)
+        L12 = 1j * dz / (6 * k0) * (P0 + 4 * P1 + P2 - c / 2 * (P1 @ Q1 @ P0 + P2 @ Q1 @ P1))
+        L21 = 1j * dz / (6 * k0) * (Q0 + 4 * Q1 + Q2 - c / 2 * (Q1 @ P1 @ Q0 + Q2 @ P1 @ Q1))
+        L22 = I - c / 6 * (Q1 @ P0 + Q1 @ P1 + Q2 @ P1 - c / 4 * Q2 @ P1 @ Q1 @ P0)
+        wl11, wl12 = np.linalg.solve(W1, L11), np.linalg.solve(W1, L12)
+        vl21, vl22 = np.linalg.solve(V1, L21), np.linalg.solve(V1, L22)
+        A11, A12 = 0.5 * (wl11 + vl21), 0.5 * (wl12 + vl22)
+        A21, A22 = 0.5 * (wl11 - vl21), 0.5 * (wl12 - vl22)
+        T11 = A11 @ W1 + A12 @ V1
+        T12 = A11 @ W1 - A12 @ V1
+        T21 = A21 @ W1 + A22 @ V1
+        T22 = A21 @ W1 - A22 @ V1
+        tdd = np.linalg.inv(T22)
+        rud = T12 @ tdd
+        rdu = -np.linalg.solve(T22, T21)
+        tuu = T11 + T12 @ rdu
+        S = star_product(S, {"rud": rud, "rdu": rdu, "tdd": tdd, "tuu": tuu})
+    out = _top_projection(S, W1, V1, W0, V0)
+    out.update({"W0": W0, "V0": V0, "gam0": g0, "W1": W1, "V1": V1, "gam1": g1})
+    return out
