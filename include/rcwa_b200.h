@@ -423,6 +423,44 @@ int rcwa_rcwa_integrate(rcwa_engine* e, int n, int nslab, double lambda, double 
                         rcwa_cplx* W0, rcwa_cplx* V0, rcwa_cplx* gam0,
                         rcwa_cplx* W1, rcwa_cplx* V1, rcwa_cplx* gam1);
 
+/* DifferentialIntegrator::compute(N) (core/DifferentialIntegrator.cpp:21-133):
+ * P, Q [2 nslab + 1][n*n] at z0 + k dz/2 (dz = (z1 - z0)/nslab), so slab i
+ * takes samples 2i, 2i + 1, 2i + 2 (its ends and midpoint); the modes at z0
+ * and z1 are those of samples 0 and 2 nslab.  Per slab the fourth-order
+ * transfer blocks L11, L12, L21, L22 (:55-66) are taken into the modes at z1
+ * and turned into an S-matrix (:73-97), all slabs in one batch; the cascade
+ * and the last step are those of rcwa_rcwa_integrate.  nslab >= 1; outputs
+ * and return codes as rcwa_rcwa_integrate. */
+int rcwa_differential_integrate(rcwa_engine* e, int n, int nslab, double lambda, double z0, double z1,
+                                const rcwa_cplx* P, const rcwa_cplx* Q,
+                                rcwa_cplx* Rud, rcwa_cplx* Rdu, rcwa_cplx* Tdd, rcwa_cplx* Tuu,
+                                rcwa_cplx* W0, rcwa_cplx* V0, rcwa_cplx* gam0,
+                                rcwa_cplx* W1, rcwa_cplx* V1, rcwa_cplx* gam1);
+
+/* LayerSampler::sample (core/LayerSampler.h:51-53) as a callback: P and Q
+ * (n*n row-major, host) at depth z; returns 0, or nonzero to abort. */
+typedef int (*rcwa_sampler)(void* user, double z, rcwa_cplx* P, rcwa_cplx* Q);
+
+/* RedhefferIntegrator::compute(p, maxN, pe) (core/RedhefferIntegrator.cpp:
+ * 190-328, its triple-division branch): an interval's first-order
+ * perturbation S-matrix about the modes at its midpoint
+ * (evaluatePerturbationAndDifference, :330-398) is accepted when no entry of
+ * its perturbation exceeds pe in modulus, else the interval is split in
+ * thirds (the middle third keeps the parent's modes).  The intervals of one
+ * subdivision level are evaluated in one batch (new samples through the
+ * callback, their modes in one batched eigensolve); the accepted intervals,
+ * in depth order, are projected from the modes above them, cascaded with the
+ * star product and the bottom brought into the modes at z1.  max_intervals
+ * bounds the accepted intervals (RCWA_ERR_NOCONV beyond it; the reference
+ * ignores maxN).  n_intervals = N(), n_eig = the eigen-solves performed (the
+ * reference's nEigVal() stays 2 in this branch).  Outputs as
+ * rcwa_rcwa_integrate; a failing callback gives RCWA_ERR_INVALID. */
+int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, double z0, double z1, double pe,
+                             int max_intervals, rcwa_sampler sample, void* user,
+                             rcwa_cplx* Rud, rcwa_cplx* Rdu, rcwa_cplx* Tdd, rcwa_cplx* Tuu,
+                             rcwa_cplx* W0, rcwa_cplx* V0, rcwa_cplx* gam0,
+                             rcwa_cplx* W1, rcwa_cplx* V1, rcwa_cplx* gam1, int* n_intervals, int* n_eig);
+
 /* ---- eigensolver without device allocation ---------------------------------
  * No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (code running inside another framework's memory pool, real-time loops where

@@ -40,7 +40,7 @@ EXPORTS = [
     "rcwa_plan_launch_count", "rcwa_plan_rescatter", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
-    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_rcwa_integrate", "rcwa_zgemm_batched",
+    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_rcwa_integrate", "rcwa_differential_integrate", "rcwa_redheffer_integrate", "rcwa_zgemm_batched",
     "rcwa_mlp_create", "rcwa_mlp_destroy", "rcwa_mlp_param_count", "rcwa_mlp_get_params", "rcwa_mlp_set_params",
     "rcwa_mlp_set_data", "rcwa_mlp_train", "rcwa_mlp_loss_grad", "rcwa_mlp_predict_fp32", "rcwa_mlp_predict",
     "rcwa_plan_schedule", "rcwa_tuner_create", "rcwa_tuner_destroy", "rcwa_tuner_set_sms", "rcwa_tuner_candidates",
@@ -53,6 +53,8 @@ EXPORTS = [
 
 _DP = C.POINTER(C.c_double)
 _IP = C.POINTER(C.c_int)
+# rcwa_sampler: int (*)(void* user, double z, rcwa_cplx* P, rcwa_cplx* Q)
+RCWA_SAMPLER = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p)
 
 
 class rcwa_cplx(C.Structure):
@@ -143,6 +145,9 @@ def load() -> C.CDLL:
     lib.rcwa_star_product_batched.argtypes = [C.c_void_p, C.c_int, C.c_int] + [C.c_void_p] * 8 + [_IP]
     lib.rcwa_rcwa_integrate.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double] + \
         [C.c_void_p] * 12
+    lib.rcwa_differential_integrate.argtypes = lib.rcwa_rcwa_integrate.argtypes
+    lib.rcwa_redheffer_integrate.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                             C.c_int, RCWA_SAMPLER, C.c_void_p] + [C.c_void_p] * 10 + [_IP, _IP]
     lib.rcwa_zgemm_batched.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                        C.c_void_p, rcwa_cplx, rcwa_cplx, C.c_int, C.c_void_p]
     _FP = C.POINTER(C.c_float)
@@ -462,23 +467,76 @@ class Engine:
             self._check(rc, "star_product")
         return {"Rud": Rud, "Rdu": Rdu, "Tdd": Tdd, "Tuu": Tuu}, st
 
+    def _integrate(self, fn, what, P, Q, nslab, lam, z0, z1):
+        n = P.shape[1]
+        out = {k: np.zeros((n, n), dtype=np.complex128) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "W1", "V1")}
+        out["gam0"] = np.zeros(n, dtype=np.complex128)
+        out["gam1"] = np.zeros(n, dtype=np.complex128)
+        rc = fn(self.h, n, nslab, float(lam), float(z0), float(z1), _v(P), _v(Q),
+                *[_v(out[k]) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "gam0", "W1", "V1", "gam1")])
+        self._check(rc, what)
+        return out
+
+    @staticmethod
+    def _samples(P, Q):
+        P = np.ascontiguousarray(P, dtype=np.complex128)
+        Q = np.ascontiguousarray(Q, dtype=np.complex128)
+        if P.ndim != 3 or P.shape != Q.shape or P.shape[1] != P.shape[2]:
+            raise ValueError("P, Q must be (samples, n, n)")
+        return P, Q
+
     def rcwa_integrate(self, P, Q, lam, z0, z1):
         """RCWAIntegrator::compute (core/RCWAIntegrator.cpp:21-86) over sampled
         matrices: P, Q (nslab + 2, n, n) at z0, the slab midpoints and z1.
         Returns a dict with Rud, Rdu, Tdd, Tuu, W0, V0, gam0, W1, V1, gam1."""
-        P = np.ascontiguousarray(P, dtype=np.complex128)
-        Q = np.ascontiguousarray(Q, dtype=np.complex128)
-        if P.ndim != 3 or P.shape != Q.shape or P.shape[1] != P.shape[2] or P.shape[0] < 2:
+        P, Q = self._samples(P, Q)
+        if P.shape[0] < 2:
             raise ValueError("P, Q must be (nslab + 2, n, n)")
-        ns, n = P.shape[0], P.shape[1]
+        return self._integrate(self.lib.rcwa_rcwa_integrate, "rcwa_integrate", P, Q, P.shape[0] - 2, lam, z0, z1)
+
+    def redheffer_integrate(self, sample, n, lam, z0, z1, pe, max_intervals=100000):
+        """RedhefferIntegrator::compute (core/RedhefferIntegrator.cpp:190-328):
+        ``sample(z)`` returns the (n, n) matrices (P, Q) at depth z.  Returns
+        the dict of rcwa_integrate plus N (accepted intervals) and n_eig."""
+        failure = []
+
+        def cb(user, z, Pp, Qp):
+            try:
+                P, Q = sample(z)
+                for src, dst in ((P, Pp), (Q, Qp)):
+                    a = np.ascontiguousarray(src, dtype=np.complex128)
+                    if a.shape != (n, n):
+                        raise ValueError("sampler returned shape %s" % (a.shape,))
+                    C.memmove(dst, a.ctypes.data, a.nbytes)
+                return 0
+            except Exception as ex:  # reported after the call
+                failure.append(ex)
+                return 1
+
+        fn = RCWA_SAMPLER(cb)
         out = {k: np.zeros((n, n), dtype=np.complex128) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "W1", "V1")}
         out["gam0"] = np.zeros(n, dtype=np.complex128)
         out["gam1"] = np.zeros(n, dtype=np.complex128)
-        rc = self.lib.rcwa_rcwa_integrate(self.h, n, ns - 2, float(lam), float(z0), float(z1), _v(P), _v(Q),
-                                          *[_v(out[k]) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "gam0",
-                                                                 "W1", "V1", "gam1")])
-        self._check(rc, "rcwa_integrate")
+        cnt = np.zeros(2, dtype=np.int32)
+        rc = self.lib.rcwa_redheffer_integrate(
+            self.h, n, float(lam), float(z0), float(z1), float(pe), int(max_intervals), fn, None,
+            *[_v(out[k]) for k in ("Rud", "Rdu", "Tdd", "Tuu", "W0", "V0", "gam0", "W1", "V1", "gam1")],
+            _i(cnt[0:1]), _i(cnt[1:2]))
+        if failure:
+            raise failure[0]
+        self._check(rc, "redheffer_integrate")
+        out["N"], out["n_eig"] = int(cnt[0]), int(cnt[1])
         return out
+
+    def differential_integrate(self, P, Q, lam, z0, z1):
+        """DifferentialIntegrator::compute (core/DifferentialIntegrator.cpp:21-133)
+        over sampled matrices: P, Q (2 nslab + 1, n, n) at z0 + k dz/2.
+        Returns the dict of rcwa_integrate."""
+        P, Q = self._samples(P, Q)
+        if P.shape[0] < 3 or P.shape[0] % 2 == 0:
+            raise ValueError("P, Q must be (2 nslab + 1, n, n)")
+        return self._integrate(self.lib.rcwa_differential_integrate, "differential_integrate", P, Q,
+                               (P.shape[0] - 1) // 2, lam, z0, z1)
 
     def ofd_solve(self, setup, orders=True):
         """The rcwa_run computation for a setup object with the

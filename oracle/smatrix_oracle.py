@@ -14,6 +14,8 @@ Restates, in NumPy:
   (core/RCWAIntegrator.cpp:57-67, core/RedhefferIntegrator.cpp:136-146).
 * RCWAIntegrator::compute (core/RCWAIntegrator.cpp:21-86) over sampled P, Q.
 * DifferentialIntegrator::compute (core/DifferentialIntegrator.cpp:21-133).
+* RedhefferIntegrator::compute (core/RedhefferIntegrator.cpp:190-328), the
+  adaptive triple division, with the sampler called back for new depths.
 
 Eigen's ``PartialPivLU::solve`` / ``inverse`` map to ``numpy.linalg.solve`` /
 ``numpy.linalg.inv`` (LAPACK getrf/getrs/getri).
@@ -191,3 +193,103 @@ def differential_integrate(P, Q, lam, z0, z1):
     out = _top_projection(S, W1, V1, W0, V0)
     out.update({"W0": W0, "V0": V0, "gam0": g0, "W1": W1, "V1": V1, "gam1": g1})
     return out
+
+
+def _perturbation(sample, z0, z1, lam, P0, Q0, P1, Q1, Pr, Qr, W, V, gam):
+    """RedhefferIntegrator::evaluatePerturbationAndDifference
+    (core/RedhefferIntegrator.cpp:330-398): first-order S-matrix of [z0, z1]
+    around the reference modes (W, V, gam) of the interval's midpoint, by
+    Simpson's rule; the midpoint term vanishes (the midpoint sample is the
+    reference).  Returns (tdd, tuu, rud, rdu, diffError)."""
+    k0 = 2 * math.pi / lam
+    L = z1 - z0
+    dA, dB = [], []
+    for Pk, Qk in ((P0, Q0), (P1, Q1)):
+        x = np.linalg.solve(W, (Pk - Pr) @ V)
+        y = np.linalg.solve(V, (Qk - Qr) @ W)
+        dA.append(x + y)
+        dB.append(x - y)
+    pf = np.exp(1j * L / k0 * gam)
+    c = 1j * L / (6 * 2 * k0)
+    tuu = c * (pf[:, None] * dA[0] + dA[1] * pf[None, :])
+    rud = -c * (pf[:, None] * dB[0] * pf[None, :] + dB[1])
+    rdu = -c * (dB[0] + pf[:, None] * dB[1] * pf[None, :])
+    tdd = c * (dA[0] * pf[None, :] + pf[:, None] * dA[1])
+    err = max(np.abs(m).max() for m in (tuu, rud, rdu, tdd))
+    return tdd + np.diag(pf), tuu + np.diag(pf), rud, rdu, err
+
+
+def redheffer_integrate(sample, lam, z0, z1, pe, max_intervals=100000):
+    """RedhefferIntegrator::compute (core/RedhefferIntegrator.cpp:190-328,
+    the triple-division branch): an interval whose perturbation S-matrix
+    (around its midpoint's modes) has an entry above ``pe`` is split into
+    thirds, the middle third keeping the parent's reference; accepted
+    intervals are projected from the previous interval's modes and cascaded
+    from the top down; the bottom is brought into the modes at z1.
+    ``sample(z)`` returns (P, Q).  Returns the dict of rcwa_integrate plus
+    N (accepted intervals) and nEigVal (eigen-solves)."""
+    cache = {}
+
+    def smp(z):
+        if z not in cache:
+            cache[z] = sample(z)
+        return cache[z]
+
+    P0, Q0 = smp(z0)
+    P1, Q1 = smp(z1)
+    W0, V0, g0 = wave_equation_modes(P0, Q0)
+    W1, V1, g1 = wave_equation_modes(P1, Q1)
+    zm = 0.5 * (z0 + z1)
+    Pm, Qm = smp(zm)
+    Wm, Vm, gm = wave_equation_modes(Pm, Qm)
+    n = W0.shape[0]
+    state = {"S": identity_smatrix(n), "leftW": W0, "leftV": V0, "N": 0, "nEig": 3}
+
+    def accept(s, W, V):
+        tdd, tuu, rud, rdu = s
+        F = np.linalg.solve(W, state["leftW"])
+        G = np.linalg.solve(V, state["leftV"])
+        A, B = 0.5 * (F + G), 0.5 * (F - G)
+        M = A - rdu @ B
+        rdu = np.linalg.solve(M, rdu @ A - B)
+        tdd = np.linalg.solve(M, tdd)
+        rud = tuu @ B @ tdd + rud
+        tuu = tuu @ A + tuu @ B @ rdu
+        state["leftW"], state["leftV"] = W, V
+        state["S"] = star_product(state["S"], {"rud": rud, "rdu": rdu, "tdd": tdd, "tuu": tuu})
+        state["N"] += 1
+
+    def rec(Pr, Qr, W, V, g, za, zb, Pa, Qa, Pb, Qb):
+        tdd, tuu, rud, rdu, err = _perturbation(None, za, zb, lam, Pa, Qa, Pb, Qb, Pr, Qr, W, V, g)
+        if err <= pe:
+            if state["N"] >= max_intervals:
+                raise RuntimeError("interval limit")
+            accept((tdd, tuu, rud, rdu), W, V)
+            return
+        zm0 = 2.0 / 3.0 * za + 1.0 / 3.0 * zb
+        zm1 = 1.0 / 3.0 * za + 2.0 / 3.0 * zb
+        Pt, Qt = smp(0.5 * (za + zm0))
+        Pk, Qk = smp(zm0)
+        Wt, Vt, gt = wave_equation_modes(Pt, Qt)
+        state["nEig"] += 1
+        rec(Pt, Qt, Wt, Vt, gt, za, zm0, Pa, Qa, Pk, Qk)
+        Pt2, Qt2 = smp(zm1)
+        rec(Pr, Qr, W, V, g, zm0, zm1, Pk, Qk, Pt2, Qt2)
+        Pk2, Qk2 = smp(0.5 * (zm1 + zb))
+        Wk, Vk, gk = wave_equation_modes(Pk2, Qk2)
+        state["nEig"] += 1
+        rec(Pk2, Qk2, Wk, Vk, gk, zm1, zb, Pt2, Qt2, Pb, Qb)
+
+    rec(Pm, Qm, Wm, Vm, gm, z0, z1, P0, Q0, P1, Q1)
+    # the bottom into the modes at z1 (:235-245)
+    S = state["S"]
+    F = np.linalg.solve(state["leftW"], W1)
+    G = np.linalg.solve(state["leftV"], V1)
+    A, B = 0.5 * (F + G), 0.5 * (F - G)
+    M = A - S["Rud"] @ B
+    Tuu = np.linalg.solve(M, S["Tuu"])
+    Rud = np.linalg.solve(M, S["Rud"] @ A - B)
+    Rdu = S["Rdu"] + S["Tdd"] @ B @ Tuu
+    Tdd = S["Tdd"] @ (B @ Rud + A)
+    return {"Tdd": Tdd, "Tuu": Tuu, "Rud": Rud, "Rdu": Rdu, "W0": W0, "V0": V0, "gam0": g0,
+            "W1": W1, "V1": V1, "gam1": g1, "N": state["N"], "nEigVal": state["nEig"]}

@@ -42,3 +42,11 @@ def samples(nslab, moving, z0=Z0, z1=Z1):
     zs = [z0] + [z0 + (i + 0.5) * dz for i in range(nslab)] + [z1]
     PQ = [sample(z, moving) for z in zs]
     return np.array([p for p, _ in PQ]), np.array([q for _, q in PQ])
+
+
+def half_step_samples(nslab, moving, z0=Z0, z1=Z1):
+    """P, Q stacked as [2 nslab + 1, n, n] at z0 + k dz/2 (the differential
+    integrator's left ends, midpoints and right ends)."""
+    dz = (z1 - z0) / nslab
+    PQ = [sample(z0 + k * dz / 2, moving) for k in range(2 * nslab + 1)]
+    return np.array([p for p, _ in PQ]), np.array([q for _, q in PQ])

@@ -59,3 +59,49 @@ def test_moving_edge_converges_at_second_order(eng):
         errs.append(np.abs(eng.rcwa_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1)["Tuu"] - Tref).max() / scale)
     assert all(a / b > 3.0 for a, b in zip(errs, errs[1:])), errs
     assert errs[-1] < 1e-4
+
+
+@pytest.mark.parametrize("nslab", [1, 7, 16])
+def test_differential_matches_oracle_in_field_space(eng, nslab):
+    P, Q = ic.half_step_samples(nslab, moving=True)
+    got = eng.differential_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1)
+    want = so.differential_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1)
+    fg, fw = so.field_space(got), so.field_space(want)
+    for key in fg:
+        assert np.abs(fg[key] - fw[key]).max() < 1e-9 * max(1.0, np.abs(fw[key]).max()), key
+
+
+def test_differential_agrees_with_rcwa_on_the_device(eng):
+    # in field space: the two integrators' end modes need not be ordered alike
+    P, Q = ic.samples(512, moving=True)
+    Tr = so.field_space(eng.rcwa_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1))["Tuu"]
+    P, Q = ic.half_step_samples(512, moving=True)
+    Td = so.field_space(eng.differential_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1))["Tuu"]
+    assert np.abs(Td - Tr).max() / np.abs(Tr).max() < 1e-5
+
+
+@pytest.mark.parametrize("pe", [1e-2, 1e-3])
+def test_redheffer_matches_oracle(eng, pe):
+    sampler = lambda z: ic.sample(z, True)
+    n = 2 * ic.NX * ic.NY
+    got = eng.redheffer_integrate(sampler, n, ic.LAM, ic.Z0, ic.Z1, pe)
+    want = so.redheffer_integrate(sampler, ic.LAM, ic.Z0, ic.Z1, pe)
+    # the same subdivision, and the same S-matrix in field space
+    assert got["N"] == want["N"] and got["n_eig"] == want["nEigVal"]
+    fg, fw = so.field_space(got), so.field_space(want)
+    for key in fg:
+        assert np.abs(fg[key] - fw[key]).max() < 1e-9 * max(1.0, np.abs(fw[key]).max()), key
+
+
+def test_redheffer_uniform_and_sampler_failure(eng):
+    n = 2 * ic.NX * ic.NY
+    out = eng.redheffer_integrate(lambda z: ic.sample(z, False), n, ic.LAM, ic.Z0, ic.Z1, 1e-3)
+    L = (ic.Z1 - ic.Z0) * ic.LAM / (2 * np.pi)
+    assert out["N"] == 1
+    assert np.abs(out["Tuu"] - np.diag(np.exp(1j * out["gam0"] * L))).max() < 1e-8
+
+    def bad(z):
+        raise KeyError("no sample at %g" % z)
+
+    with pytest.raises(KeyError):
+        eng.redheffer_integrate(bad, n, ic.LAM, ic.Z0, ic.Z1, 1e-3)

@@ -52,3 +52,43 @@ def test_field_space_blocks_ignore_the_mode_gauge(monkeypatch):
     other = so.field_space(so.rcwa_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1))
     for k in base:
         assert np.abs(base[k] - other[k]).max() < 1e-12 * max(1.0, np.abs(base[k]).max()), k
+
+
+def test_differential_converges_to_the_uniform_phase():
+    # tests/test_core_integrators.cpp:100-116: the numerical integration
+    # approaches the analytic phase as the slab count grows
+    L = (ic.Z1 - ic.Z0) * ic.LAM / (2 * np.pi)
+    errs = []
+    for N in (64, 128, 256):
+        P, Q = ic.half_step_samples(N, moving=False)
+        out = so.differential_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1)
+        errs.append(np.abs(out["Tuu"] - np.diag(np.exp(1j * out["gam0"] * L))).max())
+    assert errs[0] > errs[1] > errs[2] and errs[2] < 1e-5, errs
+
+
+def test_differential_agrees_with_rcwa():
+    # tests/test_core_integrators.cpp:141-146 (at 256 slabs each)
+    P, Q = ic.samples(256, moving=True)
+    Tr = so.field_space(so.rcwa_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1))["Tuu"]
+    P, Q = ic.half_step_samples(256, moving=True)
+    Td = so.field_space(so.differential_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1))["Tuu"]
+    assert np.abs(Td - Tr).max() / np.abs(Tr).max() < 1e-5
+
+
+def test_redheffer_agrees_with_rcwa():
+    # tests/test_core_integrators.cpp:141-151: pe = 1e-3 against the RCWA
+    # integrator with 256 slabs (the reference takes 512), relative 1e-3
+    P, Q = ic.samples(256, moving=True)
+    Tr = so.field_space(so.rcwa_integrate(P, Q, ic.LAM, ic.Z0, ic.Z1))["Tuu"]
+    out = so.redheffer_integrate(lambda z: ic.sample(z, True), ic.LAM, ic.Z0, ic.Z1, 1e-3)
+    Th = so.field_space(out)["Tuu"]
+    assert out["N"] > 1
+    assert np.abs(Th - Tr).max() / np.abs(Tr).max() < 1e-3
+
+
+def test_redheffer_uniform_region_is_one_interval():
+    out = so.redheffer_integrate(lambda z: ic.sample(z, False), ic.LAM, ic.Z0, ic.Z1, 1e-3)
+    L = (ic.Z1 - ic.Z0) * ic.LAM / (2 * np.pi)
+    assert out["N"] == 1
+    assert np.abs(out["Tuu"] - np.diag(np.exp(1j * out["gam0"] * L))).max() < 1e-8
+    assert np.abs(out["Rud"]).max() < 1e-8
