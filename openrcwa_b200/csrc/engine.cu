@@ -917,18 +917,41 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
       const size_t oItemsM = meta.add_vec(itm), oMpq = meta.add_vec(mpq), oMq = meta.add_vec(mq);
       const size_t opA = meta.add_vec(pA), opB = meta.add_vec(pB), opD = meta.add_vec(pD);
       const size_t oqA = meta.add_vec(qA), oqB = meta.add_vec(qB), oqD = meta.add_vec(qD);
-      // V GEMMs: top = fe22 * Wb, bottom = fe11 * Wt
-      std::vector<const cplx*> vA(2 * nn_j), vB(2 * nn_j);
-      std::vector<cplx*> vD(2 * nn_j);
-      for (int q = 0; q < nn_j; ++q) {
-        vA[q] = itn[q].fe22;
-        vB[q] = itn[q].W + (size_t)N * n;
-        vD[q] = itn[q].V;
-        vA[nn_j + q] = itn[q].fe11;
-        vB[nn_j + q] = itn[q].W;
-        vD[nn_j + q] = itn[q].V + (size_t)N * n;
-      }
+      // V GEMMs: top = fe22 * Wb, bottom = fe11 * Wt; the jobs of points
+      // whose products run in 3xTF32 first (their top and bottom products),
+      // then those of the FP64 points
+      const bool tc_modes = precision == RCWA_PREC_MIXED && c.prod != 1;
+      std::vector<int> vorder;
+      for (int pass = 0; pass < 2; ++pass)
+        for (int q = 0; q < nn_j; ++q) {
+          const bool tc = tc_modes && !c.fp64_pt[c.job_point[jn[q]]];
+          if (tc == (pass == 0)) vorder.push_back(q);
+        }
+      int ntv = 0;  // 3xTF32 V products
+      for (int q = 0; q < nn_j; ++q) ntv += (tc_modes && !c.fp64_pt[c.job_point[jn[q]]]) ? 2 : 0;
+      std::vector<const cplx*> vA, vB;
+      std::vector<cplx*> vD;
+      auto vput = [&](int q0, int q1) {
+        for (int i = q0; i < q1; ++i) {
+          const LayerItem& t = itn[vorder[i]];
+          vA.push_back(t.fe22); vB.push_back(t.W + (size_t)N * n); vD.push_back(t.V);
+        }
+        for (int i = q0; i < q1; ++i) {
+          const LayerItem& t = itn[vorder[i]];
+          vA.push_back(t.fe11); vB.push_back(t.W); vD.push_back(t.V + (size_t)N * n);
+        }
+      };
+      vput(0, ntv / 2);
+      vput(ntv / 2, nn_j);
       const size_t ovA = meta.add_vec(vA), ovB = meta.add_vec(vB), ovD = meta.add_vec(vD);
+      int* tcerr_m = P->dTcErr;
+      int* tcscale_m = P->dTcScale;
+      float* planes_m = (float*)(wb + c.planes);
+      const size_t planes_bytes_m = c.planes_bytes;
+      // 3xTF32 products per call: the scale workspace's 2048 items, and as
+      // many as the plane scratch holds split (else the per-tile split kernel)
+      const size_t per_v = zgemm_tf32x3_planes_bytes(N, n, N, 1);
+      const int sub_v = (int)std::max<size_t>(1, std::min<size_t>(2048, per_v ? planes_bytes_m / per_v : 2048));
       cplx* mu = W_(c.mu);
       void* eigw = wb + c.eigw;
       int* einfo = (int*)(wb + c.einfo);
@@ -983,8 +1006,21 @@ int plan_create_impl(rcwa_engine* e, const std::vector<StackInfo>& si, const rcw
           v.M = N; v.N = n; v.K = N;
           v.lda = N; v.ldb = n; v.ldc = n; v.ldd = n;
           v.alpha = mkc(1, 0); v.beta = mkc(0, 0); v.gammaI = mkc(0, 0);
-          v.batch = 2 * nn_j;
-          if ((err = zgemm_batched(v, st)) != cudaSuccess) return err;
+          // 3xTF32 for the points with tensor-core products (a mixed plan's
+          // modal V, like its cascade products), FP64 for the rest
+          for (int b0 = 0; b0 < ntv; b0 += sub_v) {
+            GemmArgs t = v;
+            t.A = v.A + b0; t.B = v.B + b0; t.D = v.D + b0;
+            t.batch = std::min(sub_v, ntv - b0);
+            if ((err = zgemm_tf32x3_batched(t, tcscale_m, tcerr_m, st, 128, planes_m, planes_bytes_m)) != cudaSuccess)
+              return err;
+          }
+          if (ntv < 2 * nn_j) {
+            GemmArgs f = v;
+            f.A = v.A + ntv; f.B = v.B + ntv; f.D = v.D + ntv;
+            f.batch = 2 * nn_j - ntv;
+            if ((err = zgemm_batched(f, st)) != cudaSuccess) return err;
+          }
           if ((err = finish_modes(it, nn_j, N, status, st)) != cudaSuccess) return err;
         }
         if (nm_j > 0) {
