@@ -389,7 +389,8 @@ def run_cfg5(args):
                     "400 nm, Nx=Ny=%d (%d orders, %d x %d layer matrices), first %d of 32 wavelengths 500-900 nm, "
                     "normal incidence, TE+TM" % ("2.1" if lossless else "2.1+0.01i", nh, stacks[0].N, n, n, npts),
         "precision": ("fp64" if lossless else
-                      "mixed: cascade products and blocked-LU updates 3xTF32 on tcgen05, eigensolve FP64"),
+                      "mixed: cascade products, modal V and blocked-LU updates 3xTF32 on tcgen05, "
+                      "eigensolve FP64"),
         "solves_per_s": npts / (ms * 1e-3), "ms_per_execution": ms, "plan_create_s": t_create,
         "chunks": len(chunks), "eigensolves": nj,
         "ctas_per_matrix": {"eigensolver": o.eig_cluster_size(n, nj // max(1, len(chunks))),
@@ -838,10 +839,10 @@ def main():
             "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128 with tf32x3 cascade products", "data": "synthetic",
             "config": {"workload": WORKLOAD, "batch_points_per_gpu": B, "orders": N, "matrix": n,
-                       "precision": "mixed: cascade GEMMs and the K = 128 updates of the blocked interface/tau "
-                                    "LU factorisations and solves 3xTF32 on tcgen05 (FP32 accumulation within "
-                                    "K-blocks, FP64 across); eigensolve, LU panels and triangles, half-spaces "
-                                    "and efficiency sums FP64",
+                       "precision": "mixed: cascade GEMMs, modal V products and the K = 128 updates of the "
+                                    "blocked interface/tau LU factorisations and solves 3xTF32 on tcgen05 (FP32 "
+                                    "accumulation within K-blocks, FP64 across); eigensolve, LU panels and "
+                                    "triangles, half-spaces and efficiency sums FP64",
                        "parallelism": f"replicas x{world}",
                        "l2": "per-step working set several GB > 126 MB L2"},
             "outputs_per_s": {"value": value * bpxy.shape[1], "unit": "(point, polarisation) R/T outputs/s",
