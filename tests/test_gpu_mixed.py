@@ -1,9 +1,8 @@
 """The mixed-precision solve (cascade GEMMs, modal V products and the updates
 between the 128-wide blocks of the interface and tau factorisations and
 solves in 3xTF32 on tcgen05; eigensolve, LU panels and triangles in FP64):
-every efficiency
-within 1e-4 of the FP64 oracle (the mixed-precision accuracy bound), and the
-FP64 plan on the same inputs within 1e-9."""
+every efficiency within 1e-4 of the FP64 oracle (the mixed-precision
+accuracy bound), and the FP64 plan on the same inputs within 1e-9."""
 import numpy as np
 import pytest
 
