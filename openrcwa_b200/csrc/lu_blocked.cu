@@ -24,6 +24,13 @@
 namespace {
 
 constexpr int kNb = 128;  // rows per block
+// right-hand sides per CTA of the diagonal-block solves (one per thread): the
+// tiles of the triangle staged in shared memory serve all of them; a build
+// parameter
+#ifndef RCWA_DIAG_THREADS
+#define RCWA_DIAG_THREADS 64
+#endif
+constexpr int kDiagThreads = RCWA_DIAG_THREADS;
 
 // B <- P B: the interchanges of getrf, one thread per column
 __global__ void laswp_kernel(cplx* const* Barr, int n, int ldb, int nrhs, const int* ipiv_all) {
@@ -53,12 +60,12 @@ __device__ __forceinline__ void load_tile32(cplx (*Tsm)[33], const cplx* LU, int
 // [c_lo, nrhs) only (the inverse's forward pass skips columns whose rows
 // here are still zero).
 template <bool kUpper>
-__global__ void __launch_bounds__(64) trsm_diag_kernel(const cplx* const* LUarr, int lda, cplx* const* Barr, int ldb,
+__global__ void __launch_bounds__(kDiagThreads) trsm_diag_kernel(const cplx* const* LUarr, int lda, cplx* const* Barr, int ldb,
                                                       int nrhs, int r0, int rows, int c_lo) {
   __shared__ cplx Tsm[32][33];
   __shared__ cplx dinv[32];  // backward: reciprocals of the quarter's diagonal
   const int b = blockIdx.y;
-  const int c = c_lo + blockIdx.x * 64 + threadIdx.x;
+  const int c = c_lo + blockIdx.x * kDiagThreads + threadIdx.x;
   const bool col = c < nrhs;
   const cplx* LU = LUarr[b];
   cplx* B = Barr[b];
@@ -141,8 +148,8 @@ cudaError_t zgetrf_blocked_batched(cplx* const* A, int n, int lda, int* ipiv, in
     if ((e = zgetrf_columns(A, n, lda, kb, ke, ipiv, info, batch, st)) != cudaSuccess) return e;
     if (ke == n) break;
     // U12 = L11^-1 A12: the block's rows, columns ke .. n-1
-    trsm_diag_kernel<false><<<dim3((n - ke + 63) / 64, batch), 64, 0, st>>>((const cplx* const*)A, lda, A, lda, n, kb,
-                                                                            ke - kb, ke);
+    trsm_diag_kernel<false><<<dim3((n - ke + kDiagThreads - 1) / kDiagThreads, batch), kDiagThreads, 0, st>>>(
+        (const cplx* const*)A, lda, A, lda, n, kb, ke - kb, ke);
     ++launch_counter();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     // A22 -= L21 U12
@@ -178,8 +185,8 @@ cudaError_t zgetrs_blocked_batched(const cplx* const* LU, int n, int lda, const 
     const int rw = min(kNb, n - kb);
     // the inverse's rows kb.. are zero in the columns past the block (L^-1 is lower triangular)
     const int c_lo = 0, c_hi = inverse ? kb + rw : nrhs;
-    trsm_diag_kernel<false><<<dim3((c_hi - c_lo + 63) / 64, batch), 64, 0, st>>>(LU, lda, B, ldb, c_hi, kb, rw,
-                                                                                   c_lo);
+    trsm_diag_kernel<false><<<dim3((c_hi - c_lo + kDiagThreads - 1) / kDiagThreads, batch), kDiagThreads, 0, st>>>(
+        LU, lda, B, ldb, c_hi, kb, rw, c_lo);
     ++launch_counter();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     const int m2 = n - kb - rw;
@@ -199,7 +206,8 @@ cudaError_t zgetrs_blocked_batched(const cplx* const* LU, int n, int lda, const 
   // backward: U
   for (int kb = ((n - 1) / kNb) * kNb; kb >= 0; kb -= kNb) {
     const int rw = min(kNb, n - kb);
-    trsm_diag_kernel<true><<<dim3((nrhs + 63) / 64, batch), 64, 0, st>>>(LU, lda, B, ldb, nrhs, kb, rw, 0);
+    trsm_diag_kernel<true><<<dim3((nrhs + kDiagThreads - 1) / kDiagThreads, batch), kDiagThreads, 0, st>>>(
+        LU, lda, B, ldb, nrhs, kb, rw, 0);
     ++launch_counter();
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (kb > 0) {
