@@ -52,6 +52,12 @@ def test_status_strings_and_argument_checks():
     assert lib.rcwa_plan_execute(None, None) == o.abi.RCWA_ERR_INVALID
     assert lib.rcwa_plan_rescatter(None, None) == o.abi.RCWA_ERR_INVALID
     assert lib.rcwa_zgeev_batched_noalloc(0, 1, None, None, None, None, None) == o.abi.RCWA_ERR_INVALID
+    # the z-integrators reject a missing engine or missing samples before any device work
+    null12 = [None] * 12
+    assert lib.rcwa_rcwa_integrate(None, 4, 2, 1.0, 0.0, 1.0, *null12) == o.abi.RCWA_ERR_INVALID
+    assert lib.rcwa_differential_integrate(None, 4, 2, 1.0, 0.0, 1.0, *null12) == o.abi.RCWA_ERR_INVALID
+    assert lib.rcwa_redheffer_integrate(None, 4, 1.0, 0.0, 1.0, 1e-3, 100, o.abi.RCWA_SAMPLER(),
+                                        None, *([None] * 10), None, None) == o.abi.RCWA_ERR_INVALID
 
 
 def test_product_fails_loudly_without_its_library(monkeypatch):
