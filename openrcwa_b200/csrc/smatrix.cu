@@ -1130,7 +1130,12 @@ extern "C" int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, do
   std::sort(acc.begin(), acc.end(), [](const Accepted& a, const Accepted& b) { return a.za < b.za; });
   const int na = (int)acc.size();
   SBank S(n, na);
-  if (!S.buf.p) return set_err(e, RCWA_ERR_NOMEM, "allocation failed");
+  // statuses of the projection, cascade and bottom steps, one per accepted
+  // interval (the cascade's star products report by interval)
+  Buf dcstat(sizeof(int) * na);
+  if (!S.buf.p || !dcstat.p || cudaMemsetAsync(dcstat.p, 0, sizeof(int) * na, st) != cudaSuccess)
+    return set_err(e, RCWA_ERR_NOMEM, "allocation failed");
+  int* cstat = (int*)dcstat.p;
   {
     std::vector<cplx*> src, dst;
     for (int i = 0; i < na; ++i)
@@ -1149,8 +1154,8 @@ extern "C" int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, do
       lW[i] = i ? refs[acc[i - 1].ref].W : top.W;
       lV[i] = i ? refs[acc[i - 1].ref].V : top.V;
     }
-    rc = project_items(e, n, iW, iV, lW, lV, S, stat, st);
-    if (rc == RCWA_OK) rc = cascade_tree(e, n, na, S, stat, st);
+    rc = project_items(e, n, iW, iV, lW, lV, S, cstat, st);
+    if (rc == RCWA_OK) rc = cascade_tree(e, n, na, S, cstat, st);
     if (rc != RCWA_OK) return rc;
   }
   // the bottom into the modes at z1 (:235-245): F = iW_last W1,
@@ -1186,7 +1191,7 @@ extern "C" int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, do
     mm(pRud, pB, pM, -1.0, (long)pA, 1.0);     // M = A - Rud B
     mm(pRud, pA, pX1, 1.0, (long)pB, -1.0);    // X1 = Rud A - B
     run(zgetrf_batched(pb.at(pM), n, n, (int*)dpiv.p, (int*)dinf.p, 1, st));
-    run(fold_info((int*)dinf.p, pb.ints(pI), 1, RCWA_ERR_SINGULAR, stat, st));
+    run(fold_info((int*)dinf.p, pb.ints(pI), 1, RCWA_ERR_SINGULAR, cstat, st));
     run(zgetrs_batched(pb.cat(pM), n, n, (int*)dpiv.p, pb.at(pTuu), n, n, 1, st));  // Tuu'
     run(zgetrs_batched(pb.cat(pM), n, n, (int*)dpiv.p, pb.at(pX1), n, n, 1, st));   // Rud'
     mm(pB, pTuu, pT, 1.0, -1, 0.0);                  // T = B Tuu'
@@ -1195,10 +1200,12 @@ extern "C" int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, do
     mm(pTdd, pT, pM, 1.0, -1, 0.0);                  // Tdd'
     if (err != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
       return set_err(e, RCWA_ERR_CUDA, "integrator kernels failed");
-    int hs = 0;
-    if (cudaMemcpy(&hs, stat, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    std::vector<int> hs(na + 1);
+    if (cudaMemcpy(hs.data(), stat, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess ||
+        cudaMemcpy(hs.data() + 1, cstat, sizeof(int) * na, cudaMemcpyDeviceToHost) != cudaSuccess)
       return set_err(e, RCWA_ERR_CUDA, "download failed");
-    if (hs != RCWA_OK) return set_err(e, hs, "singular matrix in the integrator");
+    for (int v : hs)
+      if (v != RCWA_OK) return set_err(e, v, "singular matrix in the integrator");
     const size_t mb = sizeof(cplx) * nn;
     struct Out { rcwa_cplx* h; const void* d; } outs[] = {
         {Rud, dx.c() + nn * kX1}, {Rdu, S.at(1, 0)}, {Tdd, dx.c() + nn * kM}, {Tuu, S.at(3, 0)}};
