@@ -40,7 +40,8 @@ EXPORTS = [
     "rcwa_plan_launch_count", "rcwa_plan_rescatter", "rcwa_plan_set_profiling", "rcwa_plan_stage_times", "rcwa_stage_name",
     "rcwa_plan_destroy", "rcwa_fourier1d", "rcwa_fourier2d",
     "rcwa_layer_solve", "rcwa_zgeev_batched", "rcwa_zgeev_batched_noalloc", "rcwa_ofd_solve",
-    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_rcwa_integrate", "rcwa_differential_integrate", "rcwa_redheffer_integrate", "rcwa_zgemm_batched",
+    "rcwa_slab_smatrix_batched", "rcwa_star_product_batched", "rcwa_rcwa_integrate", "rcwa_differential_integrate",
+    "rcwa_redheffer_integrate", "rcwa_zgemm_batched",
     "rcwa_mlp_create", "rcwa_mlp_destroy", "rcwa_mlp_param_count", "rcwa_mlp_get_params", "rcwa_mlp_set_params",
     "rcwa_mlp_set_data", "rcwa_mlp_train", "rcwa_mlp_loss_grad", "rcwa_mlp_predict_fp32", "rcwa_mlp_predict",
     "rcwa_plan_schedule", "rcwa_tuner_create", "rcwa_tuner_destroy", "rcwa_tuner_set_sms", "rcwa_tuner_candidates",

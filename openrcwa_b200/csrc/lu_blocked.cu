@@ -62,8 +62,9 @@ __device__ __forceinline__ void load_tile32(cplx (*Tsm)[33], const cplx* LU, int
 // [c_lo, nrhs) only (the inverse's forward pass skips columns whose rows
 // here are still zero).
 template <bool kUpper>
-__global__ void __launch_bounds__(kDiagThreads) trsm_diag_kernel(const cplx* const* LUarr, int lda, cplx* const* Barr, int ldb,
-                                                      int nrhs, int r0, int rows, int c_lo) {
+__global__ void __launch_bounds__(kDiagThreads) trsm_diag_kernel(const cplx* const* LUarr, int lda,
+                                                                 cplx* const* Barr, int ldb, int nrhs, int r0,
+                                                                 int rows, int c_lo) {
   __shared__ cplx Tsm[32][33];
   __shared__ cplx dinv[32];  // backward: reciprocals of the quarter's diagonal
   const int b = blockIdx.y;

@@ -1037,9 +1037,10 @@ extern "C" int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, do
       const RedInterval* iv = pending.data() + c0;
       const size_t Pa = lst([&](int i) { return iv[i].a.P; }), Qa = lst([&](int i) { return iv[i].a.Q; });
       const size_t Pb = lst([&](int i) { return iv[i].b.P; }), Qb = lst([&](int i) { return iv[i].b.Q; });
-      const size_t Pr = lst([&](int i) { return refs[iv[i].ref].P; }), Qr = lst([&](int i) { return refs[iv[i].ref].Q; });
-      const size_t Wr = lst([&](int i) { return refs[iv[i].ref].W; }), Vr = lst([&](int i) { return refs[iv[i].ref].V; });
-      const size_t iWr = lst([&](int i) { return refs[iv[i].ref].iW; }), iVr = lst([&](int i) { return refs[iv[i].ref].iV; });
+      auto ref_of = [&](int i) -> const RedRef& { return refs[iv[i].ref]; };
+      const size_t Pr = lst([&](int i) { return ref_of(i).P; }), Qr = lst([&](int i) { return ref_of(i).Q; });
+      const size_t Wr = lst([&](int i) { return ref_of(i).W; }), Vr = lst([&](int i) { return ref_of(i).V; });
+      const size_t iWr = lst([&](int i) { return ref_of(i).iW; }), iVr = lst([&](int i) { return ref_of(i).iV; });
       size_t t[kCnt];
       for (int k = 0; k < kCnt; ++k) t[k] = lst([&](int i) { return T(k, i); });
       if (!pb.upload(st)) return set_err(e, RCWA_ERR_CUDA, "upload failed");
