@@ -39,13 +39,17 @@ extern "C" {
 
 /* ---- precision of the batched solve ---------------------------------------- */
 #define RCWA_PREC_FP64  0     /* every stage complex128                           */
-#define RCWA_PREC_MIXED 1     /* cascade GEMMs (F, G, Rud, Tdd) in 3xTF32 on the
-                                 tensor cores with FP32 accumulation; the
-                                 eigensolve, the interface and tau solves, the
-                                 half-spaces and the efficiency sums stay FP64.
-                                 Stacks with a metallic layer (Re eps < 0 in
-                                 some cell) keep FP64 products: their cascade
-                                 is too ill-conditioned for 3xTF32             */
+#define RCWA_PREC_MIXED 1     /* cascade GEMMs (F, G, Rud, Tdd), modal V = Q W
+                                 products and the updates between the 128-wide
+                                 blocks of the interface and tau LU
+                                 factorisations and solves in 3xTF32 on the
+                                 tensor cores (FP32 accumulation within
+                                 K-blocks of 256, FP64 across); the eigensolve,
+                                 the LU panels and triangles, the half-spaces
+                                 and the efficiency sums stay FP64.  Stacks
+                                 with a metallic layer (Re eps < 0 in some
+                                 cell) keep FP64 throughout: their cascade is
+                                 too ill-conditioned for 3xTF32               */
 
 typedef struct { double re, im; } rcwa_cplx;
 
