@@ -78,6 +78,27 @@ def test_cpp_adapters_compile_without_eigen():
                     "-I", os.path.join(ROOT, "include", "openrcwa_b200"), src], check=True)
 
 
+def test_integrator_adapters_build_and_fail_softly_without_a_device(tmp_path):
+    # the core/ integrator adapters with a LayerSampler-shaped sampler: they
+    # compile without Eigen, link against the library, and with no device
+    # report and leave their outputs empty, as the other adapters do
+    o, lib = _lib()
+    h = ctypes.c_void_p()
+    if lib.rcwa_engine_create(0, ctypes.byref(h)) == 0:
+        lib.rcwa_engine_destroy(h)
+        pytest.skip("a GPU is present")
+    src = os.path.join(ROOT, "tests", "cpp", "adapter_integrators.cpp")
+    libdir = os.path.dirname(o.abi.LIB_PATH)
+    exe = os.path.join(tmp_path, "adapter_integrators")
+    inc = os.path.join(ROOT, "include", "openrcwa_b200")
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-DRCWA_B200_NO_EIGEN", "-I", inc, src, "-L", libdir, "-lrcwa_b200",
+                    "-Wl,-rpath," + libdir, "-o", exe], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0
+    assert out.stdout.split() == ["0", "0", "0", "0"]
+    assert "engine unavailable" in out.stderr
+
+
 # where the reference sources are mounted: the drop-in recipe knows (REF env var)
 REF = subprocess.run(["sh", os.path.join(ROOT, "oracle", "build_ref.sh"), "--print-ref"], capture_output=True,
                      text=True).stdout.strip()
