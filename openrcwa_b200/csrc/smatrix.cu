@@ -959,8 +959,9 @@ extern "C" int rcwa_redheffer_integrate(rcwa_engine* e, int n, double lambda, do
     for (size_t i = 0; i < fresh.size(); ++i) {
       if (sample(user, fresh[i], hP.data(), hQ.data()) != 0) return set_err(e, RCWA_ERR_INVALID, "sampler failed");
       RedSample sm{blk + 2 * nn * i, blk + 2 * nn * i + nn};
-      if (cudaMemcpy(sm.P, hP.data(), sizeof(cplx) * nn, cudaMemcpyHostToDevice) != cudaSuccess ||
-          cudaMemcpy(sm.Q, hQ.data(), sizeof(cplx) * nn, cudaMemcpyHostToDevice) != cudaSuccess)
+      // ordered on the engine's stream ahead of the kernels that read them
+      // (pageable sources are staged before the call returns)
+      if (!up(sm.P, hP.data(), nn, st) || !up(sm.Q, hQ.data(), nn, st))
         return set_err(e, RCWA_ERR_CUDA, "upload failed");
       samples[fresh[i]] = sm;
     }
